@@ -1,0 +1,380 @@
+"""Benchmark: contracted ERI quartets/s on one B200 (or N, weak scaling).
+
+Workload (one step = one pass of the ERI path over one batch):
+  1e6 shell quartets, l in {0,1,2} per shell (class uniform over the 81
+  (la,lb,lc,ld) classes), K uniform in {1..6} per shell, exponents log-uniform
+  in [0.05, 1e4], coefficients uniform [0.1, 1] then normalised, centres
+  uniform in a 30-bohr cube, spherical output, seed 1 (rank r uses seed 1+r).
+  Synthetic data with the shapes of that configuration.
+
+Arms:
+  default          : this library, FP64 path and mixed-precision path
+  --impl reference : the reference's own CPU implementation of the path (the
+                     C99 its generator emits, oracle/_ref, OpenMP over the
+                     box's cores) on a bounded sample of the same workload.
+
+Prints one JSON line (rank 0).  value = quartets/s of the headline path over
+all ranks, device-timed with inputs resident in HBM (inputs + outputs ~1 GB,
+larger than L2, so no flush is needed); e2e = the same through the public API
+with host buffers and the H2D/D2H copies inside the timed region.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'contracted ERI quartets/s on B200: mixed-prec vs FP64 at <=1e-10 max abs err'
+WORKLOAD = ('1e6 quartets, l<=2 per shell (81 classes uniform), K in 1..6, alpha log-uniform [0.05,1e4], '
+            '30-bohr cube, spherical, seed 1')
+MIXED_THRESHOLD = 1e-4  # FP32 VRR below this Schwarz bound, FP64 above
+ERR_BAR = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--nq', type=int, default=1_000_000)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-mixed', action='store_true')
+    ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_init(n):
+    import torch
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def alg_flops(batch):
+    """Algorithmic FP64 work of one step (see DESIGN: per primitive quartet the
+    emitted VRR count plus geometry and Boys; per quartet the HRR and the
+    spherical transform), from the emitter's per-class counts."""
+    with open(os.path.join(ROOT, 'intception_b200', 'class_stats.json')) as fh:
+        stats = {s['cid']: s for s in json.load(fh)}
+    ls = batch.shell_l[batch.quartets].astype(np.int64)
+    ks = batch.shell_k[batch.quartets].astype(np.int64)
+    # canonical class id, as the device computes it
+    la, lb, lc, ld = ls.T.copy()
+    sw = la < lb
+    la[sw], lb[sw] = lb[sw], la[sw].copy()
+    sw = lc < ld
+    lc[sw], ld[sw] = ld[sw], lc[sw].copy()
+    pb = la * (la + 1) // 2 + lb
+    pk = lc * (lc + 1) // 2 + ld
+    sw = pb < pk
+    pb2 = np.where(sw, pk, pb)
+    pk2 = np.where(sw, pb, pk)
+    cid = pb2 * (pb2 + 1) // 2 + pk2
+    nprim = ks.prod(axis=1)
+    vrr = np.array([stats[c]['vrr_flops'] + 74 + 2 * stats[c]['L'] for c in range(len(stats))])
+    hrr = np.array([stats[c]['hrr_flops'] + (stats[c]['sph_flops'] if batch.spherical else 0)
+                    for c in range(len(stats))])
+    return float((nprim * vrr[cid] + hrr[cid]).sum()), cid
+
+
+def schwarz_bounds(batch, eng_cls):
+    """Per-quartet Schwarz bound sqrt(max|(ab|ab)|) * sqrt(max|(cd|cd)|), from
+    diagonal quartets evaluated on the GPU (FP64).  Returns (bounds, ms)."""
+    import torch
+    from intception_b200 import basis
+    q = batch.quartets
+    pairs = np.concatenate([q[:, [0, 1]], q[:, [2, 3]]])
+    diag = np.ascontiguousarray(np.concatenate([pairs, pairs], axis=1).astype(np.int32))
+    off, total = basis.packed_offsets(batch.shell_l, diag, batch.spherical)
+    db = basis.ShellBatch(batch.shell_l, batch.shell_k, batch.shell_ptr, batch.shell_xyz, batch.prim_exp,
+                          batch.prim_coef, diag, off, batch.spherical, total)
+    eng = eng_cls(db)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    out = eng.compute()
+    sizes = torch.as_tensor(basis.block_sizes(batch.shell_l, diag, batch.spherical), device='cuda')
+    seg = torch.repeat_interleave(torch.arange(len(diag), device='cuda'), sizes)
+    mx = torch.zeros(len(diag), dtype=torch.float64, device='cuda')
+    mx.scatter_reduce_(0, seg, out.abs(), reduce='amax')
+    qab = mx.sqrt()
+    nq = batch.nq
+    bounds = qab[:nq] * qab[nq:]
+    ev1.record()
+    torch.cuda.synchronize()
+    return bounds.contiguous(), ev0.elapsed_time(ev1)
+
+
+def cpu_reference(batch, seconds, step_index=0):
+    """Time the reference's emitted C99 (oracle/_ref) -- or, when it was not
+    built, the oracle port -- on all host cores over a bounded sample.
+    Returns (quartets/s, kind, cores, sample description)."""
+    from intception_b200 import basis
+    from oracle import loader
+    T = basis.sph_matrices(6)
+    cores = os.cpu_count() or 1
+    lib = loader.load_ref('sph' if batch.spherical else 'cart')
+    kind = 'reference' if lib is not None else 'port'
+    rng = np.random.default_rng(99 + step_index)
+
+    def run(n):
+        idx = rng.choice(batch.nq, n, replace=False)
+        sub = batch.subset(np.sort(idx))
+        t0 = time.perf_counter()
+        if lib is not None:
+            loader.ref_batch(sub, T, nthreads=cores)
+        else:
+            loader.oracle_batch(sub, T)
+        return time.perf_counter() - t0
+
+    n = 2000
+    dt = run(n)
+    n2 = int(min(batch.nq, max(n, n * seconds / max(dt, 1e-3))))
+    dt2 = run(n2)
+    used = cores if lib is not None else 1
+    return n2 / dt2, kind, used, '%d random quartets of the workload (uniform sample)' % n2
+
+
+def run_reference_arm(args, rank, world):
+    from intception_b200 import basis
+    if rank != 0:
+        return
+    batch = basis.config_mixed_l2(nq=args.nq, seed=1, spherical=True)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, kind, cores, sample = cpu_reference(batch, max(2.0, args.cpu_seconds / 3), i)
+        if i >= args.warmup:
+            vals.append(v)
+    v = float(np.median(vals))
+    line = {'metric': METRIC, 'value': v, 'unit': 'quartets/s', 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * args.nq / v, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'nq': args.nq, 'parallelism': 'openmp host cores'},
+            'impl': 'reference',
+            'cpu_baseline': {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample},
+            'e2e': {'value': v, 'unit': 'quartets/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == 'reference':
+        run_reference_arm(args, rank, world)
+        return
+    import torch
+    from intception_b200 import basis, eri
+    batch = basis.config_mixed_l2(nq=args.nq, seed=1 + rank, spherical=True)
+    eng = eri.EriEngine(batch)
+    stream = torch.cuda.current_stream()
+    out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+
+    def step(precision=eri.PREC_FP64, bounds=None):
+        eng.compute(out=out, precision=precision, bounds=bounds, threshold=MIXED_THRESHOLD)
+
+    # ---------------- FP64 path, device-resident inputs
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert eng.device_status() == 0
+    launches = eri.EriEngine.last_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms64 = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+    value64 = args.nq * world / (ms64 * 1e-3)
+    ref64 = out.clone()
+
+    # ---------------- mixed precision path
+    mixed = None
+    if not args.no_mixed:
+        bounds, schwarz_ms = schwarz_bounds(batch, eri.EriEngine)
+        for _ in range(args.warmup):
+            step(eri.PREC_MIXED, bounds)
+        torch.cuda.synchronize()
+        assert eng.device_status() == 0
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(eri.PREC_MIXED, bounds)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        msmx = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+        err = float((out - ref64).abs().max().item())
+        err = max_over_ranks(err, world)
+        frac32 = float((bounds < MIXED_THRESHOLD).double().mean().item())
+        mixed = {'value': args.nq * world / (msmx * 1e-3), 'ms_per_step': msmx, 'max_abs_err_vs_fp64': err,
+                 'fp32_fraction': frac32, 'threshold': MIXED_THRESHOLD, 'schwarz_ms': schwarz_ms}
+
+    headline_mixed = mixed is not None and mixed['max_abs_err_vs_fp64'] <= ERR_BAR
+    value = mixed['value'] if headline_mixed else value64
+    ms = mixed['ms_per_step'] if headline_mixed else ms64
+
+    # ---------------- roofline of the FP64 step against the measured FP64 FMA peak
+    flops, _ = alg_flops(batch)
+    peak64 = eri.fma_peak(True) if rank == 0 else 0.0
+    achieved = flops / (ms64 * 1e-3)
+    roofline = {'bound': 'fp64', 'achieved': achieved / 1e12, 'peak': peak64 / 1e12, 'unit': 'TFLOP/s',
+                'frac': achieved / peak64 if peak64 else None, 'traffic': None,
+                'peak_source': 'measured FP64 FMA-chain kernel (intception_b200_fma_peak), this run',
+                'kernel': 'whole FP64 step (per-class kernels run concurrently)',
+                'alg_flops_per_step': flops}
+    prof = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            roofline['traffic'] = json.load(fh).get('bytes_per_step')
+
+    # ---------------- e2e through the public API with host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        h_in = [pin(batch.shell_l), pin(batch.shell_k), pin(batch.shell_ptr), pin(batch.shell_xyz),
+                pin(batch.prim_exp), pin(batch.prim_coef), pin(batch.quartets.reshape(-1)), pin(batch.out_off)]
+        d_in = [eng.shell_l, eng.shell_k, eng.shell_ptr, eng.shell_xyz, eng.prim_exp, eng.prim_coef,
+                eng.quartets, eng.out_off]
+        h_out = torch.empty(batch.out_size, dtype=torch.float64).pin_memory()
+        h2d = sum(t.numel() * t.element_size() for t in h_in)
+        d2h = h_out.numel() * 8
+        prec = eri.PREC_MIXED if headline_mixed else eri.PREC_FP64
+        bnd = bounds if headline_mixed else None
+
+        def e2e_step():
+            for h, d in zip(h_in, d_in):
+                d.copy_(h, non_blocking=True)
+            eng.compute(out=out, precision=prec, bounds=bnd, threshold=MIXED_THRESHOLD)
+            h_out.copy_(out, non_blocking=True)
+
+        for _ in range(args.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        mse = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+        e2e = {'value': args.nq * world / (mse * 1e-3), 'unit': 'quartets/s', 'h2d_bytes_per_step': h2d,
+               'd2h_bytes_per_step': d2h, 'ms_per_step': mse}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds)
+        cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
+
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f64+f32' if headline_mixed else 'f64', 'data': 'synthetic',
+                'config': {'workload': WORKLOAD, 'nq_per_gpu': args.nq,
+                           'l2': 'inputs+outputs ~1 GB per step, larger than L2; no flush',
+                           'headline_path': 'mixed' if headline_mixed else 'fp64'},
+                'fp64': {'value': value64, 'ms_per_step': ms64},
+                'mixed': mixed,
+                'mixed_over_fp64': (mixed['value'] / value64) if mixed else None,
+                'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
+                'gpu_launches': launches * args.steps,
+                'gpu_launches_per_step': launches,
+                'clocks': clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

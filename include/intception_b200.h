@@ -1,0 +1,155 @@
+/*
+ * intception_b200.h -- C ABI of the B200 (sm_100a) ERI backend.
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-ins with the exact prototypes the reference generator emits for the
+ *    ERI input script (the class "eri" with indices a,b,c,d and auxiliary m).
+ *    A host program linked against the generated C99 links against this
+ *    library instead; pointers are HOST pointers and the call is synchronous.
+ *    The device work runs on the library's own stream on the current device.
+ *
+ * 2. Batched device entry points (device pointers, a caller stream, status
+ *    return) for millions of quartets: class sort, persistent per-class
+ *    kernels, optional mixed precision.
+ *
+ * The drop-ins return void like the reference; intception_b200_last_status()
+ * reports the outcome of the last call on the calling thread.
+ */
+#ifndef INTCEPTION_B200_H
+#define INTCEPTION_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------------------
+ * 1. Drop-in replacements
+ * ------------------------------------------------------------------------- */
+
+/* Replaces intception_integral_eri_abcd_m_cont_cart_main, emitted by the
+ * reference into intception_integral_eri_abcd_m_cont_cart.h
+ * (argument list: generator/callables/main_source_algorithms/contracted_general.py:42-68;
+ * per-index names: generator/wrappers.py:41-143).  Contracted Cartesian
+ * (ab|cd) block into output_array with the caller's strides; work_array is
+ * accepted for compatibility and not touched. */
+void intception_integral_eri_abcd_m_cont_cart_main(
+    const double *xa, const double cA[3], const int la, const int na, const int iskipa, const int na_prim,
+    const int na_cont, const int iskipa_cont, const double *contract_array_a,
+    const double *xb, const double cB[3], const int lb, const int nb, const int iskipb, const int nb_prim,
+    const int nb_cont, const int iskipb_cont, const double *contract_array_b,
+    const double *xc, const double cC[3], const int lc, const int nc, const int iskipc, const int nc_prim,
+    const int nc_cont, const int iskipc_cont, const double *contract_array_c,
+    const double *xd, const double cD[3], const int ld, const int nd, const int iskipd, const int nd_prim,
+    const int nd_cont, const int iskipd_cont, const double *contract_array_d,
+    double *work_array, double *output_array);
+
+/* Replaces intception_integral_eri_abcd_m_cont_cart_work_array_size
+ * (contracted_general.py:240-502): same integer result, so callers that size
+ * their work arrays with it keep working. */
+int intception_integral_eri_abcd_m_cont_cart_work_array_size(
+    const int la, const int lb, const int lc, const int ld, const int na_prim, const int nb_prim,
+    const int nc_prim, const int nd_prim, const int na_cont, const int nb_cont, const int nc_cont,
+    const int nd_cont);
+
+/* Replaces intception_integral_eri_abcd_m_cont_sph_main (spherical variant:
+ * generator_options(spherical_transformed=True), generator.py:102-268).  The
+ * caller's matrices sph_trans_array_?[icart + isph*ncart] are applied
+ * (generator_sph_trans_function.py:69-125). */
+void intception_integral_eri_abcd_m_cont_sph_main(
+    const double *xa, const double cA[3], const int la, const int na, const int iskipa, const int na_prim,
+    const int na_cont, const int iskipa_cont, const double *contract_array_a, const double *sph_trans_array_a,
+    const double *xb, const double cB[3], const int lb, const int nb, const int iskipb, const int nb_prim,
+    const int nb_cont, const int iskipb_cont, const double *contract_array_b, const double *sph_trans_array_b,
+    const double *xc, const double cC[3], const int lc, const int nc, const int iskipc, const int nc_prim,
+    const int nc_cont, const int iskipc_cont, const double *contract_array_c, const double *sph_trans_array_c,
+    const double *xd, const double cD[3], const int ld, const int nd, const int iskipd, const int nd_prim,
+    const int nd_cont, const int iskipd_cont, const double *contract_array_d, const double *sph_trans_array_d,
+    double *work_array, double *output_array);
+
+/* Replaces intception_integral_eri_abcd_m_cont_sph_work_array_size. */
+int intception_integral_eri_abcd_m_cont_sph_work_array_size(
+    const int la, const int lb, const int lc, const int ld, const int na_prim, const int nb_prim,
+    const int nc_prim, const int nd_prim, const int na_cont, const int nb_cont, const int nc_cont,
+    const int nd_cont);
+
+/* Replaces intception_boys from the emitted boys_function.h
+ * (generator_boys_function.py:98-205): f[m*ifskip] = F_m(x), m = nmin..nmax,
+ * evaluated by the device Boys module.  For many arguments use
+ * intception_b200_boys_batch. */
+void intception_boys(double *f, const int ifskip, const int nmin, const int nmax, const double x);
+
+/* ----------------------------------------------------------------------------
+ * Status
+ * ------------------------------------------------------------------------- */
+#define IB_OK 0
+#define IB_ERR_ARG 1       /* invalid argument (l out of range, n mismatch, null pointer) */
+#define IB_ERR_CUDA 2      /* CUDA runtime error */
+#define IB_ERR_SCRATCH 3   /* a class needed more scratch than reserved */
+#define IB_ERR_NODEVICE 4  /* no CUDA device */
+
+/* Status of the last call made on this thread (drop-ins included). */
+int intception_b200_last_status(void);
+/* Human-readable message for the last failing call on this thread. */
+const char *intception_b200_last_error(void);
+/* Highest angular momentum per shell the library accepts (6, the reference's global_user_lmax default). */
+int intception_b200_lmax(void);
+
+/* ----------------------------------------------------------------------------
+ * 2. Batched device API
+ * ------------------------------------------------------------------------- */
+
+/* Shell table in device memory (structure of arrays, segmented contraction).
+ * prim_coef holds normalised contraction coefficients, as contract_array_?. */
+typedef struct {
+  const int *shell_l;      /* [nshell] */
+  const int *shell_k;      /* [nshell] primitives per shell, 1..64 */
+  const int *shell_ptr;    /* [nshell] offset of the first primitive */
+  const double *shell_xyz; /* [3*nshell] centres */
+  const double *prim_exp;  /* [nprim] */
+  const double *prim_coef; /* [nprim] */
+  int nshell;
+  int nprim;
+  int lmax;                /* max shell_l (<= intception_b200_lmax()) */
+} intception_b200_basis;
+
+#define IB_PREC_FP64 0  /* every quartet in FP64 */
+#define IB_PREC_MIXED 1 /* FP32 VRR for quartets whose bound < threshold, FP64 otherwise */
+
+/* Contracted ERIs for nq quartets.  quartets[4*q+0..3] are shell indices
+ * (a,b,c,d); quartet q writes its block at out + out_off[q] with a fastest,
+ * index = ia + na*(ib + nb*(ic + nc*id)), na = 2l+1 (spherical, library
+ * matrices, m = -l..l) or (l+1)(l+2)/2 (Cartesian).  bounds (device, [nq],
+ * may be NULL for IB_PREC_FP64) is a per-quartet magnitude bound, e.g. a
+ * Schwarz product.  Asynchronous on stream (a cudaStream_t; NULL = the
+ * library stream). */
+int intception_b200_eri_batch(const intception_b200_basis *basis, const int *quartets, const long long *out_off,
+                              int nq, int spherical, int precision, const double *bounds, double threshold,
+                              double *out, void *stream);
+
+/* Number of library kernels the last intception_b200_eri_batch launched. */
+int intception_b200_last_launch_count(void);
+
+/* Waits for the library stream and returns the device status word of the last
+ * batch (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
+int intception_b200_batch_status(void);
+
+/* The library's Cartesian->spherical matrix for l (host memory,
+ * T[icart + isph*ncart], ncart x (2l+1)). */
+int intception_b200_sph_matrix(int l, double *T);
+
+/* F_m(x[i]) for m = 0..nmax into f[i*(nmax+1) + m]; device pointers. */
+int intception_b200_boys_batch(const double *x, int n, int nmax, double *f, void *stream);
+
+/* Block until the library stream is idle. */
+int intception_b200_synchronize(void);
+
+/* Diagnostics: FP64 (fp64 != 0) or FP32 FMA throughput of the current device
+ * in FLOP/s, from a kernel of independent FMA chains (iters x 128 FMAs per
+ * thread); the roofline denominator of the ERI kernels. */
+int intception_b200_fma_peak(int fp64, int iters, double *flops_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INTCEPTION_B200_H */

@@ -1,0 +1,287 @@
+// eri_generic.cu -- one thread block per contracted quartet, any l <= IB_LMAX.
+//
+// Used for the classes that have no unrolled kernel (some l > the emitted
+// maximum).  Same schedule as the emitted kernels (HGP: bra VRR, ket VRR with
+// the electron-transfer term, contraction, bra HRR, ket HRR, spherical
+// transform), but every stage is a loop over the elements of one recurrence
+// level, spread over the block's threads, with the levels in global scratch
+// (one slice per resident block).  FP64 throughout.
+//
+// Scratch slice layout (doubles), sizes from ib_generic_dims():
+//   acc  [ne * nf]                 contracted [e0|f0], e in [la,la+lb], f in [lc,lc+ld]
+//   bra  [(L+1) * ncumE]           [e0|00]^(m) over every e <= la+lb
+//   ket  sum_f (F-f+1)*ncart(f)*ncumE   [e0|f0]^(m) for each ket level f >= 1
+//   h0,h1 [hmax] ping-pong buffers for HRR and the spherical transform
+#include "ib_eri_device.cuh"
+#include "ib_generic.cuh"
+
+namespace {
+
+__device__ __forceinline__ void ib_comp_of(int cum, int& x, int& y, int& z) {
+  // level l with ncum(l-1) <= cum < ncum(l), then the in-level index k
+  int l = 0;
+  while (ib_ncum(l) <= cum) ++l;
+  int k = cum - ib_ncum(l - 1);
+  // k = mz + (my+mz)(my+mz+1)/2 ; s = my + mz
+  int s = 0;
+  while ((s + 1) * (s + 2) / 2 <= k) ++s;
+  z = k - s * (s + 1) / 2;
+  y = s - z;
+  x = l - s;
+}
+
+struct IbGenShared {
+  IbGenericDims d;
+  double A[3], B[3], C[3], D[3], AB[3], CD[3];
+  double PA[3], WP[3], QC[3], WQ[3];
+  double o2z, roz, o2e, roe, o2zpe;
+  double F[4 * IB_LMAX + 1];
+  int k[4], ptr[4], st[4];
+  long long off;
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
+                                                               double* __restrict__ scratch, long long slice) {
+  __shared__ IbGenShared sh;
+  const int beg = a.ranges[range_slot], end = a.ranges[range_slot + 1];
+  double* __restrict__ w = scratch + (size_t)blockIdx.x * (size_t)slice;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int p = beg + blockIdx.x; p < end; p += gridDim.x) {
+    if (tid == 0) {
+      const IbItem it = a.items[p];
+      int l[4];
+      for (int i = 0; i < 4; ++i) {
+        const int s = it.s[i];
+        l[i] = a.shell_l[s];
+        sh.k[i] = a.shell_k[s];
+        sh.ptr[i] = a.shell_ptr[s];
+        sh.st[i] = it.st[i];
+        double* R = i == 0 ? sh.A : (i == 1 ? sh.B : (i == 2 ? sh.C : sh.D));
+        for (int c = 0; c < 3; ++c) R[c] = a.shell_xyz[3 * s + c];
+      }
+      sh.off = it.off;
+      for (int c = 0; c < 3; ++c) {
+        sh.AB[c] = sh.A[c] - sh.B[c];
+        sh.CD[c] = sh.C[c] - sh.D[c];
+      }
+      sh.d = ib_generic_dims(l[0], l[1], l[2], l[3]);
+    }
+    __syncthreads();
+    const IbGenericDims d = sh.d;
+    if ((long long)d.total > slice) {
+      if (tid == 0) atomicExch(a.status, 3);  // scratch slice too small for this class
+      __syncthreads();
+      continue;
+    }
+    double* acc = w + d.o_acc;
+    double* bra = w + d.o_bra;
+    double* ket = w + d.o_ket;
+    for (int i = tid; i < d.ne * d.nf; i += nt) acc[i] = 0.0;
+    const double RAB2 = sh.AB[0] * sh.AB[0] + sh.AB[1] * sh.AB[1] + sh.AB[2] * sh.AB[2];
+    const double RCD2 = sh.CD[0] * sh.CD[0] + sh.CD[1] * sh.CD[1] + sh.CD[2] * sh.CD[2];
+    const int nprim = sh.k[0] * sh.k[1] * sh.k[2] * sh.k[3];
+    for (int pq = 0; pq < nprim; ++pq) {
+      __syncthreads();
+      if (tid == 0) {
+        int r = pq;
+        const int id = r % sh.k[3]; r /= sh.k[3];
+        const int ic = r % sh.k[2]; r /= sh.k[2];
+        const int ib = r % sh.k[1]; r /= sh.k[1];
+        const int ia = r;
+        const double xa = a.prim_exp[sh.ptr[0] + ia], ca = a.prim_coef[sh.ptr[0] + ia];
+        const double xb = a.prim_exp[sh.ptr[1] + ib], cb = a.prim_coef[sh.ptr[1] + ib];
+        const double xc = a.prim_exp[sh.ptr[2] + ic], cc = a.prim_coef[sh.ptr[2] + ic];
+        const double xd = a.prim_exp[sh.ptr[3] + id], cd = a.prim_coef[sh.ptr[3] + id];
+        const double zeta = xa + xb, oz = 1.0 / zeta, eta = xc + xd, oe = 1.0 / eta;
+        const double ozpe = 1.0 / (zeta + eta), rho = zeta * eta * ozpe;
+        double P[3], Q[3], PQ[3];
+        for (int c = 0; c < 3; ++c) {
+          P[c] = (xa * sh.A[c] + xb * sh.B[c]) * oz;
+          Q[c] = (xc * sh.C[c] + xd * sh.D[c]) * oe;
+          PQ[c] = P[c] - Q[c];
+          const double W = (zeta * P[c] + eta * Q[c]) * ozpe;
+          sh.PA[c] = P[c] - sh.A[c];
+          sh.WP[c] = W - P[c];
+          sh.QC[c] = Q[c] - sh.C[c];
+          sh.WQ[c] = W - Q[c];
+        }
+        sh.o2z = 0.5 * oz;
+        sh.roz = rho * oz;
+        sh.o2e = 0.5 * oe;
+        sh.roe = rho * oe;
+        sh.o2zpe = 0.5 * ozpe;
+        const double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+        ib_boys_rt(rho * RPQ2, d.L, a.boys_tab, sh.F);
+        const double pref = ib_two_pi52() * oz * oe * sqrt(ozpe) * ca * cb * cc * cd *
+                            exp(-xa * xb * oz * RAB2 - xc * xd * oe * RCD2);
+        for (int m = 0; m <= d.L; ++m) sh.F[m] *= pref;
+      }
+      __syncthreads();
+      // ---- bra VRR, level by level: bra[m*ncumE + e]
+      for (int m = tid; m <= d.L; m += nt) {
+        bra[m * d.ncumE] = sh.F[m];
+        if (m == 0 && d.lc == 0 && d.la == 0) acc[0] += sh.F[0];
+      }
+      for (int le = 1; le <= d.E; ++le) {
+        __syncthreads();
+        const int nce = ib_ncart(le), nm = d.L - le + 1;
+        for (int idx = tid; idx < nce * nm; idx += nt) {
+          const int m = idx / nce, e = ib_ncum(le - 1) + idx % nce;
+          int ex, ey, ez;
+          ib_comp_of(e, ex, ey, ez);
+          int ev[3] = {ex, ey, ez};
+          const int i = ev[0] > 0 ? 0 : (ev[1] > 0 ? 1 : 2);
+          ev[i] -= 1;
+          const int e1 = ib_cidx(ev[0], ev[1], ev[2]);
+          double v = sh.PA[i] * bra[m * d.ncumE + e1] + sh.WP[i] * bra[(m + 1) * d.ncumE + e1];
+          if (ev[i] > 0) {
+            const int n = ev[i];
+            ev[i] -= 1;
+            const int e2 = ib_cidx(ev[0], ev[1], ev[2]);
+            v += n * sh.o2z * (bra[m * d.ncumE + e2] - sh.roz * bra[(m + 1) * d.ncumE + e2]);
+          }
+          bra[m * d.ncumE + e] = v;
+          if (m == 0 && d.lc == 0 && e >= d.e0) acc[(e - d.e0) * d.nf] += v;
+        }
+      }
+      // ---- ket VRR: level f stored at ket + koff(f) as [m][fcomp][e]
+      for (int lf = 1; lf <= d.F; ++lf) {
+        __syncthreads();
+        const int ncf = ib_ncart(lf), nm = d.F - lf + 1;
+        const long long n = (long long)nm * ncf * d.ncumE;
+        double* dst = ket + ib_koff(d, lf);
+        for (long long idx = tid; idx < n; idx += nt) {
+          const int e = (int)(idx % d.ncumE);
+          const int rest = (int)(idx / d.ncumE);
+          const int fc = rest % ncf, m = rest / ncf;
+          int fx, fy, fz;
+          ib_comp_of(ib_ncum(lf - 1) + fc, fx, fy, fz);
+          int fv[3] = {fx, fy, fz};
+          const int i = fv[0] > 0 ? 0 : (fv[1] > 0 ? 1 : 2);
+          fv[i] -= 1;
+          const int f1 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 2);  // in-level index at lf-1
+          // level lf-1 accessor
+          const double* s1 = lf == 1 ? bra : ket + ib_koff(d, lf - 1);
+          const int nc1 = ib_ncart(lf - 1);
+          double v = sh.QC[i] * s1[((size_t)m * nc1 + f1) * d.ncumE + e] +
+                     sh.WQ[i] * s1[((size_t)(m + 1) * nc1 + f1) * d.ncumE + e];
+          if (fv[i] > 0) {
+            const int nn = fv[i];
+            fv[i] -= 1;
+            const int f2 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 3);
+            fv[i] += 1;
+            const double* s2 = lf == 2 ? bra : ket + ib_koff(d, lf - 2);
+            const int nc2 = ib_ncart(lf - 2);
+            v += nn * sh.o2e *
+                 (s2[((size_t)m * nc2 + f2) * d.ncumE + e] - sh.roe * s2[((size_t)(m + 1) * nc2 + f2) * d.ncumE + e]);
+          }
+          int ex, ey, ez;
+          ib_comp_of(e, ex, ey, ez);
+          int ev[3] = {ex, ey, ez};
+          if (ev[i] > 0) {
+            const int ne_i = ev[i];
+            ev[i] -= 1;
+            const int e1 = ib_cidx(ev[0], ev[1], ev[2]);
+            v += ne_i * sh.o2zpe * s1[((size_t)(m + 1) * nc1 + f1) * d.ncumE + e1];
+          }
+          dst[((size_t)m * ncf + fc) * d.ncumE + e] = v;
+          if (m == 0 && lf >= d.lc && e >= d.e0)
+            acc[(e - d.e0) * d.nf + (ib_ncum(lf - 1) + fc - d.f0)] += v;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- bra HRR: [e][b][f] layers, (a, b+1i) = (a+1i, b) + AB_i (a, b)
+    double* src = acc;
+    double* h0 = w + d.o_h0;
+    double* h1 = w + d.o_h1;
+    for (int j = 1; j <= d.lb; ++j) {
+      double* dst = (j & 1) ? h0 : h1;
+      const int ne_j = ib_ncum(d.E - j) - d.e0, ne_p = ib_ncum(d.E - j + 1) - d.e0;
+      const int ncb = ib_ncart(j), ncp = ib_ncart(j - 1);
+      (void)ne_p;
+      const int n = ne_j * ncb * d.nf;
+      for (int idx = tid; idx < n; idx += nt) {
+        const int f = idx % d.nf, rest = idx / d.nf;
+        const int b = rest % ncb, e = rest / ncb;
+        int bx, by, bz;
+        ib_comp_of(ib_ncum(j - 1) + b, bx, by, bz);
+        int bv[3] = {bx, by, bz};
+        const int i = bv[0] > 0 ? 0 : (bv[1] > 0 ? 1 : 2);
+        bv[i] -= 1;
+        const int bm = ib_cidx(bv[0], bv[1], bv[2]) - ib_ncum(j - 2);
+        int ex, ey, ez;
+        ib_comp_of(d.e0 + e, ex, ey, ez);
+        int ev[3] = {ex, ey, ez};
+        ev[i] += 1;
+        const int ep = ib_cidx(ev[0], ev[1], ev[2]) - d.e0;
+        dst[idx] = src[((size_t)ep * ncp + bm) * d.nf + f] + sh.AB[i] * src[((size_t)e * ncp + bm) * d.nf + f];
+      }
+      __syncthreads();
+      src = dst;
+    }
+    // src: [a][b][f] = [ab][f], nab = ncart(la)*ncart(lb)
+    const int nab = ib_ncart(d.la) * ib_ncart(d.lb);
+    for (int j = 1; j <= d.ld; ++j) {
+      double* dst = (src == h0) ? h1 : h0;
+      const int nc_j = ib_ncum(d.F - j) - d.f0, nc_p = ib_ncum(d.F - j + 1) - d.f0;
+      const int ndj = ib_ncart(j), ndp = ib_ncart(j - 1);
+      const int n = nab * nc_j * ndj;
+      for (int idx = tid; idx < n; idx += nt) {
+        const int dd = idx % ndj, rest = idx / ndj;
+        const int c = rest % nc_j, ab = rest / nc_j;
+        int dx, dy, dz;
+        ib_comp_of(ib_ncum(j - 1) + dd, dx, dy, dz);
+        int dv[3] = {dx, dy, dz};
+        const int i = dv[0] > 0 ? 0 : (dv[1] > 0 ? 1 : 2);
+        dv[i] -= 1;
+        const int dm = ib_cidx(dv[0], dv[1], dv[2]) - ib_ncum(j - 2);
+        int cx, cy, cz;
+        ib_comp_of(d.f0 + c, cx, cy, cz);
+        int cv[3] = {cx, cy, cz};
+        cv[i] += 1;
+        const int cp = ib_cidx(cv[0], cv[1], cv[2]) - d.f0;
+        dst[idx] = src[((size_t)ab * nc_p + cp) * ndp + dm] + sh.CD[i] * src[((size_t)ab * nc_p + c) * ndp + dm];
+      }
+      __syncthreads();
+      src = dst;
+    }
+    // src: [a][b][c][d] Cartesian block
+    int dims[4] = {ib_ncart(d.la), ib_ncart(d.lb), ib_ncart(d.lc), ib_ncart(d.ld)};
+    const int ls[4] = {d.la, d.lb, d.lc, d.ld};
+    if (sph) {
+      for (int axis = 3; axis >= 0; --axis) {
+        double* dst = (src == h0) ? h1 : h0;
+        const int l = ls[axis], ncs = ib_ncart(l), ns = 2 * l + 1;
+        const double* T = a.sph + ib_sph_offset(l);
+        int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+        nd[axis] = ns;
+        const int n = nd[0] * nd[1] * nd[2] * nd[3];
+        int inner = 1;
+        for (int k = axis + 1; k < 4; ++k) inner *= dims[k];
+        for (int idx = tid; idx < n; idx += nt) {
+          const int in = idx % inner, rest = idx / inner;
+          const int s = rest % ns, outer = rest / ns;
+          double v = 0.0;
+          for (int c = 0; c < ncs; ++c) v += T[c + s * ncs] * src[((size_t)outer * ncs + c) * inner + in];
+          dst[idx] = v;
+        }
+        __syncthreads();
+        dims[axis] = ns;
+        src = dst;
+      }
+    }
+    double* o = a.out + sh.off;
+    const int n = dims[0] * dims[1] * dims[2] * dims[3];
+    for (int idx = tid; idx < n; idx += nt) {
+      const int i3 = idx % dims[3], r3 = idx / dims[3];
+      const int i2 = r3 % dims[2], r2 = r3 / dims[2];
+      const int i1 = r2 % dims[1], i0 = r2 / dims[1];
+      o[(long long)i0 * sh.st[0] + (long long)i1 * sh.st[1] + (long long)i2 * sh.st[2] + (long long)i3 * sh.st[3]] =
+          src[idx];
+    }
+    __syncthreads();
+  }
+}

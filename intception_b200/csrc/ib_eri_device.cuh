@@ -1,0 +1,211 @@
+// ib_eri_device.cuh -- device-side building blocks shared by every ERI kernel.
+//
+// Data model (HBM, structure of arrays):
+//   shell_l/k/ptr [nshell] int32, shell_xyz [3*nshell] f64,
+//   prim_exp/prim_coef [nprim] f64 (coefficients already normalised, as the
+//   reference's contract_array_?; contracted_general.py:42-68),
+//   items [n] IbItem: the four shells of one quartet after canonical permutation
+//   and the output strides that undo it.
+// Boys: F_L(T) by 7-term Taylor about the nearest point of a 1/16 grid (the
+// seven columns L..L+6, divided by k!, staged in shared memory per block),
+// downward recursion to F_0; T >= 36 uses the asymptotic F_0 and upward
+// recursion (the scheme of generator_boys_function.py:98-205 on a finer grid).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "_gen/boys_table.h"
+
+#ifndef IB_BLOCK
+#define IB_BLOCK 128
+#endif
+
+#define IB_LMAX 6
+#define IB_NPAIR ((IB_LMAX + 1) * (IB_LMAX + 2) / 2)
+#define IB_NCLASS (IB_NPAIR * (IB_NPAIR + 1) / 2)
+#define IB_BOYS_TAYLOR 7
+
+struct IbItem {
+  int s[4];         // shells (a, b, c, d) in canonical order
+  int st[4];        // output strides of the canonical indices
+  long long off;    // block offset into the output
+};
+
+struct IbLaunch {
+  const IbItem* items;
+  const int* ranges;  // [2*IB_NCLASS] begin/end of each class id in items
+  const int* shell_l;
+  const int* shell_k;
+  const int* shell_ptr;
+  const double* shell_xyz;
+  const double* prim_exp;
+  const double* prim_coef;
+  const double* boys_tab;  // [IB_BOYS_NPTS * IB_BOYS_NCOL]
+  const double* sph;       // library Cartesian->spherical matrices, packed per l
+  double* out;
+  int* status;             // device error word (0 = ok)
+};
+
+typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch& a);
+typedef int (*IbOccFn)(int variant);
+struct IbClassEntry {
+  int cid;
+  IbLaunchFn launch;
+  IbOccFn occupancy;
+};
+
+__host__ __device__ inline constexpr double ib_two_pi52() { return 34.98683665524972497; }  // 2 pi^(5/2)
+
+__host__ inline size_t ib_boys_smem_bytes() {
+  return sizeof(double) * IB_BOYS_NPTS * IB_BOYS_TAYLOR;
+}
+
+// Stage the Taylor coefficients g_k = F_{L+k}(T_i)/k! for k = 0..6 of every grid point.
+__device__ __forceinline__ void ib_stage_boys(double* __restrict__ s, const double* __restrict__ tab, int L) {
+  const double invfact[IB_BOYS_TAYLOR] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
+  for (int idx = threadIdx.x; idx < IB_BOYS_NPTS * IB_BOYS_TAYLOR; idx += blockDim.x) {
+    const int i = idx / IB_BOYS_TAYLOR, k = idx - i * IB_BOYS_TAYLOR;
+    s[idx] = __ldg(tab + i * IB_BOYS_NCOL + L + k) * invfact[k];
+  }
+}
+
+// F_m(T), m = 0..L, into F[] (compile-time L so the recursion unrolls).
+template <int L>
+__device__ __forceinline__ void ib_boys(double T, const double* __restrict__ s, double* F) {
+  if (T < IB_BOYS_TMAX) {
+    const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
+    const double dx = (double)i * (1.0 / IB_BOYS_H_INV) - T;
+    const double* r = s + i * IB_BOYS_TAYLOR;
+    double f = r[6];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) f = fma(f, dx, r[k]);
+    F[L] = f;
+    if (L > 0) {
+      const double e = exp(-T), t2 = T + T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    const double oT = 1.0 / T;
+    F[0] = sqrt(0.78539816339744830962 * oT);  // (1/2) sqrt(pi/T)
+    if (L > 0) {
+      const double he = 0.5 * exp(-T);
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = fma((double)m + 0.5, F[m], -he) * oT;
+    }
+  }
+}
+
+// Runtime-L variant reading the global table directly (one thread, no staging).
+__device__ inline void ib_boys_rt(double T, int L, const double* __restrict__ tab, double* F) {
+  if (T < IB_BOYS_TMAX) {
+    const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
+    const double dx = (double)i * (1.0 / IB_BOYS_H_INV) - T;
+    const double* r = tab + i * IB_BOYS_NCOL + L;
+    const double invfact[IB_BOYS_TAYLOR] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
+    double f = r[6] * invfact[6];
+    for (int k = 5; k >= 0; --k) f = fma(f, dx, r[k] * invfact[k]);
+    F[L] = f;
+    const double e = exp(-T), t2 = T + T;
+    for (int m = L - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) / (double)(2 * m + 1);
+  } else {
+    const double oT = 1.0 / T;
+    F[0] = sqrt(0.78539816339744830962 * oT);
+    const double he = 0.5 * exp(-T);
+    for (int m = 0; m < L; ++m) F[m + 1] = fma((double)m + 0.5, F[m], -he) * oT;
+  }
+}
+
+struct IbQuartet {
+  double A[3], B[3], C[3], D[3];
+  double AB[3], CD[3];
+  double RAB2, RCD2;
+  int k[4], ptr[4], st[4];
+  long long off;
+};
+
+__device__ __forceinline__ void ib_load_quartet(const IbLaunch& a, int p, IbQuartet& g) {
+  const IbItem it = a.items[p];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int s = it.s[i];
+    g.k[i] = __ldg(a.shell_k + s);
+    g.ptr[i] = __ldg(a.shell_ptr + s);
+    g.st[i] = it.st[i];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    g.A[d] = __ldg(a.shell_xyz + 3 * it.s[0] + d);
+    g.B[d] = __ldg(a.shell_xyz + 3 * it.s[1] + d);
+    g.C[d] = __ldg(a.shell_xyz + 3 * it.s[2] + d);
+    g.D[d] = __ldg(a.shell_xyz + 3 * it.s[3] + d);
+  }
+  g.off = it.off;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    g.AB[d] = g.A[d] - g.B[d];
+    g.CD[d] = g.C[d] - g.D[d];
+  }
+  g.RAB2 = g.AB[0] * g.AB[0] + g.AB[1] * g.AB[1] + g.AB[2] * g.AB[2];
+  g.RCD2 = g.CD[0] * g.CD[0] + g.CD[1] * g.CD[1] + g.CD[2] * g.CD[2];
+}
+
+struct IbBraPair {
+  double zeta, oz, K;
+  double P[3], PA[3];
+};
+
+__device__ __forceinline__ void ib_bra_pair(const IbLaunch& a, const IbQuartet& g, int ia, int ib, IbBraPair& bp) {
+  const double xa = __ldg(a.prim_exp + g.ptr[0] + ia), ca = __ldg(a.prim_coef + g.ptr[0] + ia);
+  const double xb = __ldg(a.prim_exp + g.ptr[1] + ib), cb = __ldg(a.prim_coef + g.ptr[1] + ib);
+  bp.zeta = xa + xb;
+  bp.oz = 1.0 / bp.zeta;
+  bp.K = ca * cb * exp(-xa * xb * bp.oz * g.RAB2);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    bp.P[d] = (xa * g.A[d] + xb * g.B[d]) * bp.oz;
+    bp.PA[d] = bp.P[d] - g.A[d];
+  }
+}
+
+template <typename R>
+struct IbPrimQuartet {
+  R PA[3], WP[3], QC[3], WQ[3];
+  R o2z, roz, o2e, roe, o2zpe;
+};
+
+// Ket pair, quartet geometry and the scaled Boys values F[m] = pref * F_m(T).
+template <typename R, int L>
+__device__ __forceinline__ void ib_prim_quartet(const IbLaunch& a, const IbQuartet& g, const IbBraPair& bp, int ic,
+                                                int id, const double* __restrict__ boys_s, double* F,
+                                                IbPrimQuartet<R>& pq) {
+  const double xc = __ldg(a.prim_exp + g.ptr[2] + ic), cc = __ldg(a.prim_coef + g.ptr[2] + ic);
+  const double xd = __ldg(a.prim_exp + g.ptr[3] + id), cd = __ldg(a.prim_coef + g.ptr[3] + id);
+  const double eta = xc + xd, oe = 1.0 / eta;
+  const double Kcd = cc * cd * exp(-xc * xd * oe * g.RCD2);
+  const double ozpe = 1.0 / (bp.zeta + eta);
+  const double rho = bp.zeta * eta * ozpe;
+  double Q[3], PQ[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    Q[d] = (xc * g.C[d] + xd * g.D[d]) * oe;
+    PQ[d] = bp.P[d] - Q[d];
+  }
+  const double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+  ib_boys<L>(rho * RPQ2, boys_s, F);
+  const double pref = ib_two_pi52() * bp.oz * oe * sqrt(ozpe) * bp.K * Kcd;
+#pragma unroll
+  for (int m = 0; m <= L; ++m) F[m] *= pref;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double W = (bp.zeta * bp.P[d] + eta * Q[d]) * ozpe;
+    pq.PA[d] = (R)bp.PA[d];
+    pq.WP[d] = (R)(W - bp.P[d]);
+    pq.QC[d] = (R)(Q[d] - g.C[d]);
+    pq.WQ[d] = (R)(W - Q[d]);
+  }
+  pq.o2z = (R)(0.5 * bp.oz);
+  pq.roz = (R)(rho * bp.oz);
+  pq.o2e = (R)(0.5 * oe);
+  pq.roe = (R)(rho * oe);
+  pq.o2zpe = (R)(0.5 * ozpe);
+}

@@ -1,0 +1,842 @@
+// ib_runtime.cu -- host runtime and C ABI of the B200 ERI backend.
+//
+// Batch pipeline (all on the device, stream-ordered, no host round trip):
+//   1. ib_classify   : per quartet, canonical class id (la>=lb, lc>=ld,
+//                      bra pair >= ket pair), precision bit, primitive-pair
+//                      counts -> 22-bit sort key
+//   2. CUB radix sort: quartets grouped by (precision, class, Kab, Kcd) so a warp
+//                      sees one class and one loop shape
+//   3. ib_build_items: permuted shells + output strides per sorted quartet, and
+//                      the [begin,end) range of every (precision, class)
+//   4. per-class persistent kernels (unrolled, emitted) fanned out over side
+//      streams, plus the generic block-per-quartet kernel for the rest.
+// The drop-ins build the same items on the host for one quartet (all
+// contraction combinations) and reuse the class kernels.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/intception_b200.h"
+#include "_gen/boys_table_data.h"
+#include "ib_eri_device.cuh"
+#include "ib_generic.cuh"
+
+void ib_register_emitted_classes(IbClassEntry* table);
+// Real solid harmonics in the library convention (m = -l..l, each scaled to the
+// norm of x^l); computed once on the host and kept on the device.
+void build_sph_host(std::vector<double>& out);
+extern const int ib_n_emitted_classes;
+extern const int ib_lmax_emitted;
+__global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double* scratch, long long slice);
+
+namespace {
+
+constexpr int kNSide = 4;                       // side streams for concurrent class kernels
+constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 copies
+constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
+constexpr int kNRanges = 4 * IB_NCLASS + 2;
+constexpr int kKeyBits = 22;
+constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
+
+thread_local int tl_status = IB_OK;
+thread_local std::string tl_msg;
+thread_local int tl_launches = 0;
+
+int set_status(int st, const std::string& msg) {
+  tl_status = st;
+  tl_msg = msg;
+  return st;
+}
+
+#define IB_CUDA(call)                                                                             \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return set_status(IB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+
+int ncart_h(int l) { return (l + 1) * (l + 2) / 2; }
+int pair_index_h(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(bytes, cap + cap / 2);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(bytes, size_t(1) << 16);
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+};
+
+struct Context {
+  int device = -1;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t side[kNSide] = {};
+  cudaEvent_t fork = nullptr, join[kNSide] = {};
+  DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
+  DevBuf d_stage, d_cart, d_res;
+  HostBuf h_stage, h_res;
+  IbClassEntry table[IB_NCLASS] = {};
+  int occ[IB_NCLASS][4] = {};
+  std::mutex mu;
+};
+
+Context* g_ctx[64] = {};
+std::mutex g_ctx_mu;
+
+// ---------------------------------------------------------------- kernels
+
+__device__ __forceinline__ int ib_ncart_d(int l) { return (l + 1) * (l + 2) / 2; }
+__device__ __forceinline__ int ib_pair_d(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+// canonical order: (a,b) with la>=lb, (c,d) with lc>=ld, bra pair index >= ket pair index
+__device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
+  if (l[0] < l[1]) {
+    int t = s[0]; s[0] = s[1]; s[1] = t;
+    t = l[0]; l[0] = l[1]; l[1] = t;
+    t = st[0]; st[0] = st[1]; st[1] = t;
+  }
+  if (l[2] < l[3]) {
+    int t = s[2]; s[2] = s[3]; s[3] = t;
+    t = l[2]; l[2] = l[3]; l[3] = t;
+    t = st[2]; st[2] = st[3]; st[3] = t;
+  }
+  if (ib_pair_d(l[0], l[1]) < ib_pair_d(l[2], l[3])) {
+    for (int k = 0; k < 2; ++k) {
+      int t = s[k]; s[k] = s[k + 2]; s[k + 2] = t;
+      t = l[k]; l[k] = l[k + 2]; l[k + 2] = t;
+      t = st[k]; st[k] = st[k + 2]; st[k + 2] = t;
+    }
+  }
+}
+
+__global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
+                            const int* __restrict__ shell_k, int nq, int lmax, const double* __restrict__ bounds,
+                            double thr, int mixed, int n_emit, unsigned* __restrict__ keys, int* __restrict__ vals,
+                            int* status) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    int s[4], l[4], st[4] = {0, 0, 0, 0};
+    bool bad = false;
+    for (int i = 0; i < 4; ++i) {
+      s[i] = quartets[4 * q + i];
+      l[i] = shell_l[s[i]];
+      bad |= (l[i] < 0) | (l[i] > lmax) | (l[i] > IB_LMAX);
+    }
+    if (bad) {
+      atomicExch(status, IB_ERR_ARG);
+      for (int i = 0; i < 4; ++i) l[i] = 0;
+    }
+    ib_canon(s, l, st);
+    const int pb = ib_pair_d(l[0], l[1]), pk = ib_pair_d(l[2], l[3]);
+    const int cid = pb * (pb + 1) / 2 + pk;
+    const int kab = min(shell_k[s[0]] * shell_k[s[1]], 63), kcd = min(shell_k[s[2]] * shell_k[s[3]], 63);
+    const int fp32 = (mixed && cid < n_emit && bounds[q] < thr) ? 1 : 0;
+    keys[q] = (unsigned(fp32) << 21) | (unsigned(cid) << 12) | (unsigned(kab) << 6) | unsigned(kcd);
+    vals[q] = q;
+  }
+}
+
+__global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __restrict__ order, int nq,
+                               const int* __restrict__ quartets, const int* __restrict__ shell_l,
+                               const long long* __restrict__ out_off, int spherical, int n_emit,
+                               IbItem* __restrict__ items, int* __restrict__ ranges) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
+    const int q = order[p];
+    int s[4], l[4], n[4];
+    for (int i = 0; i < 4; ++i) {
+      s[i] = quartets[4 * q + i];
+      l[i] = min(max(shell_l[s[i]], 0), IB_LMAX);
+      n[i] = spherical ? 2 * l[i] + 1 : ib_ncart_d(l[i]);
+    }
+    int st[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
+    ib_canon(s, l, st);
+    IbItem it;
+    for (int i = 0; i < 4; ++i) {
+      it.s[i] = s[i];
+      it.st[i] = st[i];
+    }
+    it.off = out_off[q];
+    items[p] = it;
+    const unsigned key = keys[p];
+    const int slot = (int)(key >> 12);  // fp32 bit * 512 + cid
+    const int cid = slot & 511, fp32 = slot >> 9;
+    const int rs = 2 * (cid + fp32 * IB_NCLASS);
+    const int prev = p > 0 ? (int)(keys[p - 1] >> 12) : -1;
+    const int next = p + 1 < nq ? (int)(keys[p + 1] >> 12) : -1;
+    if (prev != slot) ranges[rs] = p;
+    if (next != slot) ranges[rs + 1] = p + 1;
+    const bool gen = (fp32 == 0 && cid >= n_emit);
+    const bool gprev = p > 0 && ((prev >> 9) == 0) && ((prev & 511) >= n_emit);
+    const bool gnext = p + 1 < nq && ((next >> 9) == 0) && ((next & 511) >= n_emit);
+    if (gen && !gprev) ranges[kSlotGeneric] = p;
+    if (gen && !gnext) ranges[kSlotGeneric + 1] = p + 1;
+  }
+}
+
+// Apply 4 spherical (or truncating) transforms index by index and emit the
+// caller-ordered compact block: res[blk][ia + na*(ib + nb*(ic + nc*id))].
+// One block per contraction combination; T[i] == nullptr keeps the first n[i]
+// Cartesian components.
+struct IbXform {
+  const double* T[4];
+  int l[4], n[4];
+  int nblk, cart_block, res_block;
+};
+
+__global__ void ib_transform_blocks(const IbXform x, const double* __restrict__ cart, double* __restrict__ res,
+                                    double* __restrict__ tmp) {
+  const int blk = blockIdx.x;
+  if (blk >= x.nblk) return;
+  int dims[4];
+  for (int i = 0; i < 4; ++i) dims[i] = ib_ncart_d(x.l[i]);
+  const double* src = cart + (size_t)blk * x.cart_block;
+  double* bufs[2] = {tmp + (size_t)blk * 2 * x.cart_block, tmp + (size_t)blk * 2 * x.cart_block + x.cart_block};
+  int which = 0;
+  // layout of src: a fastest (index ia + na*(ib + nb*(ic + nc*id)))
+  for (int axis = 0; axis < 4; ++axis) {
+    const int nin = dims[axis], nout = x.n[axis];
+    int inner = 1, outer = 1;
+    for (int k = 0; k < axis; ++k) inner *= dims[k];
+    for (int k = axis + 1; k < 4; ++k) outer *= dims[k];
+    double* dst = (axis == 3) ? res + (size_t)blk * x.res_block : bufs[which];
+    const int total = inner * nout * outer;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const int in = idx % inner, rest = idx / inner;
+      const int s = rest % nout, o = rest / nout;
+      double v;
+      if (x.T[axis]) {
+        v = 0.0;
+        for (int c = 0; c < nin; ++c) v += x.T[axis][c + s * nin] * src[((size_t)o * nin + c) * inner + in];
+      } else {
+        v = src[((size_t)o * nin + s) * inner + in];
+      }
+      dst[idx] = v;
+    }
+    __syncthreads();
+    dims[axis] = nout;
+    src = dst;
+    which ^= 1;
+  }
+}
+
+__global__ void ib_boys_kernel(const double* __restrict__ x, int n, int nmax, const double* __restrict__ tab,
+                               double* __restrict__ f) {
+  double F[4 * IB_LMAX + 8];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    ib_boys_rt(x[i], nmax, tab, F);
+    for (int m = 0; m <= nmax; ++m) f[(size_t)i * (nmax + 1) + m] = F[m];
+  }
+}
+
+// ---------------------------------------------------------------- context
+
+int packed_sph_size() {
+  int n = 0;
+  for (int l = 0; l <= IB_LMAX; ++l) n += ncart_h(l) * (2 * l + 1);
+  return n;
+}
+
+int get_context(Context** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_status(IB_ERR_NODEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_status(IB_ERR_NODEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (!g_ctx[dev]) {
+    Context* c = new Context();
+    c->device = dev;
+    IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
+    IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < kNSide; ++i) {
+      IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
+      IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
+    }
+    IB_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    IB_CUDA(c->boys_tab.ensure(sizeof(ib_boys_host_table)));
+    IB_CUDA(cudaMemcpy(c->boys_tab.p, ib_boys_host_table, sizeof(ib_boys_host_table), cudaMemcpyHostToDevice));
+    std::vector<double> sph;
+    build_sph_host(sph);
+    IB_CUDA(c->sph.ensure(sph.size() * sizeof(double)));
+    IB_CUDA(cudaMemcpy(c->sph.p, sph.data(), sph.size() * sizeof(double), cudaMemcpyHostToDevice));
+    IB_CUDA(c->ranges.ensure(kNRanges * sizeof(int)));
+    IB_CUDA(c->status.ensure(sizeof(int)));
+    IB_CUDA(cudaMemset(c->status.p, 0, sizeof(int)));
+    ib_register_emitted_classes(c->table);
+    for (int cid = 0; cid < ib_n_emitted_classes; ++cid)
+      for (int v = 0; v < 4; ++v) {
+        c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
+      }
+    IB_CUDA(cudaGetLastError());
+    g_ctx[dev] = c;
+  }
+  *out = g_ctx[dev];
+  return IB_OK;
+}
+
+IbLaunch base_launch(Context* c) {
+  IbLaunch a;
+  std::memset(&a, 0, sizeof(a));
+  a.boys_tab = c->boys_tab.as<double>();
+  a.sph = c->sph.as<double>();
+  a.status = c->status.as<int>();
+  return a;
+}
+
+// Scratch doubles per block of the generic kernel, for shells up to lmax.
+long long generic_slice(int lmax) {
+  long long best = 0;
+  for (int a = 0; a <= lmax; ++a)
+    for (int b = 0; b <= a; ++b)
+      for (int cc = 0; cc <= lmax; ++cc)
+        for (int d = 0; d <= cc; ++d) {
+          IbGenericDims g = ib_generic_dims(a, b, cc, d);
+          best = std::max(best, g.total);
+        }
+  return (best + 31) / 32 * 32;
+}
+
+// Launch the emitted kernels for the given variants and the generic kernel;
+// items/ranges already on the device.  Returns the number of kernels launched.
+int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
+             int lmax, int* nlaunch) {
+  IB_CUDA(cudaEventRecord(c->fork, s));
+  for (int i = 0; i < kNSide; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
+  int k = 0;
+  for (int prec = 0; prec < 2; ++prec) {
+    if ((prec == 0 && !fp64_present) || (prec == 1 && !fp32_present)) continue;
+    IbLaunch ap = a;
+    if (prec == 1) ap.ranges = a.ranges + kSlotFp32;
+    const int variant = prec * 2 + (sph ? 1 : 0);
+    // heaviest classes first so they start early on their streams
+    for (int cid = ib_n_emitted_classes - 1; cid >= 0; --cid) {
+      const int grid = c->nsm * c->occ[cid][variant];
+      c->table[cid].launch(variant, grid, c->side[k % kNSide], ap);
+      ++k;
+    }
+  }
+  if (lmax > ib_lmax_emitted && fp64_present) {
+    const long long slice = generic_slice(lmax);
+    long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
+    nblk = std::max<long long>(nblk, 1);
+    IB_CUDA(c->scratch.ensure((size_t)nblk * slice * sizeof(double)));
+    ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, c->side[k % kNSide]>>>(a, kSlotGeneric, sph ? 1 : 0,
+                                                                         c->scratch.as<double>(), slice);
+    ++k;
+  }
+  IB_CUDA(cudaGetLastError());
+  for (int i = 0; i < kNSide; ++i) {
+    IB_CUDA(cudaEventRecord(c->join[i], c->side[i]));
+    IB_CUDA(cudaStreamWaitEvent(s, c->join[i], 0));
+  }
+  *nlaunch += k;
+  return IB_OK;
+}
+
+// ---------------------------------------------------------------- drop-in
+
+struct DropShell {
+  const double* x;
+  const double* cen;
+  int l, n, iskip, nprim, ncont, iskip_cont;
+  const double* coef;
+  const double* T;
+};
+
+int dropin(DropShell* sh, bool sph, double* output_array) {
+  for (int i = 0; i < 4; ++i) {
+    const DropShell& s = sh[i];
+    if (s.l < 0 || s.l > IB_LMAX)
+      return set_status(IB_ERR_ARG, "angular momentum outside [0, " + std::to_string(IB_LMAX) + "]");
+    const int natural = sph ? 2 * s.l + 1 : ncart_h(s.l);
+    if (s.n != natural)
+      return set_status(IB_ERR_ARG, "n? must equal the component count of l? ((l+1)(l+2)/2 Cartesian, 2l+1 spherical)");
+    if (s.nprim < 1 || s.ncont < 1 || s.nprim > 64) return set_status(IB_ERR_ARG, "need 1 <= n?_prim <= 64, n?_cont >= 1");
+    if (!s.x || !s.cen || !s.coef || (sph && !s.T)) return set_status(IB_ERR_ARG, "null input pointer");
+  }
+  if (!output_array) return set_status(IB_ERR_ARG, "null output_array");
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  IB_CUDA(cudaSetDevice(c->device));
+  // virtual shells: one per (index, contracted function)
+  int nshell = 0, nprim = 0;
+  int shell0[4];
+  for (int i = 0; i < 4; ++i) {
+    shell0[i] = nshell;
+    nshell += sh[i].ncont;
+    nprim += sh[i].ncont * sh[i].nprim;
+  }
+  const int nblk = sh[0].ncont * sh[1].ncont * sh[2].ncont * sh[3].ncont;
+  int nc[4];
+  for (int i = 0; i < 4; ++i) nc[i] = ncart_h(sh[i].l);
+  const int cart_block = nc[0] * nc[1] * nc[2] * nc[3];
+  const int res_block = sh[0].n * sh[1].n * sh[2].n * sh[3].n;
+  int tsize[4] = {0, 0, 0, 0};
+  if (sph)
+    for (int i = 0; i < 4; ++i) tsize[i] = nc[i] * (2 * sh[i].l + 1);
+  // host staging layout
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  size_t o_l = 0;
+  size_t o_k = al(o_l + nshell * sizeof(int));
+  size_t o_p = al(o_k + nshell * sizeof(int));
+  size_t o_xyz = al(o_p + nshell * sizeof(int));
+  size_t o_e = al(o_xyz + 3 * nshell * sizeof(double));
+  size_t o_c = al(o_e + nprim * sizeof(double));
+  size_t o_it = al(o_c + nprim * sizeof(double));
+  size_t o_rg = al(o_it + nblk * sizeof(IbItem));
+  size_t o_T[4];
+  size_t cur = al(o_rg + kNRanges * sizeof(int));
+  for (int i = 0; i < 4; ++i) {
+    o_T[i] = cur;
+    cur = al(cur + tsize[i] * sizeof(double));
+  }
+  const size_t total = cur;
+  IB_CUDA(c->h_stage.ensure(total));
+  IB_CUDA(c->d_stage.ensure(total));
+  char* h = static_cast<char*>(c->h_stage.p);
+  int* hl = reinterpret_cast<int*>(h + o_l);
+  int* hk = reinterpret_cast<int*>(h + o_k);
+  int* hp = reinterpret_cast<int*>(h + o_p);
+  double* hxyz = reinterpret_cast<double*>(h + o_xyz);
+  double* he = reinterpret_cast<double*>(h + o_e);
+  double* hc = reinterpret_cast<double*>(h + o_c);
+  IbItem* hit = reinterpret_cast<IbItem*>(h + o_it);
+  int* hrg = reinterpret_cast<int*>(h + o_rg);
+  int ps = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int k = 0; k < sh[i].ncont; ++k) {
+      const int s = shell0[i] + k;
+      hl[s] = sh[i].l;
+      hk[s] = sh[i].nprim;
+      hp[s] = ps;
+      for (int d = 0; d < 3; ++d) hxyz[3 * s + d] = sh[i].cen[d];
+      for (int p = 0; p < sh[i].nprim; ++p) {
+        he[ps + p] = sh[i].x[p];
+        hc[ps + p] = sh[i].coef[p + k * sh[i].nprim];
+      }
+      ps += sh[i].nprim;
+    }
+  // canonical permutation, shared by every combination
+  int lperm[4] = {sh[0].l, sh[1].l, sh[2].l, sh[3].l};
+  int sperm[4] = {0, 1, 2, 3};
+  int stperm[4] = {1, nc[0], nc[0] * nc[1], nc[0] * nc[1] * nc[2]};
+  auto swp = [&](int i, int j) {
+    std::swap(lperm[i], lperm[j]);
+    std::swap(sperm[i], sperm[j]);
+    std::swap(stperm[i], stperm[j]);
+  };
+  if (lperm[0] < lperm[1]) swp(0, 1);
+  if (lperm[2] < lperm[3]) swp(2, 3);
+  if (pair_index_h(lperm[0], lperm[1]) < pair_index_h(lperm[2], lperm[3])) {
+    swp(0, 2);
+    swp(1, 3);
+  }
+  const int pb = pair_index_h(lperm[0], lperm[1]), pk = pair_index_h(lperm[2], lperm[3]);
+  const int cid = pb * (pb + 1) / 2 + pk;
+  int b = 0;
+  for (int ka = 0; ka < sh[0].ncont; ++ka)
+    for (int kb = 0; kb < sh[1].ncont; ++kb)
+      for (int kc = 0; kc < sh[2].ncont; ++kc)
+        for (int kd = 0; kd < sh[3].ncont; ++kd, ++b) {
+          const int orig[4] = {shell0[0] + ka, shell0[1] + kb, shell0[2] + kc, shell0[3] + kd};
+          IbItem it;
+          for (int i = 0; i < 4; ++i) {
+            it.s[i] = orig[sperm[i]];
+            it.st[i] = stperm[i];
+          }
+          it.off = (long long)b * cart_block;
+          hit[b] = it;
+        }
+  std::memset(hrg, 0, kNRanges * sizeof(int));
+  const bool emitted = cid < ib_n_emitted_classes;
+  if (emitted) {
+    hrg[2 * cid] = 0;
+    hrg[2 * cid + 1] = nblk;
+  } else {
+    hrg[kSlotGeneric] = 0;
+    hrg[kSlotGeneric + 1] = nblk;
+  }
+  for (int i = 0; i < 4; ++i)
+    if (sph) std::memcpy(h + o_T[i], sh[i].T, tsize[i] * sizeof(double));
+  IB_CUDA(c->d_cart.ensure((size_t)nblk * cart_block * sizeof(double)));
+  IB_CUDA(c->d_res.ensure((size_t)nblk * (res_block + 2 * cart_block) * sizeof(double)));
+  IB_CUDA(c->h_res.ensure((size_t)nblk * res_block * sizeof(double)));
+  cudaStream_t s = c->stream;
+  char* d = static_cast<char*>(c->d_stage.p);
+  IB_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, s));
+  IbLaunch a = base_launch(c);
+  a.items = reinterpret_cast<const IbItem*>(d + o_it);
+  a.ranges = reinterpret_cast<const int*>(d + o_rg);
+  a.shell_l = reinterpret_cast<const int*>(d + o_l);
+  a.shell_k = reinterpret_cast<const int*>(d + o_k);
+  a.shell_ptr = reinterpret_cast<const int*>(d + o_p);
+  a.shell_xyz = reinterpret_cast<const double*>(d + o_xyz);
+  a.prim_exp = reinterpret_cast<const double*>(d + o_e);
+  a.prim_coef = reinterpret_cast<const double*>(d + o_c);
+  a.out = c->d_cart.as<double>();
+  IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
+  if (emitted) {
+    const int grid = std::max(1, std::min(c->nsm * c->occ[cid][0], (nblk + IB_BLOCK - 1) / IB_BLOCK));
+    c->table[cid].launch(0, grid, s, a);
+  } else {
+    const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
+    long long nb = std::min<long long>({(long long)nblk, 2LL * c->nsm,
+                                        (long long)(kScratchCap / (slice * sizeof(double)))});
+    nb = std::max<long long>(nb, 1);
+    IB_CUDA(c->scratch.ensure((size_t)nb * slice * sizeof(double)));
+    ib_eri_generic<<<(int)nb, IB_GEN_BLOCK, 0, s>>>(a, kSlotGeneric, 0, c->scratch.as<double>(), slice);
+  }
+  IB_CUDA(cudaGetLastError());
+  IbXform x;
+  for (int i = 0; i < 4; ++i) {
+    x.T[i] = sph ? reinterpret_cast<const double*>(d + o_T[i]) : nullptr;
+    x.l[i] = sh[i].l;
+    x.n[i] = sh[i].n;
+  }
+  x.nblk = nblk;
+  x.cart_block = cart_block;
+  x.res_block = res_block;
+  double* dres = c->d_res.as<double>();
+  ib_transform_blocks<<<nblk, 128, 0, s>>>(x, c->d_cart.as<double>(), dres, dres + (size_t)nblk * res_block);
+  IB_CUDA(cudaGetLastError());
+  int hstatus = 0;
+  IB_CUDA(cudaMemcpyAsync(c->h_res.p, dres, (size_t)nblk * res_block * sizeof(double), cudaMemcpyDeviceToHost, s));
+  IB_CUDA(cudaMemcpyAsync(&hstatus, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  IB_CUDA(cudaStreamSynchronize(s));
+  if (hstatus) return set_status(hstatus, "device kernel reported status " + std::to_string(hstatus));
+  // place the compact result at the caller's strides (the emitted code's final
+  // copy loop, contracted_general.py:1808-1876)
+  const double* r = static_cast<const double*>(c->h_res.p);
+  b = 0;
+  for (int ka = 0; ka < sh[0].ncont; ++ka)
+    for (int kb = 0; kb < sh[1].ncont; ++kb)
+      for (int kc = 0; kc < sh[2].ncont; ++kc)
+        for (int kd = 0; kd < sh[3].ncont; ++kd, ++b) {
+          const long long base = (long long)ka * sh[0].iskip_cont + (long long)kb * sh[1].iskip_cont +
+                                 (long long)kc * sh[2].iskip_cont + (long long)kd * sh[3].iskip_cont;
+          const double* rb = r + (size_t)b * res_block;
+          int e = 0;
+          for (int id = 0; id < sh[3].n; ++id)
+            for (int ic = 0; ic < sh[2].n; ++ic)
+              for (int ib = 0; ib < sh[1].n; ++ib)
+                for (int ia = 0; ia < sh[0].n; ++ia, ++e)
+                  output_array[base + (long long)ia * sh[0].iskip + (long long)ib * sh[1].iskip +
+                               (long long)ic * sh[2].iskip + (long long)id * sh[3].iskip] = rb[e];
+        }
+  return set_status(IB_OK, "");
+}
+
+// contracted_general.py:240-502, integer formula emitted as <class>_work_array_size
+int ncum_h(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
+int work_array_size(int la, int lb, int lc, int ld, int ka, int kb, int kc, int kd, int ca, int cb, int cc, int cd) {
+  const int nw = ncum_h(la + lb) * ncum_h(lc) * ncum_h(ld);
+  int n1 = ka * kb * kd * kc;
+  int mem1 = 2 * (nw * n1 + ld + lc + la + lb + 1);
+  int n2 = ca * kb * kd * kc;
+  if (n1 < n2) n1 = n2;
+  n2 = ca * cb * kd * kc;
+  if (n1 < n2) n1 = n2;
+  n2 = ca * cb * cd * kc;
+  if (n1 < n2) n1 = n2;
+  n2 = ca * cb * cd * cc;
+  if (n1 < n2) n1 = n2;
+  int mem2 = 2 * nw * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  n1 = ca * cb * cd * cc;
+  int layer = 0;  // generator.py:1112-1157 hrr_layer[lb][la]
+  for (int j = 0; j <= lb; ++j) layer = std::max(layer, (ncum_h(la + lb - j) - ncum_h(la - 1)) * ncart_h(j));
+  mem2 = 2 * layer * ncart_h(lc) * ncart_h(ld) * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  mem2 = 2 * ncart_h(lc) * ncart_h(ld) * ncart_h(lb) * ncart_h(la) * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  return mem1;
+}
+
+// ---------------------------------------------------------------- sph matrices
+double dfact(int n) {
+  double r = 1.0;
+  while (n > 1) {
+    r *= n;
+    n -= 2;
+  }
+  return r;
+}
+double binom(int n, int k) {
+  if (k < 0 || k > n) return 0.0;
+  double r = 1.0;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+void sph_matrix_host(int l, double* T) {
+  const int nc = ncart_h(l), ns = 2 * l + 1;
+  std::vector<int> cx, cy, cz;
+  for (int mx = l; mx >= 0; --mx)
+    for (int my = l - mx; my >= 0; --my) {
+      cx.push_back(mx);
+      cy.push_back(my);
+      cz.push_back(l - mx - my);
+    }
+  auto idx = [&](int i, int j, int k) {
+    for (int c = 0; c < nc; ++c)
+      if (cx[c] == i && cy[c] == j && cz[c] == k) return c;
+    return -1;
+  };
+  for (int c = 0; c < nc * ns; ++c) T[c] = 0.0;
+  for (int col = 0; col < ns; ++col) {
+    const int m = col - l, am = std::abs(m);
+    const double vm = m < 0 ? 0.5 : 0.0;
+    for (int t = 0; t <= (l - am) / 2; ++t)
+      for (int u = 0; u <= t; ++u)
+        for (double v = vm; v <= std::floor(am / 2.0 - vm) + vm + 1e-9; v += 1.0) {
+          const int two_v = (int)std::lround(2 * v);
+          const double sign = ((int)std::lround(t + v - vm) % 2) ? -1.0 : 1.0;
+          const double coef = sign * std::pow(0.25, t) * binom(l, t) * binom(l - t, am + t) * binom(t, u) *
+                              binom(am, two_v);
+          const int i = 2 * t + am - 2 * u - two_v, j = 2 * u + two_v, k = l - 2 * t - am;
+          const int c = idx(i, j, k);
+          if (c >= 0 && coef != 0.0) T[c + col * nc] += coef;
+        }
+    // scale to the norm of x^l (monomial overlaps up to an l-only factor)
+    double nrm = 0.0;
+    for (int p = 0; p < nc; ++p)
+      for (int q = 0; q < nc; ++q) {
+        const int a = cx[p] + cx[q], bq = cy[p] + cy[q], cq = cz[p] + cz[q];
+        if ((a | bq | cq) & 1) continue;
+        nrm += T[p + col * nc] * T[q + col * nc] * dfact(a - 1) * dfact(bq - 1) * dfact(cq - 1);
+      }
+    const double sc = std::sqrt(dfact(2 * l - 1) / nrm);
+    for (int p = 0; p < nc; ++p) T[p + col * nc] *= sc;
+  }
+}
+
+}  // namespace
+
+void build_sph_host(std::vector<double>& out) {
+  out.assign(packed_sph_size(), 0.0);
+  for (int l = 0; l <= IB_LMAX; ++l) sph_matrix_host(l, out.data() + ib_sph_offset(l));
+}
+
+namespace {
+int resolve_stream(Context* c, void* stream, cudaStream_t* s) {
+  *s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  return IB_OK;
+}
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+void intception_integral_eri_abcd_m_cont_cart_main(
+    const double* xa, const double cA[3], const int la, const int na, const int iskipa, const int na_prim,
+    const int na_cont, const int iskipa_cont, const double* contract_array_a, const double* xb, const double cB[3],
+    const int lb, const int nb, const int iskipb, const int nb_prim, const int nb_cont, const int iskipb_cont,
+    const double* contract_array_b, const double* xc, const double cC[3], const int lc, const int nc,
+    const int iskipc, const int nc_prim, const int nc_cont, const int iskipc_cont, const double* contract_array_c,
+    const double* xd, const double cD[3], const int ld, const int nd, const int iskipd, const int nd_prim,
+    const int nd_cont, const int iskipd_cont, const double* contract_array_d, double* work_array,
+    double* output_array) {
+  (void)work_array;
+  DropShell sh[4] = {{xa, cA, la, na, iskipa, na_prim, na_cont, iskipa_cont, contract_array_a, nullptr},
+                     {xb, cB, lb, nb, iskipb, nb_prim, nb_cont, iskipb_cont, contract_array_b, nullptr},
+                     {xc, cC, lc, nc, iskipc, nc_prim, nc_cont, iskipc_cont, contract_array_c, nullptr},
+                     {xd, cD, ld, nd, iskipd, nd_prim, nd_cont, iskipd_cont, contract_array_d, nullptr}};
+  dropin(sh, false, output_array);
+}
+
+int intception_integral_eri_abcd_m_cont_cart_work_array_size(const int la, const int lb, const int lc,
+                                                              const int ld, const int na_prim, const int nb_prim,
+                                                              const int nc_prim, const int nd_prim,
+                                                              const int na_cont, const int nb_cont,
+                                                              const int nc_cont, const int nd_cont) {
+  return work_array_size(la, lb, lc, ld, na_prim, nb_prim, nc_prim, nd_prim, na_cont, nb_cont, nc_cont, nd_cont);
+}
+
+void intception_integral_eri_abcd_m_cont_sph_main(
+    const double* xa, const double cA[3], const int la, const int na, const int iskipa, const int na_prim,
+    const int na_cont, const int iskipa_cont, const double* contract_array_a, const double* sph_trans_array_a,
+    const double* xb, const double cB[3], const int lb, const int nb, const int iskipb, const int nb_prim,
+    const int nb_cont, const int iskipb_cont, const double* contract_array_b, const double* sph_trans_array_b,
+    const double* xc, const double cC[3], const int lc, const int nc, const int iskipc, const int nc_prim,
+    const int nc_cont, const int iskipc_cont, const double* contract_array_c, const double* sph_trans_array_c,
+    const double* xd, const double cD[3], const int ld, const int nd, const int iskipd, const int nd_prim,
+    const int nd_cont, const int iskipd_cont, const double* contract_array_d, const double* sph_trans_array_d,
+    double* work_array, double* output_array) {
+  (void)work_array;
+  DropShell sh[4] = {{xa, cA, la, na, iskipa, na_prim, na_cont, iskipa_cont, contract_array_a, sph_trans_array_a},
+                     {xb, cB, lb, nb, iskipb, nb_prim, nb_cont, iskipb_cont, contract_array_b, sph_trans_array_b},
+                     {xc, cC, lc, nc, iskipc, nc_prim, nc_cont, iskipc_cont, contract_array_c, sph_trans_array_c},
+                     {xd, cD, ld, nd, iskipd, nd_prim, nd_cont, iskipd_cont, contract_array_d, sph_trans_array_d}};
+  dropin(sh, true, output_array);
+}
+
+int intception_integral_eri_abcd_m_cont_sph_work_array_size(const int la, const int lb, const int lc,
+                                                             const int ld, const int na_prim, const int nb_prim,
+                                                             const int nc_prim, const int nd_prim,
+                                                             const int na_cont, const int nb_cont,
+                                                             const int nc_cont, const int nd_cont) {
+  return work_array_size(la, lb, lc, ld, na_prim, nb_prim, nc_prim, nd_prim, na_cont, nb_cont, nc_cont, nd_cont);
+}
+
+int intception_b200_last_status(void) { return tl_status; }
+const char* intception_b200_last_error(void) { return tl_msg.c_str(); }
+int intception_b200_lmax(void) { return IB_LMAX; }
+int intception_b200_last_launch_count(void) { return tl_launches; }
+
+int intception_b200_sph_matrix(int l, double* T) {
+  if (l < 0 || l > IB_LMAX || !T) return set_status(IB_ERR_ARG, "l out of range or null T");
+  sph_matrix_host(l, T);
+  return set_status(IB_OK, "");
+}
+
+int intception_b200_boys_batch(const double* x, int n, int nmax, double* f, void* stream) {
+  if (n < 0 || nmax < 0 || nmax > 4 * IB_LMAX || (n > 0 && (!x || !f)))
+    return set_status(IB_ERR_ARG, "boys_batch: bad arguments");
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  if (n == 0) return set_status(IB_OK, "");
+  cudaStream_t s;
+  resolve_stream(c, stream, &s);
+  const int grid = std::min((n + 255) / 256, c->nsm * 8);
+  ib_boys_kernel<<<grid, 256, 0, s>>>(x, n, nmax, c->boys_tab.as<double>(), f);
+  IB_CUDA(cudaGetLastError());
+  return set_status(IB_OK, "");
+}
+
+void intception_boys(double* f, const int ifskip, const int nmin, const int nmax, const double x) {
+  if (!f || nmin < 0 || nmax < nmin || nmax > 4 * IB_LMAX || !(x >= 0.0)) {
+    set_status(IB_ERR_ARG, "intception_boys: bad arguments");
+    return;
+  }
+  Context* c = nullptr;
+  if (get_context(&c)) return;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (c->h_stage.ensure(64 * sizeof(double)) != cudaSuccess || c->d_stage.ensure(64 * sizeof(double)) != cudaSuccess) {
+    set_status(IB_ERR_CUDA, "intception_boys: allocation failed");
+    return;
+  }
+  double* h = static_cast<double*>(c->h_stage.p);
+  double* d = c->d_stage.as<double>();
+  h[0] = x;
+  cudaStream_t s = c->stream;
+  cudaMemcpyAsync(d, h, sizeof(double), cudaMemcpyHostToDevice, s);
+  ib_boys_kernel<<<1, 32, 0, s>>>(d, 1, nmax, c->boys_tab.as<double>(), d + 8);
+  cudaMemcpyAsync(h + 8, d + 8, (nmax + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_status(IB_ERR_CUDA, std::string("intception_boys: ") + cudaGetErrorString(e));
+    return;
+  }
+  for (int m = nmin; m <= nmax; ++m) f[m * ifskip] = h[8 + m];
+  set_status(IB_OK, "");
+}
+
+int intception_b200_synchronize(void) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  IB_CUDA(cudaStreamSynchronize(c->stream));
+  return set_status(IB_OK, "");
+}
+
+int intception_b200_eri_batch(const intception_b200_basis* basis, const int* quartets, const long long* out_off,
+                              int nq, int spherical, int precision, const double* bounds, double threshold,
+                              double* out, void* stream) {
+  tl_launches = 0;
+  if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out)))
+    return set_status(IB_ERR_ARG, "eri_batch: null argument");
+  if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "eri_batch: basis lmax out of range");
+  if (precision != IB_PREC_FP64 && precision != IB_PREC_MIXED) return set_status(IB_ERR_ARG, "eri_batch: precision");
+  if (precision == IB_PREC_MIXED && !bounds) return set_status(IB_ERR_ARG, "eri_batch: mixed precision needs bounds");
+  if (nq == 0) return set_status(IB_OK, "");
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t s;
+  resolve_stream(c, stream, &s);
+  IB_CUDA(c->keys.ensure((size_t)nq * sizeof(unsigned)));
+  IB_CUDA(c->keys2.ensure((size_t)nq * sizeof(unsigned)));
+  IB_CUDA(c->vals.ensure((size_t)nq * sizeof(int)));
+  IB_CUDA(c->vals2.ensure((size_t)nq * sizeof(int)));
+  IB_CUDA(c->items.ensure((size_t)nq * sizeof(IbItem)));
+  size_t tmp_bytes = 0;
+  IB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
+                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
+  IB_CUDA(c->cub_tmp.ensure(tmp_bytes));
+  int nl = 0;
+  IB_CUDA(cudaMemsetAsync(c->ranges.p, 0, kNRanges * sizeof(int), s));
+  IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
+  const int grid = std::min((nq + 255) / 256, c->nsm * 16);
+  ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, nq, basis->lmax, bounds, threshold,
+                                   precision == IB_PREC_MIXED ? 1 : 0, ib_n_emitted_classes, c->keys.as<unsigned>(),
+                                   c->vals.as<int>(), c->status.as<int>());
+  ++nl;
+  IB_CUDA(cudaGetLastError());
+  IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
+                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
+  ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
+                                      out_off, spherical ? 1 : 0, ib_n_emitted_classes, c->items.as<IbItem>(),
+                                      c->ranges.as<int>());
+  ++nl;
+  IB_CUDA(cudaGetLastError());
+  IbLaunch a = base_launch(c);
+  a.items = c->items.as<IbItem>();
+  a.ranges = c->ranges.as<int>();
+  a.shell_l = basis->shell_l;
+  a.shell_k = basis->shell_k;
+  a.shell_ptr = basis->shell_ptr;
+  a.shell_xyz = basis->shell_xyz;
+  a.prim_exp = basis->prim_exp;
+  a.prim_coef = basis->prim_coef;
+  a.out = out;
+  st = dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, &nl);
+  tl_launches = nl;
+  if (st) return st;
+  return set_status(IB_OK, "");
+}
+
+// Device status word of the last batch (reads it synchronously).
+int intception_b200_batch_status(void) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  int h = 0;
+  IB_CUDA(cudaStreamSynchronize(c->stream));
+  IB_CUDA(cudaMemcpy(&h, c->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  return h;
+}
+
+}  // extern "C"

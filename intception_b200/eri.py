@@ -1,0 +1,233 @@
+"""Python host layer over libintception_b200.so (ctypes).
+
+Mirrors the reference's interface for the ERI path:
+
+* ``cont_cart_main`` / ``cont_sph_main`` take the argument list of the
+  generated ``intception_integral_eri_abcd_m_cont_{cart,sph}_main``
+  (``contracted_general.py:42-68``), as numpy arrays, and write
+  ``output_array`` in place.  They return None like the C functions; a failed
+  call raises ``IntceptionError`` with the library's message.
+* ``work_array_size`` is the emitted ``..._work_array_size``.
+* ``boys`` is the emitted ``intception_boys``.
+* ``EriEngine`` is the batched device path (torch tensors as device memory).
+
+The CUDA library is required: importing works without it, but every call
+raises if ``libintception_b200.so`` is missing or no GPU is present.  There is
+no CPU fallback.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import basis as _basis
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, 'libintception_b200.so')
+HEADER = os.path.join(os.path.dirname(PKG), 'include', 'intception_b200.h')
+
+IB_OK, IB_ERR_ARG, IB_ERR_CUDA, IB_ERR_SCRATCH, IB_ERR_NODEVICE = 0, 1, 2, 3, 4
+PREC_FP64, PREC_MIXED = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+class IntceptionError(RuntimeError):
+    pass
+
+
+class _Basis(C.Structure):
+    _fields_ = [('shell_l', C.c_void_p), ('shell_k', C.c_void_p), ('shell_ptr', C.c_void_p),
+                ('shell_xyz', C.c_void_p), ('prim_exp', C.c_void_p), ('prim_coef', C.c_void_p),
+                ('nshell', C.c_int), ('nprim', C.c_int), ('lmax', C.c_int)]
+
+
+def header_functions(path=HEADER):
+    """Names of every function the public header declares."""
+    text = open(path).read()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    names = re.findall(r'^\s*(?:const\s+)?(?:void|int|char|double)\s*\**\s*(\w+)\s*\(', text, flags=re.M)
+    return sorted(set(names))
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise IntceptionError('libintception_b200.so not built: run python -m intception_b200.build')
+    lib = C.CDLL(LIB_PATH)
+    idx = [C.c_int] * 6
+    per_cart = [_dp, _dp] + idx + [_dp]
+    per_sph = per_cart + [_dp]
+    lib.intception_integral_eri_abcd_m_cont_cart_main.argtypes = per_cart * 4 + [_dp, _dp]
+    lib.intception_integral_eri_abcd_m_cont_cart_main.restype = None
+    lib.intception_integral_eri_abcd_m_cont_sph_main.argtypes = per_sph * 4 + [_dp, _dp]
+    lib.intception_integral_eri_abcd_m_cont_sph_main.restype = None
+    for v in ('cart', 'sph'):
+        f = getattr(lib, 'intception_integral_eri_abcd_m_cont_%s_work_array_size' % v)
+        f.argtypes = [C.c_int] * 12
+        f.restype = C.c_int
+    lib.intception_boys.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double]
+    lib.intception_boys.restype = None
+    lib.intception_b200_last_status.restype = C.c_int
+    lib.intception_b200_last_error.restype = C.c_char_p
+    lib.intception_b200_lmax.restype = C.c_int
+    lib.intception_b200_last_launch_count.restype = C.c_int
+    lib.intception_b200_sph_matrix.argtypes = [C.c_int, _dp]
+    lib.intception_b200_sph_matrix.restype = C.c_int
+    lib.intception_b200_boys_batch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    lib.intception_b200_boys_batch.restype = C.c_int
+    lib.intception_b200_synchronize.restype = C.c_int
+    lib.intception_b200_batch_status.restype = C.c_int
+    lib.intception_b200_eri_batch.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                              C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    lib.intception_b200_eri_batch.restype = C.c_int
+    lib.intception_b200_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
+    lib.intception_b200_fma_peak.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(status=None):
+    lib = load()
+    st = lib.intception_b200_last_status() if status is None else status
+    if st != IB_OK:
+        raise IntceptionError('intception_b200 status %d: %s' % (st, lib.intception_b200_last_error().decode()))
+
+
+def lmax():
+    return load().intception_b200_lmax()
+
+
+def fma_peak(fp64=True, iters=4096):
+    """Measured FMA throughput of the current device (FLOP/s)."""
+    v = C.c_double(0.0)
+    _check(load().intception_b200_fma_peak(1 if fp64 else 0, iters, C.byref(v)))
+    return v.value
+
+
+def sph_matrix(l):
+    """The library's ncart x (2l+1) matrix (T[icart + isph*ncart])."""
+    nc = (l + 1) * (l + 2) // 2
+    T = np.zeros(nc * (2 * l + 1))
+    _check(load().intception_b200_sph_matrix(l, T.ctypes.data_as(_dp)))
+    return T.reshape((nc, 2 * l + 1), order='F')
+
+
+def work_array_size(la, lb, lc, ld, na_prim, nb_prim, nc_prim, nd_prim, na_cont, nb_cont, nc_cont, nd_cont,
+                    spherical=False):
+    f = getattr(load(), 'intception_integral_eri_abcd_m_cont_%s_work_array_size' % ('sph' if spherical else 'cart'))
+    return f(la, lb, lc, ld, na_prim, nb_prim, nc_prim, nd_prim, na_cont, nb_cont, nc_cont, nd_cont)
+
+
+def _main(variant, shells, work_array, output_array):
+    lib = load()
+    fn = getattr(lib, 'intception_integral_eri_abcd_m_cont_%s_main' % variant)
+    args, keep = [], []
+    for s in shells:
+        x = np.ascontiguousarray(s['x'], dtype=np.float64)
+        cen = np.ascontiguousarray(s['cen'], dtype=np.float64)
+        coef = np.ascontiguousarray(s['coef'], dtype=np.float64)
+        keep += [x, cen, coef]
+        args += [x.ctypes.data_as(_dp), cen.ctypes.data_as(_dp), s['l'], s['n'], s['iskip'], s['nprim'],
+                 s['ncont'], s['iskip_cont'], coef.ctypes.data_as(_dp)]
+        if variant == 'sph':
+            T = np.ascontiguousarray(np.asarray(s['T'], dtype=np.float64).ravel(order='F'))
+            keep.append(T)
+            args.append(T.ctypes.data_as(_dp))
+    if output_array.dtype != np.float64 or not output_array.flags['C_CONTIGUOUS']:
+        raise IntceptionError('output_array must be a contiguous float64 array')
+    wa = work_array if work_array is not None else np.zeros(1)
+    fn(*args, wa.ctypes.data_as(_dp), output_array.ctypes.data_as(_dp))
+    _check()
+
+
+def cont_cart_main(shells, output_array, work_array=None):
+    """Drop-in for intception_integral_eri_abcd_m_cont_cart_main.  shells is
+    four dicts (a, b, c, d) with keys x, cen, l, n, iskip, nprim, ncont,
+    iskip_cont, coef (the emitted per-index arguments, wrappers.py:41-143)."""
+    _main('cart', shells, work_array, output_array)
+
+
+def cont_sph_main(shells, output_array, work_array=None):
+    """Drop-in for intception_integral_eri_abcd_m_cont_sph_main (dicts also
+    carry T = sph_trans_array_?, ncart x nsph)."""
+    _main('sph', shells, work_array, output_array)
+
+
+def boys(nmax, x, nmin=0, ifskip=1):
+    """Drop-in for intception_boys: F_m(x), m = nmin..nmax (array of nmax+1)."""
+    f = np.zeros((nmax + 1) * ifskip)
+    load().intception_boys(f.ctypes.data_as(_dp), ifskip, nmin, nmax, float(x))
+    _check()
+    return f[::ifskip]
+
+
+class EriEngine:
+    """Batched contracted ERIs on the current CUDA device.
+
+    The shell table is uploaded once (torch tensors hold the device memory);
+    ``compute`` evaluates a quartet list into a flat output vector laid out
+    per quartet with a fastest (``basis.ShellBatch`` conventions).
+    """
+
+    def __init__(self, batch, device='cuda'):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        b = batch
+        self.spherical = bool(b.spherical)
+        t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(self.device)  # noqa: E731
+        self.shell_l = t(b.shell_l, torch.int32)
+        self.shell_k = t(b.shell_k, torch.int32)
+        self.shell_ptr = t(b.shell_ptr, torch.int32)
+        self.shell_xyz = t(b.shell_xyz, torch.float64)
+        self.prim_exp = t(b.prim_exp, torch.float64)
+        self.prim_coef = t(b.prim_coef, torch.float64)
+        self.lmax = int(b.shell_l.max()) if len(b.shell_l) else 0
+        self._basis = _Basis(self.shell_l.data_ptr(), self.shell_k.data_ptr(), self.shell_ptr.data_ptr(),
+                             self.shell_xyz.data_ptr(), self.prim_exp.data_ptr(), self.prim_coef.data_ptr(),
+                             len(b.shell_l), len(b.prim_exp), self.lmax)
+        self.quartets = t(b.quartets.reshape(-1), torch.int32)
+        self.out_off = t(b.out_off, torch.int64)
+        self.nq = b.nq
+        self.out_size = b.out_size
+        load()
+
+    def compute(self, out=None, precision=PREC_FP64, bounds=None, threshold=0.0, stream=None, quartets=None,
+                out_off=None, nq=None):
+        torch = self.torch
+        if out is None:
+            out = torch.empty(self.out_size, dtype=torch.float64, device=self.device)
+        q = self.quartets if quartets is None else quartets
+        o = self.out_off if out_off is None else out_off
+        n = self.nq if nq is None else nq
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = load().intception_b200_eri_batch(
+            C.byref(self._basis), q.data_ptr(), o.data_ptr(), n, 1 if self.spherical else 0, precision,
+            bounds.data_ptr() if bounds is not None else None, float(threshold), out.data_ptr(),
+            C.c_void_p(s.cuda_stream))
+        _check(st)
+        return out
+
+    @staticmethod
+    def last_launch_count():
+        return load().intception_b200_last_launch_count()
+
+    @staticmethod
+    def device_status():
+        return load().intception_b200_batch_status()
+
+
+def batch_reference_layout(batch):
+    """List of (offset, dims) per quartet, the layout ``compute`` writes."""
+    return [(int(batch.out_off[q]), batch.block_dims(q)) for q in range(batch.nq)]
+
+
+__all__ = ['IntceptionError', 'load', 'lmax', 'sph_matrix', 'work_array_size', 'cont_cart_main', 'cont_sph_main',
+           'boys', 'EriEngine', 'header_functions', '_basis']

@@ -1,0 +1,483 @@
+/*
+ * eri_oracle.c -- CPU restatement of the reference's contracted-ERI path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: tests/, the smoke check
+ * and bench.py's cpu_baseline leg may call it; the product (intception_b200)
+ * never links or calls it.
+ *
+ * It restates, in plain C, what the C99 emitted by the reference generator for
+ * the ERI input script (oracle/eri_input.py) computes, function by function:
+ *   oracle_boys ........ generator/callables/generator_boys_function.py:98-205
+ *   base [00|00]^(m) ... generator/callables/integral_wrapper_base_function.py:84-162
+ *   VRR a, c, d ........ generator/callables/main_source_algorithms/contracted_general.py:720-1082
+ *                        (recurrence terms: the input script's vrra/vrrc/vrrd)
+ *   contraction ........ generator/callables/generator_contract_function.py:69-125,
+ *                        driven by contracted_general.py:1083-1417 (a truncated to
+ *                        [la, la+lb], c and d to exactly lc and ld)
+ *   HRR a -> b ......... generator/callables/generator_hrr_function.py:265-436,
+ *                        driver contracted_general.py:1574-1807; the HGP form of
+ *                        dsl_extensions.py:903-950, (a,b+1i) = (a+1i,b) + AB_i (a,b)
+ *   sph transform ...... generator/callables/generator_sph_trans_function.py:69-125
+ *                        out[pre + isph*n_pre] = sum_cart in[pre + cart*skip] T[cart + isph*ncart]
+ *   output copy ........ contracted_general.py:1808-1876 (caller strides)
+ *   work-array size .... contracted_general.py:240-502 (integer formula, bit-exact)
+ *
+ * Component order inside one angular-momentum level: x-descending, then
+ * y-descending (dsl.py:988-1001); index within the level
+ * mz + (my+mz)(my+mz+1)/2, cumulative offset (l)(l+1)(l+2)/6 (dsl.py:1029-1041).
+ *
+ * The Boys tables are regenerated with mpmath by oracle/gen_boys_tables.py.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "boys_tables.h"
+
+#define OR_LMAX 8
+
+static const double oracle_oof[7] = {1.0, 1.0, 1.0 / 2.0, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
+
+static int nc_l(int l) { return (l + 1) * (l + 2) / 2; }
+static int ncum(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
+static int cidx(int mx, int my, int mz) {
+  int l = mx + my + mz;
+  return ncum(l - 1) + mz + (my + mz) * (my + mz + 1) / 2;
+}
+
+/* Cartesian exponents of every cumulative component index up to OR_LMAX*2 */
+#define OR_NCUM_MAX 1771 /* ncum(20) */
+static int comp_tab[OR_NCUM_MAX][3];
+static int comp_tab_ready = 0;
+static void init_comp_tab(void) {
+  if (comp_tab_ready) return;
+  int n = 0;
+  for (int l = 0; l <= 20; ++l)
+    for (int mx = l; mx >= 0; --mx)
+      for (int my = l - mx; my >= 0; --my) {
+        comp_tab[n][0] = mx;
+        comp_tab[n][1] = my;
+        comp_tab[n][2] = l - mx - my;
+        ++n;
+      }
+  comp_tab_ready = 1;
+}
+
+/* generator_boys_function.py:98-205: small x (<=15) 7-term Taylor about the
+ * nearest 0.1 grid point then downward recursion; 15<x<35 F_0 Taylor then upward
+ * recursion; x>=35 asymptotic F_0 and upward recursion without exp(-x). */
+void oracle_boys(double *f, int ifskip, int nmin, int nmax, double x) {
+  if (x <= 15.0) {
+    int i = (int)round(x * 10.0);
+    double dx = (double)i * 0.1 - x;
+    double xn = 1.0;
+    f[nmax * ifskip] = oracle_boys_smallx[i][nmax];
+    for (int k = 1; k < 7; ++k) {
+      xn *= dx;
+      f[nmax * ifskip] += oracle_boys_smallx[i][nmax + k] * xn * oracle_oof[k];
+    }
+    double ex = exp(-x);
+    for (int m = nmax - 1; m >= nmin; --m)
+      f[m * ifskip] = (2.0 * x * f[(m + 1) * ifskip] + ex) / (2.0 * (double)m + 1.0);
+  } else if (x < 35.0) {
+    int i = (int)round(x * 10.0);
+    double dx = (double)i * 0.1 - x;
+    i -= 150;
+    double oox = 1.0 / x, xn = 1.0;
+    f[0] = oracle_boys_mediumx[i][0];
+    for (int k = 1; k < 7; ++k) {
+      xn *= dx;
+      f[0] += oracle_boys_mediumx[i][k] * xn * oracle_oof[k];
+    }
+    double ex = exp(-x);
+    for (int m = 0; m < nmax; ++m)
+      f[(m + 1) * ifskip] = ((double)m + 0.5) * oox * f[m * ifskip] - ex * 0.5 * oox;
+  } else {
+    double oox = 1.0 / x;
+    f[0] = 0.5 * sqrt(3.141592653589793 * oox);
+    for (int m = 0; m < nmax; ++m)
+      f[(m + 1) * ifskip] = ((double)m + 0.5) * oox * f[m * ifskip];
+  }
+}
+
+/* contracted_general.py:240-502 (emitted as <class>_work_array_size) */
+static int hrr_layer_size(int lb, int la) {
+  /* generator.py:1112-1157: the largest HRR layer, max over l_b' = 0..lb of
+   * ncart-sum of the a range [la, la+lb-lb'] times ncart(lb') */
+  int best = 0;
+  for (int j = 0; j <= lb; ++j) {
+    int na = ncum(la + lb - j) - ncum(la - 1);
+    int v = na * nc_l(j);
+    if (v > best) best = v;
+  }
+  return best;
+}
+
+int oracle_eri_work_array_size(int la, int lb, int lc, int ld, int na_prim, int nb_prim, int nc_prim,
+                               int nd_prim, int na_cont, int nb_cont, int nc_cont, int nd_cont) {
+  int nw = ncum(la + lb) * ncum(lc) * ncum(ld);
+  int n1 = na_prim * nb_prim * nd_prim * nc_prim;
+  int mem1 = 2 * (nw * n1 + ld + lc + la + lb + 1);
+  int n2 = na_cont * nb_prim * nd_prim * nc_prim;
+  if (n1 < n2) n1 = n2;
+  n2 = na_cont * nb_cont * nd_prim * nc_prim;
+  if (n1 < n2) n1 = n2;
+  n2 = na_cont * nb_cont * nd_cont * nc_prim;
+  if (n1 < n2) n1 = n2;
+  n2 = na_cont * nb_cont * nd_cont * nc_cont;
+  if (n1 < n2) n1 = n2;
+  int mem2 = 2 * nw * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  n1 = na_cont * nb_cont * nd_cont * nc_cont;
+  mem2 = 2 * hrr_layer_size(lb, la) * nc_l(lc) * nc_l(ld) * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  mem2 = 2 * nc_l(lc) * nc_l(ld) * nc_l(lb) * nc_l(la) * n1;
+  if (mem2 > mem1) mem1 = mem2;
+  return mem1;
+}
+
+/* One primitive quartet: V[m][a][c][d] over cumulative component indices, with
+ * a <= la+lb, c <= lc, d <= ld and m + |a| + |c| + |d| <= L.  Recurrences are the
+ * input script's vrra / vrrc / vrrd (Obara-Saika with the auxiliary index m). */
+typedef struct {
+  int L, na, nc, nd; /* cumulative counts */
+  double *v;
+} vtab;
+#define V(t, m, a, c, d) ((t)->v[(((size_t)(m) * (t)->na + (a)) * (t)->nc + (c)) * (t)->nd + (d)])
+
+static int first_dir(const int *e) { return e[0] > 0 ? 0 : (e[1] > 0 ? 1 : 2); }
+
+static void prim_vrr(vtab *t, int lab, int lc, int ld, const double *base, const double PA[3],
+                     const double WP[3], const double QC[3], const double QD[3], const double WQ[3],
+                     double o2z, double roz, double o2e, double roe, double o2zpe) {
+  int L = t->L;
+  for (int m = 0; m <= L; ++m) V(t, m, 0, 0, 0) = base[m];
+  /* vrra: [a+1i| = PA_i [a| + WP_i [a|^(m+1) + a_i/(2zeta) ([a-1i| - rho/zeta [a-1i|^(m+1)) */
+  for (int ia = 1; ia < ncum(lab); ++ia) {
+    const int *e = comp_tab[ia];
+    int la_ = e[0] + e[1] + e[2];
+    int i = first_dir(e);
+    int em[3] = {e[0], e[1], e[2]};
+    em[i] -= 1;
+    int a1 = cidx(em[0], em[1], em[2]);
+    int n2 = em[i];
+    int a2 = -1;
+    if (n2 > 0) {
+      int e2[3] = {em[0], em[1], em[2]};
+      e2[i] -= 1;
+      a2 = cidx(e2[0], e2[1], e2[2]);
+    }
+    for (int m = 0; m + la_ <= L; ++m) {
+      double v = PA[i] * V(t, m, a1, 0, 0) + WP[i] * V(t, m + 1, a1, 0, 0);
+      if (a2 >= 0) v += o2z * n2 * (V(t, m, a2, 0, 0) - roz * V(t, m + 1, a2, 0, 0));
+      V(t, m, ia, 0, 0) = v;
+    }
+  }
+  /* vrrc: [a|c+1i] = QC_i [a|c] + WQ_i [a|c]^(m+1) + c_i/(2eta)([a|c-1i] - rho/eta [..]^(m+1))
+   *                  + a_i/(2(zeta+eta)) [a-1i|c]^(m+1) */
+  for (int ic = 1; ic < ncum(lc); ++ic) {
+    const int *f = comp_tab[ic];
+    int lf = f[0] + f[1] + f[2];
+    int i = first_dir(f);
+    int fm[3] = {f[0], f[1], f[2]};
+    fm[i] -= 1;
+    int c1 = cidx(fm[0], fm[1], fm[2]);
+    int n2 = fm[i];
+    int c2 = -1;
+    if (n2 > 0) {
+      int f2[3] = {fm[0], fm[1], fm[2]};
+      f2[i] -= 1;
+      c2 = cidx(f2[0], f2[1], f2[2]);
+    }
+    for (int ia = 0; ia < ncum(lab); ++ia) {
+      const int *e = comp_tab[ia];
+      int le = e[0] + e[1] + e[2];
+      int na_i = e[i], a1 = -1;
+      if (na_i > 0) {
+        int em[3] = {e[0], e[1], e[2]};
+        em[i] -= 1;
+        a1 = cidx(em[0], em[1], em[2]);
+      }
+      for (int m = 0; m + le + lf <= L; ++m) {
+        double v = QC[i] * V(t, m, ia, c1, 0) + WQ[i] * V(t, m + 1, ia, c1, 0);
+        if (c2 >= 0) v += o2e * n2 * (V(t, m, ia, c2, 0) - roe * V(t, m + 1, ia, c2, 0));
+        if (a1 >= 0) v += o2zpe * na_i * V(t, m + 1, a1, c1, 0);
+        V(t, m, ia, ic, 0) = v;
+      }
+    }
+  }
+  /* vrrd: [a|c,d+1i] = QD_i [..] + WQ_i [..]^(m+1) + d_i/(2eta)([..d-1i] - rho/eta [..]^(m+1))
+   *        + c_i/(2eta)([a|c-1i,d] - rho/eta [..]^(m+1)) + a_i/(2(zeta+eta)) [a-1i|c,d]^(m+1) */
+  for (int id = 1; id < ncum(ld); ++id) {
+    const int *g = comp_tab[id];
+    int lg = g[0] + g[1] + g[2];
+    int i = first_dir(g);
+    int gm[3] = {g[0], g[1], g[2]};
+    gm[i] -= 1;
+    int d1 = cidx(gm[0], gm[1], gm[2]);
+    int n2 = gm[i];
+    int d2 = -1;
+    if (n2 > 0) {
+      int g2[3] = {gm[0], gm[1], gm[2]};
+      g2[i] -= 1;
+      d2 = cidx(g2[0], g2[1], g2[2]);
+    }
+    for (int ia = 0; ia < ncum(lab); ++ia) {
+      const int *e = comp_tab[ia];
+      int le = e[0] + e[1] + e[2];
+      int na_i = e[i], a1 = -1;
+      if (na_i > 0) {
+        int em[3] = {e[0], e[1], e[2]};
+        em[i] -= 1;
+        a1 = cidx(em[0], em[1], em[2]);
+      }
+      for (int ic = 0; ic < ncum(lc); ++ic) {
+        const int *f = comp_tab[ic];
+        int lf = f[0] + f[1] + f[2];
+        int nc_i = f[i], c1 = -1;
+        if (nc_i > 0) {
+          int fm[3] = {f[0], f[1], f[2]};
+          fm[i] -= 1;
+          c1 = cidx(fm[0], fm[1], fm[2]);
+        }
+        for (int m = 0; m + le + lf + lg <= L; ++m) {
+          double v = QD[i] * V(t, m, ia, ic, d1) + WQ[i] * V(t, m + 1, ia, ic, d1);
+          if (d2 >= 0) v += o2e * n2 * (V(t, m, ia, ic, d2) - roe * V(t, m + 1, ia, ic, d2));
+          if (c1 >= 0) v += o2e * nc_i * (V(t, m, ia, c1, d1) - roe * V(t, m + 1, ia, c1, d1));
+          if (a1 >= 0) v += o2zpe * na_i * V(t, m + 1, a1, ic, d1);
+          V(t, m, ia, ic, id) = v;
+        }
+      }
+    }
+  }
+}
+
+/* Full contracted quartet.  T* are the caller's Cartesian->spherical matrices
+ * (T[icart + isph*ncart]) or NULL for Cartesian output. */
+static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, int iskipa, int na_prim,
+                            int na_cont, int iskipa_cont, const double *ca, const double *Ta,
+                            const double *xb, const double *cB, int lb, int nb, int iskipb, int nb_prim,
+                            int nb_cont, int iskipb_cont, const double *cb, const double *Tb,
+                            const double *xc, const double *cC, int lc, int nc, int iskipc, int nc_prim,
+                            int nc_cont, int iskipc_cont, const double *cc, const double *Tc,
+                            const double *xd, const double *cD, int ld, int nd, int iskipd, int nd_prim,
+                            int nd_cont, int iskipd_cont, const double *cd, const double *Td,
+                            double *out) {
+  init_comp_tab();
+  const double two_pi52 = 2.0 * pow(3.14159265358979323846, 2.5);
+  int lab = la + lb, L = la + lb + lc + ld;
+  int ne = ncum(lab) - ncum(la - 1); /* a range [la, la+lb] */
+  int e0 = ncum(la - 1);
+  int ncc = nc_l(lc), ncd = nc_l(ld);
+  int c0 = ncum(lc - 1), d0 = ncum(ld - 1);
+  int ncont = na_cont * nb_cont * nc_cont * nd_cont;
+  /* contracted [e0|cd]: index ((((ka*nbk+kb)*nck+kc)*ndk+kd)*ne + e)*ncc + c)*ncd + d */
+  size_t nblk = (size_t)ne * ncc * ncd;
+  double *acc = calloc(nblk * ncont, sizeof(double));
+  vtab t;
+  t.L = L;
+  t.na = ncum(lab);
+  t.nc = ncum(lc);
+  t.nd = ncum(ld);
+  t.v = calloc((size_t)(L + 1) * t.na * t.nc * t.nd, sizeof(double));
+  double F[4 * OR_LMAX + 1];
+  double AB[3], CD[3];
+  for (int i = 0; i < 3; ++i) {
+    AB[i] = cA[i] - cB[i];
+    CD[i] = cC[i] - cD[i];
+  }
+  double RAB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+  double RCD2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+  for (int pc = 0; pc < nc_prim; ++pc)
+    for (int pd = 0; pd < nd_prim; ++pd) {
+      double eta = xc[pc] + xd[pd], oeta = 1.0 / eta;
+      double Q[3], QC[3], QD[3];
+      for (int i = 0; i < 3; ++i) {
+        Q[i] = (xc[pc] * cC[i] + xd[pd] * cD[i]) * oeta;
+        QC[i] = Q[i] - cC[i];
+        QD[i] = Q[i] - cD[i];
+      }
+      double xi_cd = xc[pc] * xd[pd] * oeta;
+      for (int pb = 0; pb < nb_prim; ++pb)
+        for (int pa = 0; pa < na_prim; ++pa) {
+          double zeta = xa[pa] + xb[pb], ozeta = 1.0 / zeta;
+          double P[3], PA[3], W[3], WP[3], WQ[3], PQ[3];
+          for (int i = 0; i < 3; ++i) {
+            P[i] = (xa[pa] * cA[i] + xb[pb] * cB[i]) * ozeta;
+            PA[i] = P[i] - cA[i];
+          }
+          double xi_ab = xa[pa] * xb[pb] * ozeta;
+          double ozpe = 1.0 / (zeta + eta);
+          double rho = zeta * eta * ozpe;
+          for (int i = 0; i < 3; ++i) {
+            PQ[i] = P[i] - Q[i];
+            W[i] = (zeta * P[i] + eta * Q[i]) * ozpe;
+            WP[i] = W[i] - P[i];
+            WQ[i] = W[i] - Q[i];
+          }
+          double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+          /* base: 2 pi^{5/2} / (zeta eta sqrt(zeta+eta)) exp(-xi_ab RAB2 - xi_cd RCD2) F_m(rho RPQ2) */
+          oracle_boys(F, 1, 0, L, rho * RPQ2);
+          double pref = two_pi52 * ozeta * oeta * sqrt(ozpe) * exp(-xi_ab * RAB2 - xi_cd * RCD2);
+          for (int m = 0; m <= L; ++m) F[m] *= pref;
+          prim_vrr(&t, lab, lc, ld, F, PA, WP, QC, QD, WQ, 0.5 * ozeta, rho * ozeta, 0.5 * oeta, rho * oeta,
+                   0.5 * ozpe);
+          for (int ka = 0; ka < na_cont; ++ka)
+            for (int kb = 0; kb < nb_cont; ++kb)
+              for (int kc = 0; kc < nc_cont; ++kc)
+                for (int kd = 0; kd < nd_cont; ++kd) {
+                  double w = ca[pa + ka * na_prim] * cb[pb + kb * nb_prim] * cc[pc + kc * nc_prim] *
+                             cd[pd + kd * nd_prim];
+                  double *blk = acc + ((((size_t)ka * nb_cont + kb) * nc_cont + kc) * nd_cont + kd) * nblk;
+                  for (int e = 0; e < ne; ++e)
+                    for (int c = 0; c < ncc; ++c)
+                      for (int d = 0; d < ncd; ++d)
+                        blk[((size_t)e * ncc + c) * ncd + d] += w * V(&t, 0, e0 + e, c0 + c, d0 + d);
+                }
+        }
+    }
+  free(t.v);
+
+  /* HRR a -> b on contracted data, layer by layer in l_b (generator_hrr_function.py:265-436):
+   * direction = x if b_x>0, else y if b_y>0, else z. */
+  int nca = nc_l(la), ncb = nc_l(lb);
+  size_t nout_cart = (size_t)nca * ncb * ncc * ncd;
+  double *cart = malloc(sizeof(double) * nout_cart * ncont); /* index (((a*ncb+b)*ncc+c)*ncd+d) */
+  for (int k = 0; k < ncont; ++k) {
+    const double *blk = acc + (size_t)k * nblk;
+    /* layer j holds (e, b) for |b| = j, e in [la, la+lb-j] (cumulative index offset e0) */
+    double *prev = malloc(sizeof(double) * nblk);
+    memcpy(prev, blk, sizeof(double) * nblk);
+    int prev_ne = ne;
+    for (int j = 1; j <= lb; ++j) {
+      int cur_ne = ncum(lab - j) - ncum(la - 1);
+      int nbj = nc_l(j), nbp = nc_l(j - 1);
+      size_t cur_sz = (size_t)cur_ne * nbj * ncc * ncd;
+      double *cur = malloc(sizeof(double) * cur_sz);
+      for (int ib = 0; ib < nbj; ++ib) {
+        const int *bb = comp_tab[ncum(j - 1) + ib];
+        int i = first_dir(bb);
+        int bm[3] = {bb[0], bb[1], bb[2]};
+        bm[i] -= 1;
+        int ibm = cidx(bm[0], bm[1], bm[2]) - ncum(j - 2);
+        for (int ie = 0; ie < cur_ne; ++ie) {
+          const int *e = comp_tab[e0 + ie];
+          int ep[3] = {e[0], e[1], e[2]};
+          ep[i] += 1;
+          int iep = cidx(ep[0], ep[1], ep[2]) - e0;
+          for (int cdx = 0; cdx < ncc * ncd; ++cdx)
+            cur[((size_t)ie * nbj + ib) * ncc * ncd + cdx] =
+                prev[((size_t)iep * nbp + ibm) * ncc * ncd + cdx] +
+                AB[i] * prev[((size_t)ie * nbp + ibm) * ncc * ncd + cdx];
+        }
+      }
+      free(prev);
+      prev = cur;
+      prev_ne = cur_ne;
+    }
+    (void)prev_ne;
+    /* prev now holds (a, b) with a in level la only (cur_ne == nca) */
+    memcpy(cart + (size_t)k * nout_cart, prev, sizeof(double) * nout_cart);
+    free(prev);
+  }
+  free(acc);
+
+  /* spherical transform of each index with the caller's matrices, then output copy */
+  /* the emitted copy loop runs over the caller's n? components (contracted_general.py:1808-1876) */
+  int oa = na, ob = nb, oc = nc, od = nd;
+  for (int ka = 0; ka < na_cont; ++ka)
+    for (int kb = 0; kb < nb_cont; ++kb)
+      for (int kc = 0; kc < nc_cont; ++kc)
+        for (int kd = 0; kd < nd_cont; ++kd) {
+          int k = ((ka * nb_cont + kb) * nc_cont + kc) * nd_cont + kd;
+          const double *X = cart + (size_t)k * nout_cart;
+          for (int sa = 0; sa < oa; ++sa)
+            for (int sb = 0; sb < ob; ++sb)
+              for (int sc = 0; sc < oc; ++sc)
+                for (int sd = 0; sd < od; ++sd) {
+                  double s = 0.0;
+                  for (int a = 0; a < nca; ++a) {
+                    double wa = Ta ? Ta[a + sa * nca] : (a == sa);
+                    if (wa == 0.0) continue;
+                    for (int b = 0; b < ncb; ++b) {
+                      double wb = Tb ? Tb[b + sb * ncb] : (b == sb);
+                      if (wb == 0.0) continue;
+                      for (int c = 0; c < ncc; ++c) {
+                        double wc = Tc ? Tc[c + sc * ncc] : (c == sc);
+                        if (wc == 0.0) continue;
+                        for (int d = 0; d < ncd; ++d) {
+                          double wd = Td ? Td[d + sd * ncd] : (d == sd);
+                          if (wd == 0.0) continue;
+                          s += wa * wb * wc * wd * X[(((size_t)a * ncb + b) * ncc + c) * ncd + d];
+                        }
+                      }
+                    }
+                  }
+                  out[(size_t)sa * iskipa + (size_t)ka * iskipa_cont + (size_t)sb * iskipb +
+                      (size_t)kb * iskipb_cont + (size_t)sc * iskipc + (size_t)kc * iskipc_cont +
+                      (size_t)sd * iskipd + (size_t)kd * iskipd_cont] = s;
+                }
+        }
+  free(cart);
+}
+
+/* Same argument list as the emitted intception_integral_eri_abcd_m_cont_cart_main */
+void oracle_eri_cont_cart_main(const double *xa, const double cA[3], int la, int na, int iskipa, int na_prim,
+                               int na_cont, int iskipa_cont, const double *ca, const double *xb,
+                               const double cB[3], int lb, int nb, int iskipb, int nb_prim, int nb_cont,
+                               int iskipb_cont, const double *cb, const double *xc, const double cC[3], int lc,
+                               int nc, int iskipc, int nc_prim, int nc_cont, int iskipc_cont, const double *cc,
+                               const double *xd, const double cD[3], int ld, int nd, int iskipd, int nd_prim,
+                               int nd_cont, int iskipd_cont, const double *cd, double *work, double *out) {
+  (void)work;
+  oracle_eri_cont(xa, cA, la, na, iskipa, na_prim, na_cont, iskipa_cont, ca, NULL, xb, cB, lb, nb, iskipb,
+                  nb_prim, nb_cont, iskipb_cont, cb, NULL, xc, cC, lc, nc, iskipc, nc_prim, nc_cont,
+                  iskipc_cont, cc, NULL, xd, cD, ld, nd, iskipd, nd_prim, nd_cont, iskipd_cont, cd, NULL, out);
+}
+
+/* Same argument list as the emitted intception_integral_eri_abcd_m_cont_sph_main */
+void oracle_eri_cont_sph_main(const double *xa, const double cA[3], int la, int na, int iskipa, int na_prim,
+                              int na_cont, int iskipa_cont, const double *ca, const double *Ta,
+                              const double *xb, const double cB[3], int lb, int nb, int iskipb, int nb_prim,
+                              int nb_cont, int iskipb_cont, const double *cb, const double *Tb,
+                              const double *xc, const double cC[3], int lc, int nc, int iskipc, int nc_prim,
+                              int nc_cont, int iskipc_cont, const double *cc, const double *Tc,
+                              const double *xd, const double cD[3], int ld, int nd, int iskipd, int nd_prim,
+                              int nd_cont, int iskipd_cont, const double *cd, const double *Td, double *work,
+                              double *out) {
+  (void)work;
+  oracle_eri_cont(xa, cA, la, na, iskipa, na_prim, na_cont, iskipa_cont, ca, Ta, xb, cB, lb, nb, iskipb,
+                  nb_prim, nb_cont, iskipb_cont, cb, Tb, xc, cC, lc, nc, iskipc, nc_prim, nc_cont, iskipc_cont,
+                  cc, Tc, xd, cD, ld, nd, iskipd, nd_prim, nd_cont, iskipd_cont, cd, Td, out);
+}
+
+/* Batch driver over a shell table (segmented contraction, n_cont = 1).  Each
+ * quartet's block is written at out + out_off[q] with a fastest:
+ * index = ia + na*(ib + nb*(ic + nc*id)).  sphT[l] is the ncart x nsph matrix
+ * for angular momentum l, or sphT == NULL for Cartesian output. */
+void oracle_eri_batch(int nq, const int *quartets, const int *shell_l, const int *shell_k,
+                      const int *shell_ptr, const double *shell_xyz, const double *prim_exp,
+                      const double *prim_coef, const double *const *sphT, const long long *out_off,
+                      double *out) {
+  for (int q = 0; q < nq; ++q) {
+    const int *s = quartets + 4 * q;
+    int l[4], n[4];
+    for (int i = 0; i < 4; ++i) {
+      l[i] = shell_l[s[i]];
+      n[i] = sphT ? 2 * l[i] + 1 : nc_l(l[i]);
+    }
+    int sk[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
+    const double *T[4] = {NULL, NULL, NULL, NULL};
+    if (sphT)
+      for (int i = 0; i < 4; ++i) T[i] = sphT[l[i]];
+    const double *x[4], *c[4], *r[4];
+    for (int i = 0; i < 4; ++i) {
+      x[i] = prim_exp + shell_ptr[s[i]];
+      c[i] = prim_coef + shell_ptr[s[i]];
+      r[i] = shell_xyz + 3 * s[i];
+    }
+    oracle_eri_cont(x[0], r[0], l[0], n[0], sk[0], shell_k[s[0]], 1, 0, c[0], T[0], x[1], r[1], l[1], n[1],
+                    sk[1], shell_k[s[1]], 1, 0, c[1], T[1], x[2], r[2], l[2], n[2], sk[2], shell_k[s[2]], 1, 0,
+                    c[2], T[2], x[3], r[3], l[3], n[3], sk[3], shell_k[s[3]], 1, 0, c[3], T[3],
+                    out + out_off[q]);
+  }
+}

@@ -1,0 +1,152 @@
+"""ctypes access to the CPU oracle and to the reference-emitted C99.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg.  The product (intception_b200) never imports this module.
+
+* ``liberi_oracle.so`` (built from oracle/eri_oracle.c by oracle/Makefile) is the
+  C restatement of the reference's path.  It is built on demand with gcc.
+* ``_ref/libref_eri_{cart,sph}.so`` (built by oracle/gen_ref.py where the
+  reference tree exists) is the reference generator's own emitted C99 plus an
+  OpenMP batch driver.  It may be absent; callers must handle ``None``.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_ORACLE_SO = os.path.join(HERE, '_gen', 'liberi_oracle.so')
+_REF_SO = {v: os.path.join(HERE, '_ref', 'libref_eri_%s.so' % v) for v in ('cart', 'sph')}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_longlong)
+
+_oracle = None
+_ref = {}
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def load_oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(_ORACLE_SO):
+            subprocess.run(['make', '-s', '-C', HERE], check=True)
+        lib = C.CDLL(_ORACLE_SO)
+        lib.oracle_boys.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double]
+        lib.oracle_boys.restype = None
+        lib.oracle_eri_work_array_size.argtypes = [C.c_int] * 12
+        lib.oracle_eri_work_array_size.restype = C.c_int
+        lib.oracle_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp, _dp]
+        lib.oracle_eri_batch.restype = None
+        idx = [C.c_int] * 6
+        per_cart = [_dp, _dp] + idx + [_dp]
+        per_sph = per_cart + [_dp]
+        lib.oracle_eri_cont_cart_main.argtypes = per_cart * 4 + [_dp, _dp]
+        lib.oracle_eri_cont_cart_main.restype = None
+        lib.oracle_eri_cont_sph_main.argtypes = per_sph * 4 + [_dp, _dp]
+        lib.oracle_eri_cont_sph_main.restype = None
+        _oracle = lib
+    return _oracle
+
+
+def load_ref(variant):
+    """The reference-emitted C99 for 'cart' or 'sph', or None if not built."""
+    if variant not in _ref:
+        path = _REF_SO[variant]
+        if not os.path.exists(path):
+            _ref[variant] = None
+        else:
+            lib = C.CDLL(path)
+            lib.ref_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp,
+                                          _dp, C.c_int]
+            lib.ref_eri_batch.restype = C.c_int
+            lib.ref_work_array_size.argtypes = [C.c_int] * 12
+            lib.ref_work_array_size.restype = C.c_int
+            main = getattr(lib, 'intception_integral_eri_abcd_m_cont_%s_main' % variant)
+            idx = [C.c_int] * 6
+            per = [_dp, _dp] + idx + [_dp] + ([_dp] if variant == 'sph' else [])
+            main.argtypes = per * 4 + [_dp, _dp]
+            main.restype = None
+            lib.intception_boys.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double]
+            lib.intception_boys.restype = None
+            _ref[variant] = lib
+    return _ref[variant]
+
+
+def boys(nmax, x, lib=None):
+    lib = lib or load_oracle()
+    f = np.zeros(nmax + 1)
+    fn = lib.oracle_boys if hasattr(lib, 'oracle_boys') else lib.intception_boys
+    fn(_ptr(f), 1, 0, nmax, float(x))
+    return f
+
+
+def _sph_table(sphT, lmax=6):
+    keep = [np.ascontiguousarray(np.asarray(T, dtype=np.float64).ravel(order='F')) for T in sphT]
+    arr = (_dp * len(keep))(*[_ptr(k) for k in keep])
+    return arr, keep
+
+
+def _batch_args(b):
+    q = np.ascontiguousarray(b.quartets, dtype=np.int32)
+    sl = np.ascontiguousarray(b.shell_l, dtype=np.int32)
+    sk = np.ascontiguousarray(b.shell_k, dtype=np.int32)
+    sp = np.ascontiguousarray(b.shell_ptr, dtype=np.int32)
+    xyz = np.ascontiguousarray(b.shell_xyz, dtype=np.float64)
+    e = np.ascontiguousarray(b.prim_exp, dtype=np.float64)
+    c = np.ascontiguousarray(b.prim_coef, dtype=np.float64)
+    off = np.ascontiguousarray(b.out_off, dtype=np.int64)
+    return q, sl, sk, sp, xyz, e, c, off
+
+
+def oracle_batch(b, sphT=None):
+    """Evaluate a ShellBatch with the C restatement (single thread)."""
+    lib = load_oracle()
+    q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
+    out = np.zeros(b.out_size)
+    tab, keep = _sph_table(sphT) if b.spherical else (None, None)
+    lib.oracle_eri_batch(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz),
+                         _ptr(e), _ptr(c), tab, _ptr(off, _lp), _ptr(out))
+    return out
+
+
+def ref_batch(b, sphT=None, nthreads=0, out=None):
+    """Evaluate a ShellBatch with the reference-emitted C99 (OpenMP).  Returns
+    None when oracle/_ref was not built."""
+    lib = load_ref('sph' if b.spherical else 'cart')
+    if lib is None:
+        return None
+    q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
+    if out is None:
+        out = np.zeros(b.out_size)
+    tab, keep = _sph_table(sphT) if b.spherical else (None, None)
+    lib.ref_eri_batch(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz), _ptr(e),
+                      _ptr(c), tab, _ptr(off, _lp), _ptr(out), int(nthreads))
+    return out
+
+
+def call_main(lib, variant, shells, work, out, prefix=None):
+    """Call a per-quartet main (oracle or reference) with the emitted argument
+    list.  shells: four dicts with keys x, cen, l, n, iskip, nprim, ncont,
+    iskip_cont, coef and (sph) T."""
+    fn = getattr(lib, prefix or ('intception_integral_eri_abcd_m_cont_%s_main' % variant))
+    args = []
+    keep = []
+    for s in shells:
+        x = np.ascontiguousarray(s['x'], dtype=np.float64)
+        cen = np.ascontiguousarray(s['cen'], dtype=np.float64)
+        coef = np.ascontiguousarray(s['coef'], dtype=np.float64)
+        keep += [x, cen, coef]
+        args += [_ptr(x), _ptr(cen), s['l'], s['n'], s['iskip'], s['nprim'], s['ncont'], s['iskip_cont'],
+                 _ptr(coef)]
+        if variant == 'sph':
+            T = np.ascontiguousarray(np.asarray(s['T'], dtype=np.float64).ravel(order='F'))
+            keep.append(T)
+            args.append(_ptr(T))
+    fn(*args, _ptr(work), _ptr(out))
+    return out

@@ -1,0 +1,132 @@
+"""CUDA path parity: the drop-ins and the batch API against the reference's
+emitted C99 (golden fixtures) and the oracle, on a B200."""
+import numpy as np
+import pytest
+
+from conftest import BATCH_FIXTURES, load_batch, load_dropin_cases, tolerance, GOLDEN
+from intception_b200 import basis, eri
+from oracle import loader
+
+pytestmark = pytest.mark.gpu
+
+
+def run_batch(b, **kw):
+    import torch
+    eng = eri.EriEngine(b)
+    out = eng.compute(**kw)
+    torch.cuda.synchronize()
+    assert eng.device_status() == 0
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize('name', BATCH_FIXTURES)
+def test_batch_matches_reference_golden(name):
+    b, T, ref = load_batch(name)
+    out = run_batch(b)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+@pytest.mark.parametrize('k', range(12))
+def test_dropin_matches_reference_golden(k):
+    shells, ref, sph = load_dropin_cases()[k]
+    out = np.full(ref.shape, -7.0)
+    (eri.cont_sph_main if sph else eri.cont_cart_main)(shells, out)
+    assert np.array_equal(out == -7.0, ref == -7.0)  # elements outside the strided block untouched
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+@pytest.mark.parametrize('sph', [False, True])
+def test_every_l2_class_vs_oracle(sph):
+    """All 81 (la,lb,lc,ld) orderings with l <= 2, i.e. every canonical class
+    reached through every permutation of shells and strides."""
+    rng = np.random.default_rng(31 + sph)
+    quartets = []
+    ls = []
+    for la in range(3):
+        for lb in range(3):
+            for lc in range(3):
+                for ld in range(3):
+                    base = len(ls)
+                    ls += [la, lb, lc, ld]
+                    quartets.append([base, base + 1, base + 2, base + 3])
+    ks = rng.integers(1, 5, len(ls)).astype(np.int32)
+    l_, k_, p_, xyz, e, c = basis.make_shells(rng, np.array(ls, np.int32), ks, 0.1, 40.0, 3.0)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    b = basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    out = run_batch(b)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+def test_boys_dropin_vs_reference():
+    z = np.load(GOLDEN + '/boys.npz')
+    nmax = int(z['nmax'])
+    for x, F in zip(z['x'], z['F']):
+        f = eri.boys(nmax, x)
+        # the reference drops exp(-x) above x = 35; both are below 1e-14 there
+        assert np.abs(f - F).max() <= 2e-14, x
+
+
+def test_boys_batch_accuracy():
+    import torch
+    from oracle import md_eri
+    xs = np.concatenate([np.linspace(0, 40, 801), [1e-13, 35.999, 36.0, 36.001, 60.0, 500.0]])
+    nmax = 16
+    x = torch.tensor(xs, dtype=torch.float64, device='cuda')
+    f = torch.empty(len(xs) * (nmax + 1), dtype=torch.float64, device='cuda')
+    lib = eri.load()
+    st = lib.intception_b200_boys_batch(x.data_ptr(), len(xs), nmax, f.data_ptr(), None)
+    assert st == 0
+    lib.intception_b200_synchronize()
+    torch.cuda.synchronize()
+    f = f.cpu().numpy().reshape(len(xs), nmax + 1)
+    ex = np.array([[md_eri.boys(m, v) for m in range(nmax + 1)] for v in xs])
+    assert np.abs(f - ex).max() < 5e-15
+
+
+def test_dropin_rejects_bad_l_and_n():
+    shells, ref, sph = load_dropin_cases()[0]
+    bad = [dict(s) for s in shells]
+    bad[0]['l'] = 7
+    out = np.full(ref.shape, -7.0)
+    with pytest.raises(eri.IntceptionError):
+        eri.cont_cart_main(bad, out)
+    assert np.all(out == -7.0)
+    bad = [dict(s) for s in shells]
+    bad[2]['n'] = bad[2]['n'] + 1
+    with pytest.raises(eri.IntceptionError):
+        eri.cont_cart_main(bad, out)
+    assert np.all(out == -7.0)
+    # a good call afterwards still works
+    eri.cont_cart_main(shells, out)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+def test_batch_reports_l_above_basis_lmax():
+    import torch
+    b, T, ref = load_batch('pppp_k3_cart')
+    eng = eri.EriEngine(b)
+    eng._basis.lmax = 0  # declared lmax below the shells' l
+    eng.compute()
+    torch.cuda.synchronize()
+    assert eng.device_status() == eri.IB_ERR_ARG
+
+
+def test_permutational_symmetry_large():
+    """(ab|cd) = (ba|cd) = (cd|ab) through different canonicalisation paths,
+    at 100k quartets of the l<=2 spherical workload."""
+    b = basis.config_mixed_l2(nq=100_000, seed=17, spherical=True)
+    out = run_batch(b)
+    q2 = b.quartets[:, [2, 3, 0, 1]].copy()
+    b2 = basis.ShellBatch(b.shell_l, b.shell_k, b.shell_ptr, b.shell_xyz, b.prim_exp, b.prim_coef, q2,
+                          *basis.packed_offsets(b.shell_l, q2, True)[:1], True, b.out_size)
+    out2 = run_batch(b2)
+    # compare block by block: (cd|ab)[ic,id,ia,ib] == (ab|cd)[ia,ib,ic,id]
+    ls = b.shell_l[b.quartets]
+    n = 2 * ls + 1
+    for q in range(0, b.nq, 997):
+        na, nb, nc, nd = n[q]
+        x = out[b.out_off[q]:b.out_off[q] + na * nb * nc * nd].reshape(nd, nc, nb, na)
+        y = out2[b2.out_off[q]:b2.out_off[q] + na * nb * nc * nd].reshape(nb, na, nd, nc)
+        assert np.abs(x - y.transpose(2, 3, 0, 1)).max() <= 1e-13 * max(1.0, np.abs(x).max())

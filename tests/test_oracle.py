@@ -1,0 +1,84 @@
+"""The CPU oracle (C restatement of the reference's ERI path) against the
+reference's own emitted C99: golden fixtures, live comparison when oracle/_ref
+is built, and an independent McMurchie-Davidson cross-check."""
+import numpy as np
+import pytest
+
+from conftest import BATCH_FIXTURES, load_batch, load_dropin_cases, tolerance, GOLDEN
+from intception_b200 import basis
+from oracle import loader, md_eri
+
+
+@pytest.mark.parametrize('name', BATCH_FIXTURES)
+def test_oracle_matches_golden(name):
+    b, T, ref = load_batch(name)
+    out = loader.oracle_batch(b, T)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+@pytest.mark.parametrize('k', range(12))
+def test_oracle_dropin_cases(k):
+    shells, ref, sph = load_dropin_cases()[k]
+    out = np.full(ref.shape, -7.0)
+    lib = loader.load_oracle()
+    loader.call_main(lib, 'sph' if sph else 'cart', shells, np.zeros(1), out,
+                     prefix='oracle_eri_cont_%s_main' % ('sph' if sph else 'cart'))
+    assert np.array_equal(out == -7.0, ref == -7.0)  # same untouched elements
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+def test_oracle_boys_golden():
+    """Same scheme as the reference; the tables are recomputed with mpmath, so
+    only their last-digit rounding may differ."""
+    z = np.load(GOLDEN + '/boys.npz')
+    for x, F in zip(z['x'], z['F']):
+        assert np.abs(loader.boys(int(z['nmax']), x) - F).max() <= 1e-15
+
+
+def test_oracle_work_array_size_golden():
+    t = np.load(GOLDEN + '/work_array_size.npz')['table']
+    lib = loader.load_oracle()
+    got = np.array([lib.oracle_eri_work_array_size(*map(int, r[:12])) for r in t])
+    assert np.array_equal(got, t[:, 12])
+
+
+def test_oracle_boys_accuracy():
+    """The reference's Boys scheme against scipy's incomplete gamma."""
+    for x in (0.0, 0.3, 3.7, 12.2, 15.05, 29.3, 40.0, 300.0):
+        f = loader.boys(12, x)
+        ex = np.array([md_eri.boys(m, x) for m in range(13)])
+        assert np.abs(f - ex).max() < 2e-14
+
+
+@pytest.mark.parametrize('ls', [(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 1, 1), (2, 1, 0, 1), (0, 2, 2, 1), (2, 2, 1, 1)])
+def test_oracle_vs_mcmurchie_davidson(ls):
+    rng = np.random.default_rng(sum(ls) * 7 + 3)
+    shells = []
+    for l in ls:
+        k = 2
+        x = np.exp(rng.uniform(np.log(0.2), np.log(8.0), k))
+        c = basis.normalize_shell(l, x, rng.uniform(0.2, 1.0, k))
+        shells.append((l, x, c, rng.uniform(0.0, 2.5, 3)))
+    ref = md_eri.contracted_eri(shells)
+    ls_ = np.array(ls, np.int32)
+    ks = np.full(4, 2, np.int32)
+    ptr = np.arange(4, dtype=np.int32) * 2
+    xyz = np.array([s[3] for s in shells])
+    e = np.concatenate([s[1] for s in shells])
+    c = np.concatenate([s[2] for s in shells])
+    q = np.array([[0, 1, 2, 3]], np.int32)
+    off, total = basis.packed_offsets(ls_, q, False)
+    b = basis.ShellBatch(ls_, ks, ptr, xyz, e, c, q, off, False, total)
+    out = loader.oracle_batch(b)
+    assert np.abs(out - ref).max() < 1e-13 * max(1.0, np.abs(ref).max())
+
+
+def test_oracle_vs_reference_live():
+    """Fresh seeded inputs through both the restatement and the emitted C99."""
+    if loader.load_ref('cart') is None:
+        pytest.skip('oracle/_ref not built here')
+    T = basis.sph_matrices(6)
+    for sph in (False, True):
+        b = basis.independent_quartet_batch(123, 50, [0, 1, 2, 3], [1, 2, 3], 0.1, 60.0, 5.0, sph)
+        ref = loader.ref_batch(b, T)
+        assert np.abs(loader.oracle_batch(b, T) - ref).max() <= tolerance(ref)
