@@ -122,7 +122,8 @@ typedef struct {
  * matrices, m = -l..l) or (l+1)(l+2)/2 (Cartesian).  bounds (device, [nq],
  * may be NULL for IB_PREC_FP64) is a per-quartet magnitude bound, e.g. a
  * Schwarz product.  Asynchronous on stream (a cudaStream_t; NULL = the
- * library stream). */
+ * legacy default stream).  Work buffers are reused between calls: calls on
+ * different streams must be ordered by the caller. */
 int intception_b200_eri_batch(const intception_b200_basis *basis, const int *quartets, const long long *out_off,
                               int nq, int spherical, int precision, const double *bounds, double threshold,
                               double *out, void *stream);
@@ -130,15 +131,16 @@ int intception_b200_eri_batch(const intception_b200_basis *basis, const int *qua
 /* Number of library kernels the last intception_b200_eri_batch launched. */
 int intception_b200_last_launch_count(void);
 
-/* Waits for the library stream and returns the device status word of the last
- * batch (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
+/* Waits for the device and returns the device status word of the last batch
+ * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
 int intception_b200_batch_status(void);
 
 /* The library's Cartesian->spherical matrix for l (host memory,
  * T[icart + isph*ncart], ncart x (2l+1)). */
 int intception_b200_sph_matrix(int l, double *T);
 
-/* F_m(x[i]) for m = 0..nmax into f[i*(nmax+1) + m]; device pointers. */
+/* F_m(x[i]) for m = 0..nmax into f[i*(nmax+1) + m]; device pointers; NULL
+ * stream = the legacy default stream. */
 int intception_b200_boys_batch(const double *x, int n, int nmax, double *f, void *stream);
 
 /* Block until the library stream is idle. */

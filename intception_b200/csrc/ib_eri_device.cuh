@@ -45,6 +45,20 @@ struct IbLaunch {
   int* status;             // device error word (0 = ok)
 };
 
+// Per-lane constants of a lane-group kernel: the lane's Cartesian component,
+// its base-chain path (direction and the exponent before each step), and the
+// lanes owning component - 1x, - 1y, - 1z inside the group.
+struct IbLaneInfo {
+  unsigned char c[3];
+  unsigned char len;
+  unsigned char dir[8];
+  unsigned char nb[8];
+  unsigned char src[3];
+};
+
+// Barrier over the 64 threads of two-warp group g of the block (named barrier g+1).
+__device__ __forceinline__ void ib_group_bar(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
+
 typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch& a);
 typedef int (*IbOccFn)(int variant);
 struct IbClassEntry {
@@ -59,12 +73,18 @@ __host__ inline size_t ib_boys_smem_bytes() {
   return sizeof(double) * IB_BOYS_NPTS * IB_BOYS_TAYLOR;
 }
 
+// 1/k! for k = 0..6 without a local array (a runtime-indexed array would live on the stack).
+__device__ __forceinline__ double ib_invfact(int k) {
+  double r = 1.0;
+  for (int i = 2; i <= k; ++i) r /= (double)i;
+  return r;
+}
+
 // Stage the Taylor coefficients g_k = F_{L+k}(T_i)/k! for k = 0..6 of every grid point.
 __device__ __forceinline__ void ib_stage_boys(double* __restrict__ s, const double* __restrict__ tab, int L) {
-  const double invfact[IB_BOYS_TAYLOR] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
   for (int idx = threadIdx.x; idx < IB_BOYS_NPTS * IB_BOYS_TAYLOR; idx += blockDim.x) {
     const int i = idx / IB_BOYS_TAYLOR, k = idx - i * IB_BOYS_TAYLOR;
-    s[idx] = __ldg(tab + i * IB_BOYS_NCOL + L + k) * invfact[k];
+    s[idx] = __ldg(tab + i * IB_BOYS_NCOL + L + k) * ib_invfact(k);
   }
 }
 
@@ -101,9 +121,13 @@ __device__ inline void ib_boys_rt(double T, int L, const double* __restrict__ ta
     const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
     const double dx = (double)i * (1.0 / IB_BOYS_H_INV) - T;
     const double* r = tab + i * IB_BOYS_NCOL + L;
-    const double invfact[IB_BOYS_TAYLOR] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
-    double f = r[6] * invfact[6];
-    for (int k = 5; k >= 0; --k) f = fma(f, dx, r[k] * invfact[k]);
+    double f = r[6] * (1.0 / 720.0);
+    f = fma(f, dx, r[5] * (1.0 / 120.0));
+    f = fma(f, dx, r[4] * (1.0 / 24.0));
+    f = fma(f, dx, r[3] * (1.0 / 6.0));
+    f = fma(f, dx, r[2] * 0.5);
+    f = fma(f, dx, r[1]);
+    f = fma(f, dx, r[0]);
     F[L] = f;
     const double e = exp(-T), t2 = T + T;
     for (int m = L - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) / (double)(2 * m + 1);

@@ -649,8 +649,10 @@ void build_sph_host(std::vector<double>& out) {
 }
 
 namespace {
+// The caller's stream; NULL is the legacy default stream (CUDA's convention).
 int resolve_stream(Context* c, void* stream, cudaStream_t* s) {
-  *s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  (void)c;
+  *s = static_cast<cudaStream_t>(stream);
   return IB_OK;
 }
 }  // namespace
@@ -834,7 +836,7 @@ int intception_b200_batch_status(void) {
   int st = get_context(&c);
   if (st) return st;
   int h = 0;
-  IB_CUDA(cudaStreamSynchronize(c->stream));
+  IB_CUDA(cudaDeviceSynchronize());
   IB_CUDA(cudaMemcpy(&h, c->status.p, sizeof(int), cudaMemcpyDeviceToHost));
   return h;
 }

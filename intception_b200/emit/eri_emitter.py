@@ -35,6 +35,9 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from intception_b200.basis import sph_matrix  # noqa: E402
 
 LMAX_EMIT = 2  # classes with every l <= LMAX_EMIT get an unrolled kernel
+# classes kept on the one-thread-per-quartet kernel (everything else whose
+# smaller side fits a warp uses the lane-group kernel of group_emitter.py)
+THREAD_CLASSES = set()
 
 DIRS = 'xyz'
 
@@ -408,9 +411,17 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=6):
     os.makedirs(outdir, exist_ok=True)
     classes = canonical_classes(lmax)
     # balance translation units by emitted size (largest classes first)
+    from .group_emitter import GroupEmitter, orientation
     bodies = []
     for c in classes:
-        body, st = Emitter(*c).kernel()
+        # the one-thread schedule's counts are the algorithmic work of the class
+        tbody, st = Emitter(*c).kernel()
+        if orientation(*c) is not None and c not in THREAD_CLASSES:
+            body, gst = GroupEmitter(*c).kernel()
+            st.update(kind='group', G=gst['G'], orient=gst['orient'], lane_flops=gst['lane_flops'])
+        else:
+            body = tbody
+            st['kind'] = 'thread'
         bodies.append((c, body, st))
     order = sorted(bodies, key=lambda x: -len(x[1]))
     groups = [[] for _ in range(ngroups)]
@@ -449,8 +460,7 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=6):
     stats = [b[2] for b in bodies]
     with open(os.path.join(outdir, 'class_stats.txt'), 'w') as fh:
         for st in stats:
-            fh.write('%(tag)s cid=%(cid)d nodes=%(nodes)d vrr_flops=%(vrr_flops)d hrr_flops=%(hrr_flops)d '
-                     'nacc=%(nacc)d\n' % st)
+            fh.write(' '.join('%s=%s' % kv for kv in sorted(st.items())) + '\n')
     return stats
 
 

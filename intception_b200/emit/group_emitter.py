@@ -1,0 +1,497 @@
+"""Lane-group ERI kernels: G lanes share one contracted quartet.
+
+Each lane of a group owns one Cartesian component s of the "lane side" (the bra
+e-range or the ket f-range, whichever has fewer components) and computes, per
+primitive quartet, the whole recurrence for the other ("chain") side for that
+component in registers:
+
+  base chain   [s|0]^(m): the lane's own component built from [0|0]^(m) along a
+               path that takes all z steps, then y, then x, so the two-back
+               term of the Obara-Saika recurrence is always the lane's previous
+               chain element (no communication);
+  chain side   [s|c+1i]^(m) = X_i [s|c]^(m) + W_i [s|c]^(m+1)
+                              + c_i/2x ([s|c-1i]^(m) - r [s|c-1i]^(m+1))
+                              + s_i/2(zeta+eta) [s-1i|c]^(m+1)
+               where the last (electron-transfer) term is the same register of
+               the lane that owns s-1i, fetched with __shfl_sync.  The direction
+               i depends only on c, so the instruction stream is uniform across
+               the group; only s_i and the source lane differ per lane.
+  contraction  acc[c] += [s|c]^(0) over the chain-side targets, FP64.
+
+After the primitive loops the group writes its accumulators to shared memory
+as [e][f], runs the bra HRR (lanes over f), the spherical transform of a and b,
+the ket HRR (lanes over ab), the spherical transform of c and d, and stores.
+
+With the bra as lane side the recurrences are the input script's vrra (base
+chain) and vrrc (chain side, transfer term from the bra); with the ket as lane
+side they are the mirror images (vrrc as base chain, the bra recurrence with
+its transfer term 1/2(zeta+eta) f_i [e|f-1i]^(m+1) as chain side).
+"""
+import itertools
+
+from .eri_emitter import comps, comps_range, class_id, sub, add, ZERO, DIRS
+
+try:
+    from intception_b200.basis import sph_matrix
+except ImportError:  # pragma: no cover
+    from ..basis import sph_matrix
+
+
+def ncum(l):
+    return 0 if l < 0 else (l + 1) * (l + 2) * (l + 3) // 6
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def cidx(c):
+    l = sum(c)
+    return ncum(l - 1) + c[2] + (c[1] + c[2]) * (c[1] + c[2] + 1) // 2
+
+
+def orientation(la, lb, lc, ld):
+    """'bra' if the lanes own bra components, 'ket' otherwise; None when
+    neither side fits a 64-lane (two-warp) group."""
+    ne, nf = ncum(la + lb), ncum(lc + ld)
+    if min(ne, nf) > 64:
+        return None
+    return 'bra' if ne <= nf else 'ket'
+
+
+def group_size(n):
+    g = 1
+    while g < n:
+        g *= 2
+    return g
+
+
+class GroupEmitter:
+    def __init__(self, la, lb, lc, ld):
+        self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
+        self.L = la + lb + lc + ld
+        self.E, self.F = la + lb, lc + ld
+        self.orient = orientation(la, lb, lc, ld)
+        assert self.orient is not None
+        if self.orient == 'bra':
+            self.S_lo, self.S_hi, self.C_lo, self.C_hi = la, self.E, lc, self.F
+        else:
+            self.S_lo, self.S_hi, self.C_lo, self.C_hi = lc, self.F, la, self.E
+        self.NL = ncum(self.S_hi)
+        self.G = group_size(self.NL)
+        # G = 64: two warps per quartet; transfer operands go through shared
+        # memory, one named barrier per recurrence level
+        self.wide = self.G > 32
+        self.QPW = max(1, 32 // self.G)
+        self.tag = '%d%d%d%d' % (la, lb, lc, ld)
+        self.cid = class_id(la, lb, lc, ld)
+        self.lines = []
+        self.nodes = {}
+        self.nvar = 0
+        self.flops = 0
+        self.mult = {}
+
+    # -------------------------------------------------------------- lane table
+    def lane_table(self):
+        rows = []
+        for j in range(self.G):
+            jj = min(j, self.NL - 1)  # padding lanes mirror the last component
+            c = comps_range(0, self.S_hi)[jj]
+            dirs, nbs = [], []
+            for d in (2, 1, 0):
+                for k in range(c[d]):
+                    dirs.append(d)
+                    nbs.append(k)
+            src = []
+            for d in range(3):
+                src.append(cidx(sub(c, d)) if c[d] > 0 else jj)
+            rows.append((c, dirs, nbs, src))
+        return rows
+
+    # -------------------------------------------------------------- chain DAG
+    def _new(self, expr, fl):
+        name = 'v%d' % self.nvar
+        self.nvar += 1
+        self.lines.append('        const R %s = %s;' % (name, expr))
+        self.flops += fl
+        return name
+
+    def _m(self, base, k):
+        if k == 1:
+            return base
+        key = (base, k)
+        if key not in self.mult:
+            self.mult[key] = '%s_%d' % (base, k)
+        return self.mult[key]
+
+    def node(self, c, m):
+        key = (c, m)
+        if key in self.nodes:
+            return self.nodes[key]
+        if c == ZERO:
+            name = 'b%d' % m
+            self.nodes[key] = name
+            return name
+        i = 0 if c[0] > 0 else (1 if c[1] > 0 else 2)
+        cm = sub(c, i)
+        d = DIRS[i]
+        a0 = self.node(cm, m)
+        a1 = self.node(cm, m + 1)
+        expr = 'CX%s * %s + CW%s * %s' % (d, a0, d, a1)
+        fl = 3
+        if cm[i] > 0:
+            c2 = sub(cm, i)
+            b0 = self.node(c2, m)
+            b1 = self.node(c2, m + 1)
+            expr += ' + %s * (%s - cro * %s)' % (self._m('co2', cm[i]), b0, b1)
+            fl += 4
+        if self.S_hi > 0:
+            # transfer term from the lane owning s - 1i
+            if self.wide:
+                lvl = sum(cm)
+                slot = self.slot_index(cm, m + 1)
+                expr += ' + tf%s * xb%d[%d * 64 + src%s]' % (d, lvl % 2, slot, 'xyz'.index(d))
+            else:
+                expr += ' + tf%s * __shfl_sync(gmask, %s, src%s, %d)' % (d, a1, 'xyz'.index(d), self.G)
+            fl += 2
+        name = self._new(expr, fl)
+        self.nodes[key] = name
+        return name
+
+    def slot_index(self, c, m):
+        """Position of chain node (c, m), m >= 1, in its level's transfer buffer."""
+        k = sum(c)
+        order = [(cc, mm) for cc in comps(k) for mm in range(1, self.C_hi - k + 1)]
+        return order.index((c, m))
+
+    def n_slots(self):
+        return max(len(comps(k)) * (self.C_hi - k) for k in range(self.C_hi + 1))
+
+    def emit_chain_wide(self):
+        """Level-ordered chain for two-warp groups: compute level k, publish its
+        m >= 1 values to shared memory, barrier, continue."""
+        targets = comps_range(self.C_lo, self.C_hi)
+        for c in targets:
+            self.node(c, 0)
+        byname = {}
+        for (c, m), name in self.nodes.items():
+            byname[name] = (c, m)
+        level_lines = {}
+        # self.lines were appended in DFS order; regroup by level
+        for ln in self.lines:
+            name = ln.split('const R ')[1].split(' =')[0]
+            c, m = byname[name]
+            level_lines.setdefault(sum(c), []).append(ln)
+        out = ['        ib_group_bar(gid);']
+        if ZERO in targets:
+            out.append('        acc[%d] += (double)b0;' % targets.index(ZERO))
+        # level 0: base values
+        for mm in range(1, self.C_hi + 1):
+            if ((0, 0, 0), mm) in self.nodes:
+                out.append('        xb0[%d * 64 + j] = b%d;' % (self.slot_index(ZERO, mm), mm))
+        out.append('        ib_group_bar(gid);')
+        t_index = {c: t for t, c in enumerate(targets)}
+        for k in range(1, self.C_hi + 1):
+            out += level_lines.get(k, [])
+            for c in comps(k):
+                if (c, 0) in self.nodes and c in t_index:
+                    out.append('        acc[%d] += (double)%s;' % (t_index[c], self.nodes[(c, 0)]))
+                    self.flops += 1
+            if k < self.C_hi:
+                for c in comps(k):
+                    for mm in range(1, self.C_hi - k + 1):
+                        if (c, mm) in self.nodes:
+                            out.append('        xb%d[%d * 64 + j] = %s;' % (k % 2, self.slot_index(c, mm),
+                                                                         self.nodes[(c, mm)]))
+                out.append('        ib_group_bar(gid);')
+        defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
+        return defs + out, len(targets)
+
+    def emit_chain(self):
+        if self.wide:
+            return self.emit_chain_wide()
+        targets = comps_range(self.C_lo, self.C_hi)
+        out = []
+        acc = []
+        for t, c in enumerate(targets):
+            v = self.node(c, 0)
+            acc.append((len(self.lines), '        acc[%d] += (double)%s;' % (t, v)))
+            self.flops += 1
+        pos = 0
+        for at, line in acc:
+            out += self.lines[pos:at]
+            out.append(line)
+            pos = at
+        out += self.lines[pos:]
+        defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
+        return defs + out, len(targets)
+
+    # -------------------------------------------------------------- HRR pieces
+    @staticmethod
+    def _hrr(targets_a, targets_b, leaf, rvec, prefix, lines, counter):
+        memo = {}
+
+        def get(a, b):
+            if b == ZERO:
+                return leaf(a)
+            if (a, b) in memo:
+                return memo[(a, b)]
+            i = 0 if b[0] > 0 else (1 if b[1] > 0 else 2)
+            x1 = get(add(a, i), sub(b, i))
+            x2 = get(a, sub(b, i))
+            name = '%s%d' % (prefix, counter[0])
+            counter[0] += 1
+            lines.append('      const double %s = %s + %s%s * %s;' % (name, x1, rvec, DIRS[i], x2))
+            memo[(a, b)] = name
+            return name
+
+        return {(a, b): get(a, b) for a in targets_a for b in targets_b}
+
+    @staticmethod
+    def _sph2(vals, l1, l2, prefix, lines):
+        """vals[(i1, i2)] Cartesian names -> spherical names over both indices."""
+        T1, T2 = sph_matrix(l1), sph_matrix(l2)
+        n1, n2 = ncart(l1), ncart(l2)
+        mid = {}
+        for s1 in range(2 * l1 + 1):
+            for i2 in range(n2):
+                terms = []
+                for i1 in range(n1):
+                    cf = T1[i1, s1]
+                    if abs(cf) > 1e-15:
+                        terms.append(vals[(i1, i2)] if abs(cf - 1) < 1e-15 else '%.17g * %s' % (cf, vals[(i1, i2)]))
+                name = '%sm%d_%d' % (prefix, s1, i2)
+                lines.append('      const double %s = %s;' % (name, ' + '.join(terms) if terms else '0.0'))
+                mid[(s1, i2)] = name
+        out = {}
+        for s1 in range(2 * l1 + 1):
+            for s2 in range(2 * l2 + 1):
+                terms = []
+                for i2 in range(n2):
+                    cf = T2[i2, s2]
+                    if abs(cf) > 1e-15:
+                        terms.append(mid[(s1, i2)] if abs(cf - 1) < 1e-15 else '%.17g * %s' % (cf, mid[(s1, i2)]))
+                name = '%ss%d_%d' % (prefix, s1, s2)
+                lines.append('      const double %s = %s;' % (name, ' + '.join(terms) if terms else '0.0'))
+                out[(s1, s2)] = name
+        return out
+
+    def emit_epilogue(self, sph):
+        la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
+        A, B, Cc, D = comps(la), comps(lb), comps(lc), comps(ld)
+        Elist = comps_range(la, self.E)
+        Flist = comps_range(lc, self.F)
+        NE, NF = len(Elist), len(Flist)
+        e_index = {e: i for i, e in enumerate(Elist)}
+        f_index = {f: i for i, f in enumerate(Flist)}
+        na = (2 * la + 1) if sph else len(A)
+        nb = (2 * lb + 1) if sph else len(B)
+        nc = (2 * lc + 1) if sph else len(Cc)
+        nd = (2 * ld + 1) if sph else len(D)
+        L = []
+        # bra HRR, lanes over f
+        L.append('    for (int t = j; t < %d; t += %d) {' % (NF, self.G))
+        for e in range(NE):
+            L.append('      const double q%d = sb[%d * %d + t];' % (e, e, NF))
+        cnt = [0]
+        body = []
+        res = self._hrr(A, B, lambda a: 'q%d' % e_index[a], 'AB', 'h', body, cnt)
+        L += body
+        if sph:
+            vals = {(A.index(a), B.index(b)): res[(a, b)] for a in A for b in B}
+            body = []
+            sres = self._sph2(vals, la, lb, 'sa', body)
+            L += body
+            outs = [sres[(i, k)] for i in range(na) for k in range(nb)]
+        else:
+            outs = [res[(a, b)] for a in A for b in B]
+        for u, name in enumerate(outs):
+            L.append('      sb[%d * %d + t] = %s;' % (u, NF, name))
+        L.append('    }')
+        L.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        # ket HRR, lanes over ab
+        NAB = na * nb
+        L.append('    for (int u = j; u < %d; u += %d) {' % (NAB, self.G))
+        for f in range(NF):
+            L.append('      const double w%d = sb[u * %d + %d];' % (f, NF, f))
+        body = []
+        cnt = [0]
+        res = self._hrr(Cc, D, lambda c: 'w%d' % f_index[c], 'CD', 'k', body, cnt)
+        L += body
+        if sph:
+            vals = {(Cc.index(c), D.index(d)): res[(c, d)] for c in Cc for d in D}
+            body = []
+            sres = self._sph2(vals, lc, ld, 'sc', body)
+            L += body
+            cd = {(i, k): sres[(i, k)] for i in range(nc) for k in range(nd)}
+        else:
+            cd = {(Cc.index(c), D.index(d)): res[(c, d)] for c in Cc for d in D}
+        L.append('      double* __restrict__ ou = o + (long long)(u / %d) * g.st[0] + (long long)(u %% %d) * g.st[1];'
+                 % (nb, nb))
+        for (i, k), name in cd.items():
+            off = ' + '.join(x for x in (('%d * g.st[2]' % i) if i else '', ('%d * g.st[3]' % k) if k else '') if x)
+            L.append('      ou[%s] = %s;' % (off or '0', name))
+        L.append('    }')
+        return L, max(NE, len(A) * len(B)) * NF
+
+    # -------------------------------------------------------------- kernel
+    def kernel(self):
+        chain, NT = self.emit_chain()
+        epi_cart, sm_cart = self.emit_epilogue(False)
+        epi_sph, sm_sph = self.emit_epilogue(True)
+        smem_group = max(sm_cart, sm_sph)
+        t = self.tag
+        bra = self.orient == 'bra'
+        Elist = comps_range(self.la, self.E)
+        Flist = comps_range(self.lc, self.F)
+        NE, NF = len(Elist), len(Flist)
+        s_lo_idx = ncum(self.S_lo - 1)
+        rows = self.lane_table()
+        src = []
+        # lane table
+        src.append('// ---- class (%d%d|%d%d) lane-group kernel: lanes own %s components, G=%d, %d quartet(s)/warp,'
+                   ' %d chain nodes, %d chain flops/primitive quartet/lane'
+                   % (self.la, self.lb, self.lc, self.ld, 'bra' if bra else 'ket', self.G, self.QPW, self.nvar,
+                      self.flops))
+        src.append('__constant__ IbLaneInfo ib_lane_%s[%d] = {' % (t, self.G))
+        for (c, dirs, nbs, sr) in rows:
+            dd = list(dirs) + [0] * (8 - len(dirs))
+            nn = list(nbs) + [0] * (8 - len(nbs))
+            src.append('  {{%d, %d, %d}, %d, {%s}, {%s}, {%d, %d, %d}},'
+                       % (c[0], c[1], c[2], len(dirs), ', '.join(map(str, dd)), ', '.join(map(str, nn)),
+                          sr[0], sr[1], sr[2]))
+        src.append('};')
+        src.append('template <typename R, bool SPH>')
+        src.append('__global__ void __launch_bounds__(IB_BLOCK) ib_eri_%s(const IbLaunch a) {' % t)
+        src.append('  extern __shared__ double ib_smem[];')
+        if self.wide:
+            src.append('  constexpr int QPB = IB_BLOCK / 64;')
+        else:
+            src.append('  constexpr int QPB = (IB_BLOCK / 32) * %d;' % self.QPW)
+        src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (self.cid, self.cid))
+        src.append('  if (beg + (int)blockIdx.x * QPB >= end) return;  // block-uniform')
+        src.append('  ib_stage_boys(ib_smem, a.boys_tab, %d);' % self.L)
+        src.append('  __syncthreads();')
+        if self.wide:
+            src.append('  const int gid = threadIdx.x / 64, j = threadIdx.x % 64;')
+            src.append('  const unsigned gmask = 0xffffffffu;')
+        else:
+            src.append('  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;')
+            src.append('  const int gq = lane / %d, j = lane %% %d;' % (self.G, self.G))
+            src.append('  const int gid = warp * %d + gq;' % self.QPW)
+            src.append('  const unsigned gmask = %s;' % ('0xffffffffu' if self.G == 32 else
+                                                       '(((1u << %d) - 1u) << (gq * %d))' % (self.G, self.G)))
+        src.append('  (void)gmask;')
+        per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0)
+        src.append('  double* __restrict__ sb = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + gid * %d;' % per_group)
+        if self.wide:
+            src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb + %d);' % smem_group)
+            src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * 64))
+            src.append('  (void)xb1;')
+        src.append('  const IbLaneInfo li = ib_lane_%s[j];' % t)
+        src.append('  const int src0 = li.src[0], src1 = li.src[1], src2 = li.src[2];')
+        src.append('  (void)src0; (void)src1; (void)src2;')
+        src.append('  for (int p = beg + (int)blockIdx.x * QPB + gid; p < end; p += (int)gridDim.x * QPB) {')
+        src.append('    IbQuartet g;')
+        src.append('    ib_load_quartet(a, p, g);')
+        src.append('    double acc[%d];' % NT)
+        src.append('#pragma unroll')
+        src.append('    for (int k = 0; k < %d; ++k) acc[k] = 0.0;' % NT)
+        src.append('    for (int ia = 0; ia < g.k[0]; ++ia)')
+        src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
+        src.append('      IbBraPair bp;')
+        src.append('      ib_bra_pair(a, g, ia, ib, bp);')
+        src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
+        src.append('      for (int id = 0; id < g.k[3]; ++id) {')
+        src.append('        IbPrimQuartet<R> pq;')
+        src.append('        double F[%d];' % (self.L + 1))
+        src.append('        ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % self.L)
+        # base chain along the lane side
+        if bra:
+            src.append('        const R SXx = pq.PA[0], SXy = pq.PA[1], SXz = pq.PA[2];')
+            src.append('        const R SWx = pq.WP[0], SWy = pq.WP[1], SWz = pq.WP[2];')
+            src.append('        const R so2 = pq.o2z, sro = pq.roz;')
+            src.append('        const R CXx = pq.QC[0], CXy = pq.QC[1], CXz = pq.QC[2];')
+            src.append('        const R CWx = pq.WQ[0], CWy = pq.WQ[1], CWz = pq.WQ[2];')
+            src.append('        const R co2 = pq.o2e, cro = pq.roe;')
+        else:
+            src.append('        const R SXx = pq.QC[0], SXy = pq.QC[1], SXz = pq.QC[2];')
+            src.append('        const R SWx = pq.WQ[0], SWy = pq.WQ[1], SWz = pq.WQ[2];')
+            src.append('        const R so2 = pq.o2e, sro = pq.roe;')
+            src.append('        const R CXx = pq.PA[0], CXy = pq.PA[1], CXz = pq.PA[2];')
+            src.append('        const R CWx = pq.WP[0], CWy = pq.WP[1], CWz = pq.WP[2];')
+            src.append('        const R co2 = pq.o2z, cro = pq.roz;')
+        src.append('        const R tfx = (R)li.c[0] * pq.o2zpe, tfy = (R)li.c[1] * pq.o2zpe, tfz = (R)li.c[2] * pq.o2zpe;')
+        src.append('        (void)tfx; (void)tfy; (void)tfz; (void)SXx; (void)SXy; (void)SXz; (void)SWx; (void)SWy;')
+        src.append('        (void)SWz; (void)so2; (void)sro; (void)CXx; (void)CXy; (void)CXz; (void)CWx; (void)CWy;')
+        src.append('        (void)CWz; (void)co2; (void)cro;')
+        L = self.L
+        for m in range(L + 1):
+            src.append('        R c1_%d = (R)F[%d], c2_%d = (R)0;' % (m, m, m))
+        for k in range(1, self.S_hi + 1):
+            src.append('        if (%d <= li.len) {' % k)
+            src.append('          const int d = li.dir[%d];' % (k - 1))
+            src.append('          const R px = d == 0 ? SXx : (d == 1 ? SXy : SXz);')
+            src.append('          const R wx = d == 0 ? SWx : (d == 1 ? SWy : SWz);')
+            src.append('          const R nb = (R)li.nb[%d] * so2;' % (k - 1))
+            for m in range(L - k + 1):
+                src.append('          const R t%d = px * c1_%d + wx * c1_%d + nb * (c2_%d - sro * c2_%d);'
+                           % (m, m, m + 1, m, m + 1))
+            for m in range(L - k + 1):
+                src.append('          c2_%d = c1_%d; c1_%d = t%d;' % (m, m, m, m))
+            src.append('        }')
+        for m in range(self.C_hi + 1):
+            src.append('        const R b%d = c1_%d;' % (m, m))
+        src += chain
+        src.append('      }')
+        src.append('    }')
+        # accumulators -> shared [e][f]
+        if bra:
+            src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
+            for tt in range(NT):
+                src.append('      sb[(j - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NF, tt, tt))
+        else:
+            src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
+            for tt in range(NT):
+                src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NF, s_lo_idx, tt))
+        src.append('    }')
+        src.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        src.append('    const double ABx = g.AB[0], ABy = g.AB[1], ABz = g.AB[2];')
+        src.append('    const double CDx = g.CD[0], CDy = g.CD[1], CDz = g.CD[2];')
+        src.append('    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;')
+        src.append('    double* __restrict__ o = a.out + g.off;')
+        src.append('    if (SPH) {')
+        src += ['  ' + s for s in epi_sph]
+        src.append('    } else {')
+        src += ['  ' + s for s in epi_cart]
+        src.append('    }')
+        src.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        src.append('  }')
+        src.append('}')
+        src.append('')
+        if self.wide:
+            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 64) * %d)' % per_group
+        else:
+            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, smem_group)
+        src.append('static size_t ib_smem_%s() { return %s; }' % (t, smem_bytes))
+        src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
+        src.append('  const size_t smem = ib_smem_%s();' % t)
+        src.append('  switch (variant) {')
+        for v, (R, S) in enumerate((('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))):
+            src.append('    case %d: ib_eri_%s<%s, %s><<<grid, IB_BLOCK, smem, s>>>(a); break;' % (v, t, R, S))
+        src.append('  }')
+        src.append('}')
+        src.append('static int ib_occupancy_%s(int variant) {' % t)
+        src.append('  int n = 0; const size_t smem = ib_smem_%s();' % t)
+        src.append('  switch (variant) {')
+        for v, (R, S) in enumerate((('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))):
+            src.append('    case %d: cudaFuncSetAttribute(ib_eri_%s<%s, %s>, cudaFuncAttributeMaxDynamicSharedMemorySize, '
+                       '(int)smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ib_eri_%s<%s, %s>, IB_BLOCK, '
+                       'smem); break;' % (v, t, R, S, t, R, S))
+        src.append('  }')
+        src.append('  return n;')
+        src.append('}')
+        src.append('')
+        stats = dict(tag=t, cid=self.cid, L=L, kind='group', G=self.G, orient=self.orient, nodes=self.nvar,
+                     lane_flops=self.flops, nacc=NE * NF)
+        return '\n'.join(src), stats
