@@ -38,7 +38,7 @@ __global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double
 
 namespace {
 
-constexpr int kNSide = 4;                       // side streams for concurrent class kernels
+constexpr int kNSide = 8;                       // side streams for concurrent class kernels
 constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 copies
 constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
 constexpr int kNRanges = 4 * IB_NCLASS + 2;

@@ -382,12 +382,16 @@ class GroupEmitter:
             src.append('  const unsigned gmask = %s;' % ('0xffffffffu' if self.G == 32 else
                                                        '(((1u << %d) - 1u) << (gq * %d))' % (self.G, self.G)))
         src.append('  (void)gmask;')
-        per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0)
+        nfield = 17 + self.L + 1
+        per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
         src.append('  double* __restrict__ sb = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + gid * %d;' % per_group)
         if self.wide:
             src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb + %d);' % smem_group)
             src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * 64))
             src.append('  (void)xb1;')
+        if self.G > 1:
+            src.append('  R* __restrict__ ps = reinterpret_cast<R*>(sb + %d);'
+                       % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0)))
         src.append('  const IbLaneInfo li = ib_lane_%s[j];' % t)
         src.append('  const int src0 = li.src[0], src1 = li.src[1], src2 = li.src[2];')
         src.append('  (void)src0; (void)src1; (void)src2;')
@@ -397,37 +401,74 @@ class GroupEmitter:
         src.append('    double acc[%d];' % NT)
         src.append('#pragma unroll')
         src.append('    for (int k = 0; k < %d; ++k) acc[k] = 0.0;' % NT)
-        src.append('    for (int ia = 0; ia < g.k[0]; ++ia)')
-        src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
-        src.append('      IbBraPair bp;')
-        src.append('      ib_bra_pair(a, g, ia, ib, bp);')
-        src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
-        src.append('      for (int id = 0; id < g.k[3]; ++id) {')
-        src.append('        IbPrimQuartet<R> pq;')
-        src.append('        double F[%d];' % (self.L + 1))
-        src.append('        ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % self.L)
-        # base chain along the lane side
-        if bra:
-            src.append('        const R SXx = pq.PA[0], SXy = pq.PA[1], SXz = pq.PA[2];')
-            src.append('        const R SWx = pq.WP[0], SWy = pq.WP[1], SWz = pq.WP[2];')
-            src.append('        const R so2 = pq.o2z, sro = pq.roz;')
-            src.append('        const R CXx = pq.QC[0], CXy = pq.QC[1], CXz = pq.QC[2];')
-            src.append('        const R CWx = pq.WQ[0], CWy = pq.WQ[1], CWz = pq.WQ[2];')
-            src.append('        const R co2 = pq.o2e, cro = pq.roe;')
+        L = self.L
+        fields = ['PA[0]', 'PA[1]', 'PA[2]', 'WP[0]', 'WP[1]', 'WP[2]', 'QC[0]', 'QC[1]', 'QC[2]',
+                  'WQ[0]', 'WQ[1]', 'WQ[2]', 'o2z', 'roz', 'o2e', 'roe', 'o2zpe']
+        names = ['PAx', 'PAy', 'PAz', 'WPx', 'WPy', 'WPz', 'QCx', 'QCy', 'QCz', 'WQx', 'WQy', 'WQz',
+                 'o2z', 'roz', 'o2e', 'roe', 'o2zpe']
+        self.nfield = len(fields) + L + 1
+        if self.G == 1:
+            # one lane per quartet: set up each primitive quartet in registers
+            src.append('    for (int ia = 0; ia < g.k[0]; ++ia)')
+            src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
+            src.append('      IbBraPair bp;')
+            src.append('      ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
+            src.append('      for (int id = 0; id < g.k[3]; ++id) {')
+            src.append('        IbPrimQuartet<R> pq;')
+            src.append('        double F[%d];' % (L + 1))
+            src.append('        ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            for f, nm in zip(fields, names):
+                src.append('        const R %s = pq.%s;' % (nm, f))
+            for m in range(L + 1):
+                src.append('        const R f%d = (R)F[%d];' % (m, m))
         else:
-            src.append('        const R SXx = pq.QC[0], SXy = pq.QC[1], SXz = pq.QC[2];')
-            src.append('        const R SWx = pq.WQ[0], SWy = pq.WQ[1], SWz = pq.WQ[2];')
-            src.append('        const R so2 = pq.o2e, sro = pq.roe;')
-            src.append('        const R CXx = pq.PA[0], CXy = pq.PA[1], CXz = pq.PA[2];')
-            src.append('        const R CWx = pq.WP[0], CWy = pq.WP[1], CWz = pq.WP[2];')
-            src.append('        const R co2 = pq.o2z, cro = pq.roz;')
-        src.append('        const R tfx = (R)li.c[0] * pq.o2zpe, tfy = (R)li.c[1] * pq.o2zpe, tfz = (R)li.c[2] * pq.o2zpe;')
+            # lane j sets up primitive quartet q0 + j of the chunk; the group
+            # then sweeps the chunk reading the shared values (broadcast)
+            sync = 'ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'
+            src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
+            src.append('    const int kcd = g.k[2] * kd_, np = g.k[0] * kb_ * kcd;')
+            src.append('    for (int q0 = 0; q0 < np; q0 += %d) {' % self.G)
+            src.append('      {')
+            src.append('        const int q = q0 + j;')
+            src.append('        if (q < np) {')
+            src.append('          const int ab = q / kcd, cd = q - ab * kcd;')
+            src.append('          const int ia = ab / kb_, ib = ab - ia * kb_;')
+            src.append('          const int ic = cd / kd_, id = cd - ic * kd_;')
+            src.append('          IbBraPair bp;')
+            src.append('          ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('          IbPrimQuartet<R> pq;')
+            src.append('          double F[%d];' % (L + 1))
+            src.append('          ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            for k, f in enumerate(fields):
+                src.append('          ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
+            for m in range(L + 1):
+                src.append('          ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
+            src.append('        }')
+            src.append('      }')
+            src.append('      %s;' % sync)
+            src.append('      const int nu = min(%d, np - q0);' % self.G)
+            src.append('      for (int u = 0; u < nu; ++u) {')
+            for k, nm in enumerate(names):
+                src.append('        const R %s = ps[%d * %d + u];' % (nm, k, self.G))
+            for m in range(L + 1):
+                src.append('        const R f%d = ps[%d * %d + u];' % (m, len(fields) + m, self.G))
+        if bra:
+            src.append('        const R SXx = PAx, SXy = PAy, SXz = PAz, SWx = WPx, SWy = WPy, SWz = WPz;')
+            src.append('        const R so2 = o2z, sro = roz;')
+            src.append('        const R CXx = QCx, CXy = QCy, CXz = QCz, CWx = WQx, CWy = WQy, CWz = WQz;')
+            src.append('        const R co2 = o2e, cro = roe;')
+        else:
+            src.append('        const R SXx = QCx, SXy = QCy, SXz = QCz, SWx = WQx, SWy = WQy, SWz = WQz;')
+            src.append('        const R so2 = o2e, sro = roe;')
+            src.append('        const R CXx = PAx, CXy = PAy, CXz = PAz, CWx = WPx, CWy = WPy, CWz = WPz;')
+            src.append('        const R co2 = o2z, cro = roz;')
+        src.append('        const R tfx = (R)li.c[0] * o2zpe, tfy = (R)li.c[1] * o2zpe, tfz = (R)li.c[2] * o2zpe;')
         src.append('        (void)tfx; (void)tfy; (void)tfz; (void)SXx; (void)SXy; (void)SXz; (void)SWx; (void)SWy;')
         src.append('        (void)SWz; (void)so2; (void)sro; (void)CXx; (void)CXy; (void)CXz; (void)CWx; (void)CWy;')
         src.append('        (void)CWz; (void)co2; (void)cro;')
-        L = self.L
         for m in range(L + 1):
-            src.append('        R c1_%d = (R)F[%d], c2_%d = (R)0;' % (m, m, m))
+            src.append('        R c1_%d = f%d, c2_%d = (R)0;' % (m, m, m))
         for k in range(1, self.S_hi + 1):
             src.append('        if (%d <= li.len) {' % k)
             src.append('          const int d = li.dir[%d];' % (k - 1))
@@ -443,8 +484,13 @@ class GroupEmitter:
         for m in range(self.C_hi + 1):
             src.append('        const R b%d = c1_%d;' % (m, m))
         src += chain
-        src.append('      }')
-        src.append('    }')
+        if self.G == 1:
+            src.append('      }')
+            src.append('    }')
+        else:
+            src.append('      }')
+            src.append('      %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+            src.append('    }')
         # accumulators -> shared [e][f]
         if bra:
             src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
@@ -472,7 +518,7 @@ class GroupEmitter:
         if self.wide:
             smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 64) * %d)' % per_group
         else:
-            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, smem_group)
+            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, per_group)
         src.append('static size_t ib_smem_%s() { return %s; }' % (t, smem_bytes))
         src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
         src.append('  const size_t smem = ib_smem_%s();' % t)
