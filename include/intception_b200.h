@@ -135,6 +135,23 @@ int intception_b200_last_launch_count(void);
  * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
 int intception_b200_batch_status(void);
 
+/* Allocation-free variant of intception_b200_eri_batch, for callers that
+ * cannot call cudaMalloc (a host framework whose pool allocator owns the device
+ * memory, or code that must not trigger the device synchronisation of
+ * cudaMalloc/cudaFree).  It has no counterpart in the reference.  Same
+ * arguments and output layout as intception_b200_eri_batch with precision
+ * IB_PREC_FP64; all quartets go through the block-per-quartet kernel, using
+ * file-scope device arrays of fixed size that every GPU loading the library
+ * holds until exit: 32 MiB of scratch and descriptors for at most 65536
+ * quartets per call (larger nq returns IB_ERR_ARG; IB_ERR_SCRATCH if one
+ * quartet of basis->lmax needs more scratch than that).  The first call on a
+ * device looks up those arrays and copies the Boys and spherical tables into
+ * them (a synchronous copy): make that first call before any stream capture.
+ * Calls share the arrays, so calls whose work overlaps on the GPU (unordered
+ * streams) race; order them.  Asynchronous on stream (NULL = legacy default). */
+int intception_b200_eri_batch_noalloc(const intception_b200_basis *basis, const int *quartets,
+                                      const long long *out_off, int nq, int spherical, double *out, void *stream);
+
 /* The library's Cartesian->spherical matrix for l (host memory,
  * T[icart + isph*ncart], ncart x (2l+1)). */
 int intception_b200_sph_matrix(int l, double *T);

@@ -87,6 +87,9 @@ def load():
     lib.intception_b200_eri_batch.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                               C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
     lib.intception_b200_eri_batch.restype = C.c_int
+    lib.intception_b200_eri_batch_noalloc.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int,
+                                                      C.c_int, C.c_void_p, C.c_void_p]
+    lib.intception_b200_eri_batch_noalloc.restype = C.c_int
     lib.intception_b200_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
     lib.intception_b200_fma_peak.restype = C.c_int
     _lib = lib
