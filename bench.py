@@ -135,6 +135,26 @@ class ClockSampler:
                 'samples': len(sm)}
 
 
+def live_pairs(batch, i, j):
+    """Per quartet, primitive pairs of shells (i, j) with c_a c_b exp(-xi R^2) != 0."""
+    sa, sb = batch.quartets[:, i], batch.quartets[:, j]
+    ka, kb = batch.shell_k[sa], batch.shell_k[sb]
+    pa, pb = batch.shell_ptr[sa], batch.shell_ptr[sb]
+    r2 = ((batch.shell_xyz[sa] - batch.shell_xyz[sb]) ** 2).sum(axis=1)
+    n = np.zeros(batch.nq, dtype=np.int64)
+    for u in range(int(ka.max())):
+        for v in range(int(kb.max())):
+            ok = (u < ka) & (v < kb)
+            ea = batch.prim_exp[np.where(ok, pa + u, 0)]
+            eb = batch.prim_exp[np.where(ok, pb + v, 0)]
+            ca = batch.prim_coef[np.where(ok, pa + u, 0)]
+            cb = batch.prim_coef[np.where(ok, pb + v, 0)]
+            with np.errstate(under='ignore', over='ignore'):
+                kab = ca * cb * np.exp(-ea * eb / (ea + eb) * r2)
+            n += (ok & (kab != 0.0)).astype(np.int64)
+    return n
+
+
 def alg_flops(batch):
     """Algorithmic FP64 work of one step (see DESIGN: per primitive quartet the
     emitted VRR count plus geometry and Boys; per quartet the HRR and the
@@ -155,7 +175,9 @@ def alg_flops(batch):
     pb2 = np.where(sw, pk, pb)
     pk2 = np.where(sw, pb, pk)
     cid = pb2 * (pb2 + 1) // 2 + pk2
-    nprim = ks.prod(axis=1)
+    # primitive quartets whose prefactor is not exactly zero (the kernels skip
+    # the others bit-exactly, so they are not work an algorithm must do)
+    nprim = live_pairs(batch, 0, 1) * live_pairs(batch, 2, 3)
     vrr = np.array([stats[c]['vrr_flops'] + 74 + 2 * stats[c]['L'] for c in range(len(stats))])
     hrr = np.array([stats[c]['hrr_flops'] + (stats[c]['sph_flops'] if batch.spherical else 0)
                     for c in range(len(stats))])

@@ -198,14 +198,18 @@ struct IbPrimQuartet {
 };
 
 // Ket pair, quartet geometry and the scaled Boys values F[m] = pref * F_m(T).
+// Returns false (and computes nothing else) when the pair prefactors multiply
+// to exactly zero: every value of that primitive quartet would be +-0, so
+// skipping it leaves the contracted sums bit-identical.
 template <typename R, int L>
-__device__ __forceinline__ void ib_prim_quartet(const IbLaunch& a, const IbQuartet& g, const IbBraPair& bp, int ic,
+__device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuartet& g, const IbBraPair& bp, int ic,
                                                 int id, const double* __restrict__ boys_s, double* F,
                                                 IbPrimQuartet<R>& pq) {
   const double xc = __ldg(a.prim_exp + g.ptr[2] + ic), cc = __ldg(a.prim_coef + g.ptr[2] + ic);
   const double xd = __ldg(a.prim_exp + g.ptr[3] + id), cd = __ldg(a.prim_coef + g.ptr[3] + id);
   const double eta = xc + xd, oe = 1.0 / eta;
   const double Kcd = cc * cd * exp(-xc * xd * oe * g.RCD2);
+  if (bp.K * Kcd == 0.0) return false;
   const double ozpe = 1.0 / (bp.zeta + eta);
   const double rho = bp.zeta * eta * ozpe;
   double Q[3], PQ[3];
@@ -232,4 +236,5 @@ __device__ __forceinline__ void ib_prim_quartet(const IbLaunch& a, const IbQuart
   pq.o2e = (R)(0.5 * oe);
   pq.roe = (R)(rho * oe);
   pq.o2zpe = (R)(0.5 * ozpe);
+  return true;
 }

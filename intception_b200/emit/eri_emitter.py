@@ -346,11 +346,12 @@ class Emitter:
         src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
         src.append('      IbBraPair bp;')
         src.append('      ib_bra_pair(a, g, ia, ib, bp);')
+        src.append('      if (bp.K == 0.0) continue;')
         src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
         src.append('      for (int id = 0; id < g.k[3]; ++id) {')
         src.append('      IbPrimQuartet<R> pq;')
         src.append('      double F[%d];' % (L + 1))
-        src.append('      ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_boys_s, F, pq);' % L)
+        src.append('      if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_boys_s, F, pq)) continue;' % L)
         for m in range(L + 1):
             src.append('      const R s%d = (R)F[%d];' % (m, m))
         src.append('      const R PAx = pq.PA[0], PAy = pq.PA[1], PAz = pq.PA[2];')

@@ -59,6 +59,11 @@ def orientation(la, lb, lc, ld):
     return 'bra' if ne <= nf else 'ket'
 
 
+# emit the chain level by level with each level's shuffles batched (True), or
+# in dependency order with shuffles inline (False: fewer live registers)
+LEVEL_ORDER = False
+
+
 def group_size(n):
     g = 1
     while g < n:
@@ -90,6 +95,7 @@ class GroupEmitter:
         self.nvar = 0
         self.flops = 0
         self.mult = {}
+        self.shuffles = {}
 
     # -------------------------------------------------------------- lane table
     def lane_table(self):
@@ -152,11 +158,19 @@ class GroupEmitter:
                 slot = self.slot_index(cm, m + 1)
                 expr += ' + tf%s * xb%d[%d * 64 + src%s]' % (d, lvl % 2, slot, 'xyz'.index(d))
             else:
-                expr += ' + tf%s * __shfl_sync(gmask, %s, src%s, %d)' % (d, a1, 'xyz'.index(d), self.G)
+                expr += ' + tf%s * %s' % (d, self._shfl(a1, i, sum(cm)))
             fl += 2
         name = self._new(expr, fl)
         self.nodes[key] = name
         return name
+
+    def _shfl(self, name, i, level):
+        """Temporary holding the value `name` of the lane owning s - 1i; the
+        shuffles of a level are issued together before its nodes."""
+        key = (name, i)
+        if key not in self.shuffles:
+            self.shuffles[key] = ('x%d' % len(self.shuffles), level)
+        return self.shuffles[key][0]
 
     def slot_index(self, c, m):
         """Position of chain node (c, m), m >= 1, in its level's transfer buffer."""
@@ -207,22 +221,72 @@ class GroupEmitter:
         defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
         return defs + out, len(targets)
 
-    def emit_chain(self):
-        if self.wide:
-            return self.emit_chain_wide()
+    def emit_chain_dfs(self):
+        """Chain side in dependency (DFS) order from each target; shuffles sit
+        inline next to their use and ptxas schedules them."""
         targets = comps_range(self.C_lo, self.C_hi)
         out = []
+        t_index = {c: t for t, c in enumerate(targets)}
+        if ZERO in t_index:
+            out.append('        acc[%d] += (double)b0;' % t_index[ZERO])
         acc = []
         for t, c in enumerate(targets):
+            if c == ZERO:
+                continue
+            n0 = len(self.lines)
             v = self.node(c, 0)
             acc.append((len(self.lines), '        acc[%d] += (double)%s;' % (t, v)))
             self.flops += 1
+        shuf = {var: (src_name, i) for (src_name, i), (var, lvl) in self.shuffles.items()}
         pos = 0
+        body = []
         for at, line in acc:
-            out += self.lines[pos:at]
-            out.append(line)
+            body += self.lines[pos:at]
+            body.append(line)
             pos = at
-        out += self.lines[pos:]
+        body += self.lines[pos:]
+        # inline the shuffle temporaries where they are used
+        import re
+        for ln in body:
+            for var in re.findall(r'\bx\d+\b', ln):
+                src_name, i = shuf[var]
+                ln = re.sub(r'\b%s\b' % var, '__shfl_sync(gmask, %s, src%d, %d)' % (src_name, i, self.G), ln)
+            out.append(ln)
+        defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
+        return defs + out, len(targets)
+
+    def emit_chain(self):
+        """Chain side level by level: the level's transfer operands are fetched
+        with back-to-back shuffles first (their latency overlaps), then its
+        nodes, then the accumulation of the level's targets."""
+        if self.wide:
+            return self.emit_chain_wide()
+        if not LEVEL_ORDER:
+            return self.emit_chain_dfs()
+        targets = comps_range(self.C_lo, self.C_hi)
+        for c in targets:
+            self.node(c, 0)
+        byname = {name: key for key, name in self.nodes.items()}
+        level_lines = {}
+        for ln in self.lines:
+            name = ln.split('const R ')[1].split(' =')[0]
+            c, m = byname[name]
+            level_lines.setdefault(sum(c), []).append(ln)
+        shuf_by_level = {}
+        for (src_name, i), (var, lvl) in self.shuffles.items():
+            shuf_by_level.setdefault(lvl + 1, []).append(
+                '        const R %s = __shfl_sync(gmask, %s, src%d, %d);' % (var, src_name, i, self.G))
+        t_index = {c: t for t, c in enumerate(targets)}
+        out = []
+        if ZERO in t_index:
+            out.append('        acc[%d] += (double)b0;' % t_index[ZERO])
+        for k in range(1, self.C_hi + 1):
+            out += shuf_by_level.get(k, [])
+            out += level_lines.get(k, [])
+            for c in comps(k):
+                if c in t_index:
+                    out.append('        acc[%d] += (double)%s;' % (t_index[c], self.nodes[(c, 0)]))
+                    self.flops += 1
         defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
         return defs + out, len(targets)
 
@@ -282,6 +346,7 @@ class GroupEmitter:
         Elist = comps_range(la, self.E)
         Flist = comps_range(lc, self.F)
         NE, NF = len(Elist), len(Flist)
+        NFP = NF if NF % 2 else NF + 1  # odd row stride: conflict-free column and row access
         e_index = {e: i for i, e in enumerate(Elist)}
         f_index = {f: i for i, f in enumerate(Flist)}
         na = (2 * la + 1) if sph else len(A)
@@ -292,7 +357,7 @@ class GroupEmitter:
         # bra HRR, lanes over f
         L.append('    for (int t = j; t < %d; t += %d) {' % (NF, self.G))
         for e in range(NE):
-            L.append('      const double q%d = sb[%d * %d + t];' % (e, e, NF))
+            L.append('      const double q%d = sb[%d * %d + t];' % (e, e, NFP))
         cnt = [0]
         body = []
         res = self._hrr(A, B, lambda a: 'q%d' % e_index[a], 'AB', 'h', body, cnt)
@@ -306,14 +371,14 @@ class GroupEmitter:
         else:
             outs = [res[(a, b)] for a in A for b in B]
         for u, name in enumerate(outs):
-            L.append('      sb[%d * %d + t] = %s;' % (u, NF, name))
+            L.append('      sb[%d * %d + t] = %s;' % (u, NFP, name))
         L.append('    }')
         L.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
         # ket HRR, lanes over ab
         NAB = na * nb
         L.append('    for (int u = j; u < %d; u += %d) {' % (NAB, self.G))
         for f in range(NF):
-            L.append('      const double w%d = sb[u * %d + %d];' % (f, NF, f))
+            L.append('      const double w%d = sb[u * %d + %d];' % (f, NFP, f))
         body = []
         cnt = [0]
         res = self._hrr(Cc, D, lambda c: 'w%d' % f_index[c], 'CD', 'k', body, cnt)
@@ -332,7 +397,7 @@ class GroupEmitter:
             off = ' + '.join(x for x in (('%d * g.st[2]' % i) if i else '', ('%d * g.st[3]' % k) if k else '') if x)
             L.append('      ou[%s] = %s;' % (off or '0', name))
         L.append('    }')
-        return L, max(NE, len(A) * len(B)) * NF
+        return L, max(NE, len(A) * len(B)) * NFP
 
     # -------------------------------------------------------------- kernel
     def kernel(self):
@@ -345,6 +410,7 @@ class GroupEmitter:
         Elist = comps_range(self.la, self.E)
         Flist = comps_range(self.lc, self.F)
         NE, NF = len(Elist), len(Flist)
+        NFP = NF if NF % 2 else NF + 1
         s_lo_idx = ncum(self.S_lo - 1)
         rows = self.lane_table()
         src = []
@@ -382,7 +448,7 @@ class GroupEmitter:
             src.append('  const unsigned gmask = %s;' % ('0xffffffffu' if self.G == 32 else
                                                        '(((1u << %d) - 1u) << (gq * %d))' % (self.G, self.G)))
         src.append('  (void)gmask;')
-        nfield = 17 + self.L + 1
+        nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
         per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
         src.append('  double* __restrict__ sb = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + gid * %d;' % per_group)
         if self.wide:
@@ -392,6 +458,8 @@ class GroupEmitter:
         if self.G > 1:
             src.append('  R* __restrict__ ps = reinterpret_cast<R*>(sb + %d);'
                        % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0)))
+            src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);'
+                       % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (17 + self.L + 1) * self.G))
         src.append('  const IbLaneInfo li = ib_lane_%s[j];' % t)
         src.append('  const int src0 = li.src[0], src1 = li.src[1], src2 = li.src[2];')
         src.append('  (void)src0; (void)src1; (void)src2;')
@@ -413,11 +481,12 @@ class GroupEmitter:
             src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
             src.append('      IbBraPair bp;')
             src.append('      ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('      if (bp.K == 0.0) continue;  // every primitive quartet of this pair is zero')
             src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
             src.append('      for (int id = 0; id < g.k[3]; ++id) {')
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
-            src.append('        ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq)) continue;' % L)
             for f, nm in zip(fields, names):
                 src.append('        const R %s = pq.%s;' % (nm, f))
             for m in range(L + 1):
@@ -439,16 +508,20 @@ class GroupEmitter:
             src.append('          ib_bra_pair(a, g, ia, ib, bp);')
             src.append('          IbPrimQuartet<R> pq;')
             src.append('          double F[%d];' % (L + 1))
-            src.append('          ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            src.append('          const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            src.append('          if (live) {')
             for k, f in enumerate(fields):
-                src.append('          ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
+                src.append('            ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
             for m in range(L + 1):
-                src.append('          ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
+                src.append('            ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
+            src.append('          }')
+            src.append('          pz[j] = live ? 1 : 0;')
             src.append('        }')
             src.append('      }')
             src.append('      %s;' % sync)
             src.append('      const int nu = min(%d, np - q0);' % self.G)
             src.append('      for (int u = 0; u < nu; ++u) {')
+            src.append('        if (!pz[u]) continue;  // group-uniform: exact-zero primitive quartet')
             for k, nm in enumerate(names):
                 src.append('        const R %s = ps[%d * %d + u];' % (nm, k, self.G))
             for m in range(L + 1):
@@ -495,11 +568,11 @@ class GroupEmitter:
         if bra:
             src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
             for tt in range(NT):
-                src.append('      sb[(j - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NF, tt, tt))
+                src.append('      sb[(j - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NFP, tt, tt))
         else:
             src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
             for tt in range(NT):
-                src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NF, s_lo_idx, tt))
+                src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NFP, s_lo_idx, tt))
         src.append('    }')
         src.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
         src.append('    const double ABx = g.AB[0], ABy = g.AB[1], ABz = g.AB[2];')
