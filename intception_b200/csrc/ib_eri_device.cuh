@@ -43,6 +43,9 @@ struct IbLaunch {
   const double* sph;       // library Cartesian->spherical matrices, packed per l
   double* out;
   int* status;             // device error word (0 = ok)
+  int* flags;              // per sorted item: 1 = FP32 result rejected, recompute in FP64
+  int recheck;             // FP64 kernels: evaluate only flagged items
+  double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
 };
 
 // Per-lane constants of a lane-group kernel: the lane's Cartesian component,
@@ -138,6 +141,26 @@ __device__ inline void ib_boys_rt(double T, int L, const double* __restrict__ ta
     for (int m = 0; m < L; ++m) F[m + 1] = fma((double)m + 0.5, F[m], -he) * oT;
   }
 }
+
+// First-order bound on the rounding error of an FP32 evaluation of the VRR of
+// one primitive quartet, for every target [s|c]^(0) (lane side s up to level
+// S, chain side c up to level C).  The absolute-value recurrence is bounded by
+// |s0| g^S h^C with g^2 >= aS g + bS (base chain: aS = |X|+|W|, bS =
+// S (1+r)/2x) and h^2 >= (aC + tC/g) h + bC (chain side with the transfer
+// term tC = S/2(zeta+eta)); each value passes through at most 4(S+C)+2
+// roundings of unit 2^-24.
+__device__ __forceinline__ double ib_fp32_err(double s0, double aS, double bS, int S, double aC, double bC,
+                                              double tC, int C) {
+  const double g = fmax(0.5 * (aS + sqrt(aS * aS + 4.0 * bS)), 1.0);
+  const double a2 = aC + tC / g;
+  const double h = fmax(0.5 * (a2 + sqrt(a2 * a2 + 4.0 * bC)), 1.0);
+  double v = fabs(s0);
+  for (int i = 0; i < S; ++i) v *= g;
+  for (int i = 0; i < C; ++i) v *= h;
+  return (4.0 * (S + C) + 2.0) * 5.9604644775390625e-08 * v;
+}
+
+__device__ __forceinline__ double ib_amax3(double x, double y, double z) { return fmax(fabs(x), fmax(fabs(y), fabs(z))); }
 
 struct IbQuartet {
   double A[3], B[3], C[3], D[3];

@@ -41,8 +41,9 @@ namespace {
 constexpr int kNSide = 8;                       // side streams for concurrent class kernels
 constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 copies
 constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
-constexpr int kNRanges = 4 * IB_NCLASS + 2;
-constexpr int kKeyBits = 22;
+constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
+constexpr int kNRanges = 4 * IB_NCLASS + 4;
+constexpr int kKeyBits = 23;                    // skip(1) fp32(1) class(9) Kab(6) Kcd(6)
 constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
 
 thread_local int tl_status = IB_OK;
@@ -104,6 +105,8 @@ struct Context {
   cudaStream_t side[kNSide] = {};
   cudaEvent_t fork = nullptr, join[kNSide] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
+  DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
+  DevBuf flags;                                             // FP32 rejections of the last mixed batch
   DevBuf d_stage, d_cart, d_res;
   HostBuf h_stage, h_res;
   IbClassEntry table[IB_NCLASS] = {};
@@ -142,8 +145,8 @@ __device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
 
 __global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
                             const int* __restrict__ shell_k, int nq, int lmax, const double* __restrict__ bounds,
-                            double thr, int mixed, int n_emit, unsigned* __restrict__ keys, int* __restrict__ vals,
-                            int* status) {
+                            double skip_below, double thr, int mixed, int n_emit, unsigned* __restrict__ keys,
+                            int* __restrict__ vals, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], st[4] = {0, 0, 0, 0};
     bool bad = false;
@@ -160,8 +163,10 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int pb = ib_pair_d(l[0], l[1]), pk = ib_pair_d(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
     const int kab = min(shell_k[s[0]] * shell_k[s[1]], 63), kcd = min(shell_k[s[2]] * shell_k[s[3]], 63);
-    const int fp32 = (mixed && cid < n_emit && bounds[q] < thr) ? 1 : 0;
-    keys[q] = (unsigned(fp32) << 21) | (unsigned(cid) << 12) | (unsigned(kab) << 6) | unsigned(kcd);
+    const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
+    const int fp32 = (!skip && mixed && cid < n_emit && bounds[q] < thr) ? 1 : 0;
+    keys[q] = (unsigned(skip) << 22) | (unsigned(fp32) << 21) | (unsigned(cid) << 12) | (unsigned(kab) << 6) |
+              unsigned(kcd);
     vals[q] = q;
   }
 }
@@ -188,11 +193,16 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     it.off = out_off[q];
     items[p] = it;
     const unsigned key = keys[p];
-    const int slot = (int)(key >> 12);  // fp32 bit * 512 + cid
-    const int cid = slot & 511, fp32 = slot >> 9;
-    const int rs = 2 * (cid + fp32 * IB_NCLASS);
+    const int slot = (int)(key >> 12);  // skip bit * 1024 + fp32 bit * 512 + cid
     const int prev = p > 0 ? (int)(keys[p - 1] >> 12) : -1;
     const int next = p + 1 < nq ? (int)(keys[p + 1] >> 12) : -1;
+    if (slot >> 10) {  // screened out: one range for all of them, sorted last
+      if (prev < 0 || !(prev >> 10)) ranges[kSlotSkip] = p;
+      if (next < 0) ranges[kSlotSkip + 1] = p + 1;
+      continue;
+    }
+    const int cid = slot & 511, fp32 = (slot >> 9) & 1;
+    const int rs = 2 * (cid + fp32 * IB_NCLASS);
     if (prev != slot) ranges[rs] = p;
     if (next != slot) ranges[rs + 1] = p + 1;
     const bool gen = (fp32 == 0 && cid >= n_emit);
@@ -200,6 +210,62 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     const bool gnext = p + 1 < nq && ((next >> 9) == 0) && ((next & 511) >= n_emit);
     if (gen && !gprev) ranges[kSlotGeneric] = p;
     if (gen && !gnext) ranges[kSlotGeneric + 1] = p + 1;
+  }
+}
+
+// Screened-out quartets (bound below the skip threshold, so |(ab|cd)| <= bound):
+// their blocks are written as zeros, one warp per quartet.
+__global__ void ib_zero_blocks(const IbItem* __restrict__ items, const int* __restrict__ ranges,
+                               const int* __restrict__ shell_l, int spherical, double* __restrict__ out) {
+  const int beg = ranges[kSlotSkip], end = ranges[kSlotSkip + 1];
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int p = beg + wg; p < end; p += nw) {
+    const IbItem it = items[p];
+    int n[4];
+    for (int i = 0; i < 4; ++i) {
+      const int l = min(max(shell_l[it.s[i]], 0), IB_LMAX);
+      n[i] = spherical ? 2 * l + 1 : ib_ncart_d(l);
+    }
+    double* o = out + it.off;
+    const int tot = n[0] * n[1] * n[2] * n[3];
+    for (int e = lane; e < tot; e += 32) {
+      const int i3 = e % n[3], r3 = e / n[3];
+      const int i2 = r3 % n[2], r2 = r3 / n[2];
+      const int i1 = r2 % n[1], i0 = r2 / n[1];
+      o[(long long)i0 * it.st[0] + (long long)i1 * it.st[1] + (long long)i2 * it.st[2] + (long long)i3 * it.st[3]] = 0.0;
+    }
+  }
+}
+
+// Diagonal quartets (a,b|a,b) of a chunk of shell pairs, their block sizes, and
+// afterwards sqrt(max |(ij|ij)|) over the diagonal of each block.
+__global__ void ib_diag_quartets(const int* __restrict__ pairs, int n, const int* __restrict__ shell_l, int spherical,
+                                 int* __restrict__ quartets, long long* __restrict__ sizes) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int a = pairs[2 * p], b = pairs[2 * p + 1];
+    quartets[4 * p] = a;
+    quartets[4 * p + 1] = b;
+    quartets[4 * p + 2] = a;
+    quartets[4 * p + 3] = b;
+    const int la = shell_l[a], lb = shell_l[b];
+    const long long na = spherical ? 2 * la + 1 : ib_ncart_d(la), nb = spherical ? 2 * lb + 1 : ib_ncart_d(lb);
+    sizes[p] = na * na * nb * nb;
+  }
+}
+
+__global__ void ib_diag_max(const int* __restrict__ pairs, int n, const int* __restrict__ shell_l, int spherical,
+                            const long long* __restrict__ off, const double* __restrict__ blocks, double* __restrict__ q) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int la = shell_l[pairs[2 * p]], lb = shell_l[pairs[2 * p + 1]];
+    const int na = spherical ? 2 * la + 1 : ib_ncart_d(la), nb = spherical ? 2 * lb + 1 : ib_ncart_d(lb);
+    const double* blk = blocks + off[p];
+    double m = 0.0;
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < nb; ++j) m = fmax(m, fabs(blk[i + na * (j + nb * (i + na * j))]));
+    // a diagonal below the normal range may have underflowed to 0 while
+    // (ab|cd) does not: flooring it at DBL_MIN keeps q an upper bound
+    q[p] = sqrt(fmax(m, 2.2250738585072014e-308)) * (1.0 + 1e-12);
   }
 }
 
@@ -340,8 +406,18 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     // heaviest classes first so they start early on their streams
     for (int cid = ib_n_emitted_classes - 1; cid >= 0; --cid) {
       const int grid = c->nsm * c->occ[cid][variant];
-      c->table[cid].launch(variant, grid, c->side[k % kNSide], ap);
+      cudaStream_t ss = c->side[k % kNSide];
+      c->table[cid].launch(variant, grid, ss, ap);
       ++k;
+      if (prec == 1) {
+        // FP64 pass over the same items: recomputes the quartets the FP32
+        // kernel rejected (same stream, so it sees their flags)
+        IbLaunch ar = ap;
+        ar.recheck = 1;
+        const int v64 = sph ? 1 : 0;
+        c->table[cid].launch(v64, c->nsm * c->occ[cid][v64], ss, ar);
+        ++k;
+      }
     }
   }
   if (lmax > ib_lmax_emitted && fp64_present) {
@@ -655,6 +731,67 @@ int resolve_stream(Context* c, void* stream, cudaStream_t* s) {
   *s = static_cast<cudaStream_t>(stream);
   return IB_OK;
 }
+
+// The batch pipeline on stream s; the caller holds the context lock.
+int batch_impl(Context* c, const intception_b200_basis* basis, const int* quartets, const long long* out_off, int nq,
+               int spherical, int precision, const double* bounds, double skip_below, double fp32_below,
+               double mixed_tol, double* out, cudaStream_t s, int* nl) {
+  if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out)))
+    return set_status(IB_ERR_ARG, "eri_batch: null argument");
+  if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "eri_batch: basis lmax out of range");
+  if (precision != IB_PREC_FP64 && precision != IB_PREC_MIXED) return set_status(IB_ERR_ARG, "eri_batch: precision");
+  if ((precision == IB_PREC_MIXED || skip_below > 0.0) && !bounds)
+    return set_status(IB_ERR_ARG, "eri_batch: mixed precision and screening need bounds");
+  if (nq == 0) return set_status(IB_OK, "");
+  IB_CUDA(c->keys.ensure((size_t)nq * sizeof(unsigned)));
+  IB_CUDA(c->keys2.ensure((size_t)nq * sizeof(unsigned)));
+  IB_CUDA(c->vals.ensure((size_t)nq * sizeof(int)));
+  IB_CUDA(c->vals2.ensure((size_t)nq * sizeof(int)));
+  IB_CUDA(c->items.ensure((size_t)nq * sizeof(IbItem)));
+  size_t tmp_bytes = 0;
+  IB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
+                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
+  IB_CUDA(c->cub_tmp.ensure(tmp_bytes));
+  IB_CUDA(cudaMemsetAsync(c->ranges.p, 0, kNRanges * sizeof(int), s));
+  IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
+  const int grid = std::min((nq + 255) / 256, c->nsm * 16);
+  const bool use_bounds = bounds != nullptr && (precision == IB_PREC_MIXED || skip_below > 0.0);
+  ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, nq, basis->lmax,
+                                   use_bounds ? bounds : nullptr, skip_below, fp32_below,
+                                   precision == IB_PREC_MIXED ? 1 : 0, ib_n_emitted_classes, c->keys.as<unsigned>(),
+                                   c->vals.as<int>(), c->status.as<int>());
+  ++*nl;
+  IB_CUDA(cudaGetLastError());
+  IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
+                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
+  ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
+                                      out_off, spherical ? 1 : 0, ib_n_emitted_classes, c->items.as<IbItem>(),
+                                      c->ranges.as<int>());
+  ++*nl;
+  IB_CUDA(cudaGetLastError());
+  IbLaunch a = base_launch(c);
+  a.items = c->items.as<IbItem>();
+  a.ranges = c->ranges.as<int>();
+  a.shell_l = basis->shell_l;
+  a.shell_k = basis->shell_k;
+  a.shell_ptr = basis->shell_ptr;
+  a.shell_xyz = basis->shell_xyz;
+  a.prim_exp = basis->prim_exp;
+  a.prim_coef = basis->prim_coef;
+  a.out = out;
+  if (precision == IB_PREC_MIXED) {
+    IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
+    IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
+    a.flags = c->flags.as<int>();
+    a.mixed_tol = mixed_tol;
+  }
+  if (use_bounds && skip_below > 0.0) {
+    ib_zero_blocks<<<c->nsm * 4, 256, 0, s>>>(a.items, a.ranges, basis->shell_l, spherical ? 1 : 0, out);
+    ++*nl;
+    IB_CUDA(cudaGetLastError());
+  }
+  return dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, nl);
+}
 }  // namespace
 
 // ================================================================ C ABI
@@ -774,60 +911,78 @@ int intception_b200_synchronize(void) {
 }
 
 int intception_b200_eri_batch(const intception_b200_basis* basis, const int* quartets, const long long* out_off,
-                              int nq, int spherical, int precision, const double* bounds, double threshold,
-                              double* out, void* stream) {
+                              int nq, int spherical, int precision, const double* bounds, double skip_below,
+                              double fp32_below, double mixed_tol, double* out, void* stream) {
   tl_launches = 0;
-  if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out)))
-    return set_status(IB_ERR_ARG, "eri_batch: null argument");
-  if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "eri_batch: basis lmax out of range");
-  if (precision != IB_PREC_FP64 && precision != IB_PREC_MIXED) return set_status(IB_ERR_ARG, "eri_batch: precision");
-  if (precision == IB_PREC_MIXED && !bounds) return set_status(IB_ERR_ARG, "eri_batch: mixed precision needs bounds");
-  if (nq == 0) return set_status(IB_OK, "");
   Context* c = nullptr;
   int st = get_context(&c);
   if (st) return st;
   std::lock_guard<std::mutex> lk(c->mu);
   cudaStream_t s;
   resolve_stream(c, stream, &s);
-  IB_CUDA(c->keys.ensure((size_t)nq * sizeof(unsigned)));
-  IB_CUDA(c->keys2.ensure((size_t)nq * sizeof(unsigned)));
-  IB_CUDA(c->vals.ensure((size_t)nq * sizeof(int)));
-  IB_CUDA(c->vals2.ensure((size_t)nq * sizeof(int)));
-  IB_CUDA(c->items.ensure((size_t)nq * sizeof(IbItem)));
-  size_t tmp_bytes = 0;
-  IB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
-                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
-  IB_CUDA(c->cub_tmp.ensure(tmp_bytes));
   int nl = 0;
-  IB_CUDA(cudaMemsetAsync(c->ranges.p, 0, kNRanges * sizeof(int), s));
-  IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
-  const int grid = std::min((nq + 255) / 256, c->nsm * 16);
-  ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, nq, basis->lmax, bounds, threshold,
-                                   precision == IB_PREC_MIXED ? 1 : 0, ib_n_emitted_classes, c->keys.as<unsigned>(),
-                                   c->vals.as<int>(), c->status.as<int>());
-  ++nl;
-  IB_CUDA(cudaGetLastError());
-  IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
-                                          c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
-  ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
-                                      out_off, spherical ? 1 : 0, ib_n_emitted_classes, c->items.as<IbItem>(),
-                                      c->ranges.as<int>());
-  ++nl;
-  IB_CUDA(cudaGetLastError());
-  IbLaunch a = base_launch(c);
-  a.items = c->items.as<IbItem>();
-  a.ranges = c->ranges.as<int>();
-  a.shell_l = basis->shell_l;
-  a.shell_k = basis->shell_k;
-  a.shell_ptr = basis->shell_ptr;
-  a.shell_xyz = basis->shell_xyz;
-  a.prim_exp = basis->prim_exp;
-  a.prim_coef = basis->prim_coef;
-  a.out = out;
-  st = dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, &nl);
+  st = batch_impl(c, basis, quartets, out_off, nq, spherical, precision, bounds, skip_below, fp32_below, mixed_tol,
+                  out, s, &nl);
   tl_launches = nl;
   if (st) return st;
   return set_status(IB_OK, "");
+}
+
+int intception_b200_schwarz(const intception_b200_basis* basis, const int* pairs, int npairs, int spherical,
+                            double* q, void* stream) {
+  if (!basis || npairs < 0 || (npairs > 0 && (!pairs || !q))) return set_status(IB_ERR_ARG, "schwarz: null argument");
+  if (npairs == 0) return set_status(IB_OK, "");
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t s;
+  resolve_stream(c, stream, &s);
+  const int chunk = 1 << 17;
+  IB_CUDA(c->sw_quartets.ensure((size_t)chunk * 4 * sizeof(int)));
+  IB_CUDA(c->sw_sizes.ensure((size_t)(chunk + 1) * sizeof(long long)));
+  IB_CUDA(c->sw_off.ensure((size_t)(chunk + 1) * sizeof(long long)));
+  size_t tmp = 0;
+  IB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, c->sw_sizes.as<long long>(), c->sw_off.as<long long>(),
+                                        chunk + 1, s));
+  IB_CUDA(c->sw_tmp.ensure(tmp));
+  for (int p0 = 0; p0 < npairs; p0 += chunk) {
+    const int n = std::min(chunk, npairs - p0);
+    const int grid = std::min((n + 255) / 256, c->nsm * 8);
+    IB_CUDA(cudaMemsetAsync(c->sw_sizes.as<long long>() + n, 0, sizeof(long long), s));
+    ib_diag_quartets<<<grid, 256, 0, s>>>(pairs + 2 * (size_t)p0, n, basis->shell_l, spherical ? 1 : 0,
+                                          c->sw_quartets.as<int>(), c->sw_sizes.as<long long>());
+    IB_CUDA(cudaGetLastError());
+    IB_CUDA(cub::DeviceScan::ExclusiveSum(c->sw_tmp.p, tmp, c->sw_sizes.as<long long>(), c->sw_off.as<long long>(),
+                                          n + 1, s));
+    long long total = 0;
+    IB_CUDA(cudaMemcpyAsync(&total, c->sw_off.as<long long>() + n, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    IB_CUDA(cudaStreamSynchronize(s));
+    IB_CUDA(c->sw_blocks.ensure((size_t)total * sizeof(double)));
+    int nl = 0;
+    st = batch_impl(c, basis, c->sw_quartets.as<int>(), c->sw_off.as<long long>(), n, spherical, IB_PREC_FP64,
+                    nullptr, 0.0, 0.0, 0.0, c->sw_blocks.as<double>(), s, &nl);
+    if (st) return st;
+    ib_diag_max<<<grid, 256, 0, s>>>(pairs + 2 * (size_t)p0, n, basis->shell_l, spherical ? 1 : 0,
+                                     c->sw_off.as<long long>(), c->sw_blocks.as<double>(), q + p0);
+    IB_CUDA(cudaGetLastError());
+  }
+  return set_status(IB_OK, "");
+}
+
+// Number of quartets of the last mixed batch whose FP32 result was rejected
+// and recomputed in FP64 (synchronous).
+int intception_b200_last_fp32_rejections(void) {
+  Context* c = nullptr;
+  if (get_context(&c)) return -1;
+  if (!c->flags.p) return 0;
+  IB_CUDA(cudaDeviceSynchronize());
+  const size_t n = c->flags.cap / sizeof(int);
+  std::vector<int> h(n);
+  IB_CUDA(cudaMemcpy(h.data(), c->flags.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  int k = 0;
+  for (int v : h) k += v != 0;
+  return k;
 }
 
 // Device status word of the last batch (reads it synchronously).

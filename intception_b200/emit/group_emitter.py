@@ -399,6 +399,37 @@ class GroupEmitter:
         L.append('    }')
         return L, max(NE, len(A) * len(B)) * NFP
 
+    def err_expr(self):
+        """FP32 error bound of the primitive quartet held in pq/F (see ib_fp32_err)."""
+        if self.orient == 'bra':
+            S, C = self.E, self.F
+            aS = 'ib_amax3(pq.PA[0], pq.PA[1], pq.PA[2]) + ib_amax3(pq.WP[0], pq.WP[1], pq.WP[2])'
+            bS = '%d.0 * (1.0 + (double)pq.roz) * (double)pq.o2z' % S
+            aC = 'ib_amax3(pq.QC[0], pq.QC[1], pq.QC[2]) + ib_amax3(pq.WQ[0], pq.WQ[1], pq.WQ[2])'
+            bC = '%d.0 * (1.0 + (double)pq.roe) * (double)pq.o2e' % C
+        else:
+            S, C = self.F, self.E
+            aS = 'ib_amax3(pq.QC[0], pq.QC[1], pq.QC[2]) + ib_amax3(pq.WQ[0], pq.WQ[1], pq.WQ[2])'
+            bS = '%d.0 * (1.0 + (double)pq.roe) * (double)pq.o2e' % S
+            aC = 'ib_amax3(pq.PA[0], pq.PA[1], pq.PA[2]) + ib_amax3(pq.WP[0], pq.WP[1], pq.WP[2])'
+            bC = '%d.0 * (1.0 + (double)pq.roz) * (double)pq.o2z' % C
+        tC = '%d.0 * (double)pq.o2zpe' % S
+        return 'ib_fp32_err(F[0], %s, %s, %d, %s, %s, %s, %d)' % (aS, bS, S, aC, bC, tC, C)
+
+    def amp_expr(self):
+        """Growth of an accumulator error through the HRRs and transforms."""
+        from intception_b200.basis import sph_matrix
+        import numpy as np
+        sph = 1.0
+        for l in (self.la, self.lb, self.lc, self.ld):
+            sph *= float(np.abs(sph_matrix(l)).sum(axis=0).max())
+        parts = []
+        for _ in range(self.lb):
+            parts.append('(1.0 + ib_amax3(g.AB[0], g.AB[1], g.AB[2]))')
+        for _ in range(self.ld):
+            parts.append('(1.0 + ib_amax3(g.CD[0], g.CD[1], g.CD[2]))')
+        return ' * '.join(parts + ['(SPH ? %.17g : 1.0)' % sph])
+
     # -------------------------------------------------------------- kernel
     def kernel(self):
         chain, NT = self.emit_chain()
@@ -464,11 +495,14 @@ class GroupEmitter:
         src.append('  const int src0 = li.src[0], src1 = li.src[1], src2 = li.src[2];')
         src.append('  (void)src0; (void)src1; (void)src2;')
         src.append('  for (int p = beg + (int)blockIdx.x * QPB + gid; p < end; p += (int)gridDim.x * QPB) {')
+        src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // group-uniform')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
         src.append('    double acc[%d];' % NT)
         src.append('#pragma unroll')
         src.append('    for (int k = 0; k < %d; ++k) acc[k] = 0.0;' % NT)
+        src.append('    double est = 0.0;  // FP32 rounding-error bound accumulated over primitive quartets')
+        src.append('    (void)est;')
         L = self.L
         fields = ['PA[0]', 'PA[1]', 'PA[2]', 'WP[0]', 'WP[1]', 'WP[2]', 'QC[0]', 'QC[1]', 'QC[2]',
                   'WQ[0]', 'WQ[1]', 'WQ[2]', 'o2z', 'roz', 'o2e', 'roe', 'o2zpe']
@@ -487,6 +521,7 @@ class GroupEmitter:
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
             src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq)) continue;' % L)
+            src.append('        if (sizeof(R) == 4) est += %s;' % self.err_expr())
             for f, nm in zip(fields, names):
                 src.append('        const R %s = pq.%s;' % (nm, f))
             for m in range(L + 1):
@@ -514,6 +549,7 @@ class GroupEmitter:
                 src.append('            ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
             for m in range(L + 1):
                 src.append('            ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
+            src.append('            if (sizeof(R) == 4) est += %s;' % self.err_expr())
             src.append('          }')
             src.append('          pz[j] = live ? 1 : 0;')
             src.append('        }')
@@ -564,6 +600,23 @@ class GroupEmitter:
             src.append('      }')
             src.append('      %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
             src.append('    }')
+        # FP32: sum the error bound over the group, reject the quartet if too large
+        src.append('    if (sizeof(R) == 4) {')
+        if self.G > 1 and not self.wide:
+            src.append('      for (int o = %d; o > 0; o >>= 1) est += __shfl_xor_sync(gmask, est, o, %d);'
+                       % (self.G // 2, self.G))
+        elif self.wide:
+            src.append('      for (int o = 16; o > 0; o >>= 1) est += __shfl_xor_sync(0xffffffffu, est, o);')
+            src.append('      ib_group_bar(gid);')
+            src.append('      if ((j & 31) == 0) sb[j >> 5] = est;')
+            src.append('      ib_group_bar(gid);')
+            src.append('      est = sb[0] + sb[1];')
+            src.append('      ib_group_bar(gid);')
+        src.append('      if (est * %s > a.mixed_tol) {' % self.amp_expr())
+        src.append('        if (j == 0) a.flags[p] = 1;')
+        src.append('        continue;  // group-uniform: the FP64 pass recomputes and stores this quartet')
+        src.append('      }')
+        src.append('    }')
         # accumulators -> shared [e][f]
         if bra:
             src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))

@@ -84,9 +84,14 @@ def load():
     lib.intception_b200_boys_batch.restype = C.c_int
     lib.intception_b200_synchronize.restype = C.c_int
     lib.intception_b200_batch_status.restype = C.c_int
+    lib.intception_b200_last_fp32_rejections.restype = C.c_int
     lib.intception_b200_eri_batch.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
-                                              C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+                                              C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                              C.c_void_p]
     lib.intception_b200_eri_batch.restype = C.c_int
+    lib.intception_b200_schwarz.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                            C.c_void_p]
+    lib.intception_b200_schwarz.restype = C.c_int
     lib.intception_b200_eri_batch_noalloc.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int,
                                                       C.c_int, C.c_void_p, C.c_void_p]
     lib.intception_b200_eri_batch_noalloc.restype = C.c_int
@@ -202,8 +207,13 @@ class EriEngine:
         self.out_size = b.out_size
         load()
 
-    def compute(self, out=None, precision=PREC_FP64, bounds=None, threshold=0.0, stream=None, quartets=None,
-                out_off=None, nq=None):
+    def compute(self, out=None, precision=PREC_FP64, bounds=None, skip_below=0.0, fp32_below=0.0, mixed_tol=5e-11,
+                stream=None, quartets=None, out_off=None, nq=None):
+        """Evaluate the quartet list (or the given one) into out.  bounds: per
+        quartet |(ab|cd)| upper bounds (torch float64, device); quartets below
+        skip_below are written as zeros; with PREC_MIXED those below
+        fp32_below use the FP32 VRR, and any whose FP32 error bound exceeds
+        mixed_tol is recomputed in FP64."""
         torch = self.torch
         if out is None:
             out = torch.empty(self.out_size, dtype=torch.float64, device=self.device)
@@ -213,14 +223,36 @@ class EriEngine:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         st = load().intception_b200_eri_batch(
             C.byref(self._basis), q.data_ptr(), o.data_ptr(), n, 1 if self.spherical else 0, precision,
-            bounds.data_ptr() if bounds is not None else None, float(threshold), out.data_ptr(),
-            C.c_void_p(s.cuda_stream))
+            bounds.data_ptr() if bounds is not None else None, float(skip_below), float(fp32_below), float(mixed_tol),
+            out.data_ptr(), C.c_void_p(s.cuda_stream))
         _check(st)
         return out
+
+    def schwarz(self, pairs, stream=None):
+        """sqrt(max |(ij|ij)|) for shell pairs (torch int32 [n, 2], device)."""
+        torch = self.torch
+        pairs = pairs.contiguous()
+        q = torch.empty(pairs.shape[0], dtype=torch.float64, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        _check(load().intception_b200_schwarz(C.byref(self._basis), pairs.data_ptr(), pairs.shape[0],
+                                              1 if self.spherical else 0, q.data_ptr(), C.c_void_p(s.cuda_stream)))
+        return q
+
+    def quartet_bounds(self, stream=None):
+        """Schwarz bound of every quartet of the batch: q_ab * q_cd."""
+        torch = self.torch
+        qv = self.quartets.view(-1, 4)
+        pairs = torch.cat([qv[:, 0:2], qv[:, 2:4]]).contiguous()
+        q = self.schwarz(pairs, stream)
+        return (q[:self.nq] * q[self.nq:]).contiguous()
 
     @staticmethod
     def last_launch_count():
         return load().intception_b200_last_launch_count()
+
+    @staticmethod
+    def fp32_rejected():
+        return load().intception_b200_last_fp32_rejections()
 
     @staticmethod
     def device_status():

@@ -130,3 +130,57 @@ def test_permutational_symmetry_large():
         x = out[b.out_off[q]:b.out_off[q] + na * nb * nc * nd].reshape(nd, nc, nb, na)
         y = out2[b2.out_off[q]:b2.out_off[q] + na * nb * nc * nd].reshape(nb, na, nd, nc)
         assert np.abs(x - y.transpose(2, 3, 0, 1)).max() <= 1e-13 * max(1.0, np.abs(x).max())
+
+
+def _block_max(b, x):
+    sizes = basis.block_sizes(b.shell_l, b.quartets, b.spherical)
+    seg = np.repeat(np.arange(b.nq), sizes)
+    m = np.zeros(b.nq)
+    np.maximum.at(m, seg, np.abs(x))
+    return m
+
+
+def test_schwarz_bounds_hold():
+    """|(ab|cd)| <= q_ab q_cd for every element (compact 8-bohr box, so most
+    bounds are far from zero)."""
+    import torch
+    b = basis.independent_quartet_batch(51, 20000, [0, 1, 2], [1, 2, 3, 4], 0.05, 1e4, 8.0, True)
+    eng = eri.EriEngine(b)
+    ref = eng.compute()
+    bounds = eng.quartet_bounds()
+    torch.cuda.synchronize()
+    m = _block_max(b, ref.cpu().numpy())
+    bd = bounds.cpu().numpy()
+    assert np.all(m <= bd * (1 + 1e-10) + 1e-300)
+    # the factors match an explicit diagonal evaluation for a few pairs
+    for p in (0, 7, 1234):
+        a, bb = b.quartets[p, 0], b.quartets[p, 1]
+        q = np.array([[a, bb, a, bb]], np.int32)
+        off, tot = basis.packed_offsets(b.shell_l, q, True)
+        sub = basis.ShellBatch(b.shell_l, b.shell_k, b.shell_ptr, b.shell_xyz, b.prim_exp, b.prim_coef, q, off,
+                               True, tot)
+        blk = loader.oracle_batch(sub, basis.sph_matrices(6))
+        na, nb = 2 * b.shell_l[a] + 1, 2 * b.shell_l[bb] + 1
+        diag = max(abs(blk[i + na * (j + nb * (i + na * j))]) for i in range(na) for j in range(nb))
+        qab = float(eng.schwarz(torch.tensor([[a, bb]], dtype=torch.int32, device='cuda'))[0])
+        assert abs(qab - np.sqrt(diag)) <= 1e-12 * max(1.0, np.sqrt(diag))
+
+
+def test_screened_and_mixed_paths_meet_error_bar():
+    """l<=2 spherical workload (30-bohr cube): screening writes zeros below
+    1e-12 (error <= bound), the mixed path keeps the max abs error <= 1e-10."""
+    import torch
+    b = basis.config_mixed_l2(nq=50000, seed=21, spherical=True)
+    eng = eri.EriEngine(b)
+    ref = eng.compute().clone()
+    bounds = eng.quartet_bounds()
+    scr = eng.compute(bounds=bounds, skip_below=1e-12).clone()
+    mix = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, skip_below=1e-12, fp32_below=1e-4,
+                      mixed_tol=5e-11).clone()
+    torch.cuda.synchronize()
+    assert eng.device_status() == 0
+    r = ref.cpu().numpy()
+    assert np.abs(scr.cpu().numpy() - r).max() <= 1e-12
+    assert np.abs(mix.cpu().numpy() - r).max() <= 1e-10
+    kept = (bounds >= 1e-12).double().mean().item()
+    assert 0.0 < kept < 1.0
