@@ -171,6 +171,27 @@ int intception_b200_batch_status(void);
 int intception_b200_eri_batch_noalloc(const intception_b200_basis *basis, const int *quartets,
                                       const long long *out_off, int nq, int spherical, double *out, void *stream);
 
+/* Density digestion (device pointers, asynchronous on stream).  quartets are
+ * unique shell quartets (a>=b, c>=d, each pair-pair once), standing for their
+ * 8-fold permutation families; blocks/out_off are their Cartesian ERI blocks
+ * (a fastest); fofs[s] is the first Cartesian function of shell s; P the
+ * symmetric nbf x nbf Cartesian density.  Adds E_J = 1/2 sum P_ij P_kl (ij|kl)
+ * to e_out[0] and E_K = -1/4 sum P_ik P_jl (ij|kl) to e_out[1]. */
+int intception_b200_jk_energy(const int *quartets, const long long *out_off, int nq, const int *shell_l,
+                              const int *fofs, const double *P, int nbf, const double *blocks, double *e_out,
+                              void *stream);
+
+/* Nuclear-gradient digestion of one auxiliary batch: for the quartets
+ * quartets[qidx[k]], centre pos (0..2) raised (sign +1: shell of l+1 with
+ * coefficients 2 alpha c) or lowered (sign -1: l-1), Cartesian blocks at
+ * blocks + aux_off[k].  Adds d(E_J + E_K)/dR of centre pos to its atom and the
+ * opposite to the atom of centre 3 (translational invariance) in
+ * force[3*atom + xyz]; natom <= 4096.  The shell arrays are indexed with the
+ * original shell numbers of quartets. */
+int intception_b200_jk_force(const int *quartets, const int *qidx, const long long *aux_off, int naux, int pos,
+                             int sign, const int *shell_l, const int *fofs, const int *shell_atom, const double *P,
+                             int nbf, int natom, const double *blocks, double *force, void *stream);
+
 /* The library's Cartesian->spherical matrix for l (host memory,
  * T[icart + isph*ncart], ncart x (2l+1)). */
 int intception_b200_sph_matrix(int l, double *T);

@@ -1,0 +1,214 @@
+// ib_jk.cu -- density digestion of ERI blocks: J/K energies and their nuclear
+// gradient (the adjoint of the integral evaluation with respect to centres).
+//
+// Quartets are unique shell quartets (a>=b, c>=d, pair(ab)>=pair(cd) in the
+// caller's ordering), each standing for its 8-fold permutation family with
+// degeneracy deg = (a!=b ? 2:1)(c!=d ? 2:1)(ab!=cd ? 2:1).  With a real
+// symmetric density P (Cartesian basis):
+//   E_J = 1/2 sum_ijkl P_ij P_kl (ij|kl),   E_K = -1/4 sum_ijkl P_ik P_jl (ij|kl)
+// so the symmetrised weight of one element is
+//   D_ijkl = 1/2 P_ij P_kl - 1/8 (P_ik P_jl + P_il P_jk).
+// Gradient: d/dA_x of a primitive x^ax y^ay z^az exp(-alpha r_A^2) is
+//   2 alpha [a+1x] - ax [a-1x],
+// so dE/dA_x = sum deg D (a~+1x b|cd) - ax D (a-1x b|cd), with a~ the shell with
+// coefficients 2 alpha c and l+1.  The caller evaluates those auxiliary
+// blocks with the ERI kernels; these kernels map every auxiliary element back
+// to the component it differentiates and accumulate the atom's force, and
+// the opposite contribution on centre D (translational invariance).
+#include <cuda_runtime.h>
+
+#include "../../include/intception_b200.h"
+#include "ib_generic.cuh"
+
+namespace {
+
+__device__ __forceinline__ void jk_comp(int l, int k, int& x, int& y, int& z) {
+  int s = 0;
+  while ((s + 1) * (s + 2) / 2 <= k) ++s;
+  z = k - s * (s + 1) / 2;
+  y = s - z;
+  x = l - s;
+}
+
+__device__ __forceinline__ int jk_index(int x, int y, int z) { return z + (y + z) * (y + z + 1) / 2; }
+
+__device__ __forceinline__ double jk_weight(const double* __restrict__ P, int n, int i, int j, int k, int l) {
+  const double pij = __ldg(P + (size_t)i * n + j), pkl = __ldg(P + (size_t)k * n + l);
+  const double pik = __ldg(P + (size_t)i * n + k), pjl = __ldg(P + (size_t)j * n + l);
+  const double pil = __ldg(P + (size_t)i * n + l), pjk = __ldg(P + (size_t)j * n + k);
+  return 0.5 * pij * pkl - 0.125 * (pik * pjl + pil * pjk);
+}
+
+__device__ __forceinline__ double jk_deg(const int* s) {
+  return (s[0] != s[1] ? 2.0 : 1.0) * (s[2] != s[3] ? 2.0 : 1.0) * ((s[0] != s[2] || s[1] != s[3]) ? 2.0 : 1.0);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One warp per quartet; e_out[0] += E_J part, e_out[1] += E_K part.
+__global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long long* __restrict__ out_off, int nq,
+                                    const int* __restrict__ shell_l, const int* __restrict__ fofs,
+                                    const double* __restrict__ P, int nbf, const double* __restrict__ blocks,
+                                    double* __restrict__ e_out) {
+  __shared__ double red[2][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
+  double ej = 0.0, ek = 0.0;
+  for (int q = warp; q < nq; q += nwarp) {
+    int s[4], n[4], f[4];
+    for (int i = 0; i < 4; ++i) {
+      s[i] = quartets[4 * q + i];
+      n[i] = ib_ncart(shell_l[s[i]]);
+      f[i] = fofs[s[i]];
+    }
+    const double deg = jk_deg(s);
+    const double* blk = blocks + out_off[q];
+    const int tot = n[0] * n[1] * n[2] * n[3];
+    double pj = 0.0, pk = 0.0;
+    for (int e = lane; e < tot; e += 32) {
+      const int ia = e % n[0], r1 = e / n[0];
+      const int ib = r1 % n[1], r2 = r1 / n[1];
+      const int ic = r2 % n[2], id = r2 / n[2];
+      const int i = f[0] + ia, j = f[1] + ib, k = f[2] + ic, l = f[3] + id;
+      const double v = blk[e];
+      pj += __ldg(P + (size_t)i * nbf + j) * __ldg(P + (size_t)k * nbf + l) * v;
+      pk += (__ldg(P + (size_t)i * nbf + k) * __ldg(P + (size_t)j * nbf + l) +
+             __ldg(P + (size_t)i * nbf + l) * __ldg(P + (size_t)j * nbf + k)) * v;
+    }
+    ej += 0.5 * deg * pj;
+    ek -= 0.125 * deg * pk;
+  }
+  ej = warp_sum(ej);
+  ek = warp_sum(ek);
+  if (lane == 0) {
+    red[0][wib] = ej;
+    red[1][wib] = ek;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    atomicAdd(e_out, a);
+    atomicAdd(e_out + 1, b);
+  }
+}
+
+// Gradient contribution of one auxiliary batch: centre `pos` (0..2) of each
+// listed quartet carries level l+1 (sign > 0, shell coefficients 2 alpha c)
+// or l-1 (sign < 0).  aux_off[k] locates the auxiliary block of quartet
+// qidx[k] of the unique quartet list.  Forces accumulate in shared memory per
+// atom and are flushed once per block.
+__global__ void ib_jk_force_kernel(const int* __restrict__ quartets, const int* __restrict__ qidx,
+                                   const long long* __restrict__ aux_off, int naux, int pos, int sign,
+                                   const int* __restrict__ shell_l, const int* __restrict__ fofs,
+                                   const int* __restrict__ shell_atom, const double* __restrict__ P, int nbf,
+                                   int natom, const double* __restrict__ blocks, double* __restrict__ force) {
+  extern __shared__ double fs[];
+  for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x) fs[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < naux; k += nwarp) {
+    const int q = qidx[k];
+    int s[4], l[4], n[4], f[4];
+    for (int i = 0; i < 4; ++i) {
+      s[i] = quartets[4 * q + i];
+      l[i] = shell_l[s[i]];
+      f[i] = fofs[s[i]];
+      n[i] = ib_ncart(l[i]);
+    }
+    const int lx = l[pos] + (sign > 0 ? 1 : -1);
+    int na[4] = {n[0], n[1], n[2], n[3]};
+    na[pos] = ib_ncart(lx);
+    const double deg = jk_deg(s);
+    const double* blk = blocks + aux_off[k];
+    const int tot = na[0] * na[1] * na[2] * na[3];
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int e = lane; e < tot; e += 32) {
+      int idx[4];
+      int r = e;
+      for (int i = 0; i < 4; ++i) {
+        idx[i] = r % na[i];
+        r /= na[i];
+      }
+      const double v = deg * blk[e];
+      int cx, cy, cz;
+      jk_comp(lx, idx[pos], cx, cy, cz);
+      int c[3] = {cx, cy, cz};
+      for (int d = 0; d < 3; ++d) {
+        int o[3] = {c[0], c[1], c[2]};
+        double coef;
+        if (sign > 0) {
+          if (o[d] == 0) continue;
+          o[d] -= 1;
+          coef = 1.0;
+        } else {
+          o[d] += 1;
+          coef = -(double)o[d];
+        }
+        int fi[4] = {f[0] + idx[0], f[1] + idx[1], f[2] + idx[2], f[3] + idx[3]};
+        fi[pos] = f[pos] + jk_index(o[0], o[1], o[2]);
+        g[d] += coef * v * jk_weight(P, nbf, fi[0], fi[1], fi[2], fi[3]);
+      }
+    }
+    for (int d = 0; d < 3; ++d) g[d] = warp_sum(g[d]);
+    if (lane == 0) {
+      const int ax = shell_atom[s[pos]], ad = shell_atom[s[3]];
+      for (int d = 0; d < 3; ++d) {
+        atomicAdd(&fs[3 * ax + d], g[d]);
+        atomicAdd(&fs[3 * ad + d], -g[d]);  // translational invariance: d/dD = -(d/dA + d/dB + d/dC)
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x)
+    if (fs[i] != 0.0) atomicAdd(force + i, fs[i]);
+}
+
+}  // namespace
+
+extern "C" int intception_b200_jk_energy(const int* quartets, const long long* out_off, int nq, const int* shell_l,
+                                         const int* fofs, const double* P, int nbf, const double* blocks,
+                                         double* e_out, void* stream) {
+  if (nq < 0 || (nq > 0 && (!quartets || !out_off || !shell_l || !fofs || !P || !blocks || !e_out)))
+    return IB_ERR_ARG;
+  if (nq == 0) return IB_OK;
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return IB_ERR_NODEVICE;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int threads = 256, wpb = threads / 32;
+  int blocks_n = (nq + wpb - 1) / wpb;
+  if (blocks_n > nsm * 16) blocks_n = nsm * 16;
+  ib_jk_energy_kernel<<<blocks_n, threads, 0, static_cast<cudaStream_t>(stream)>>>(quartets, out_off, nq, shell_l,
+                                                                                  fofs, P, nbf, blocks, e_out);
+  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+}
+
+extern "C" int intception_b200_jk_force(const int* quartets, const int* qidx, const long long* aux_off, int naux,
+                                        int pos, int sign, const int* shell_l, const int* fofs,
+                                        const int* shell_atom, const double* P, int nbf, int natom,
+                                        const double* blocks, double* force, void* stream) {
+  if (naux < 0 || pos < 0 || pos > 2 || (sign != 1 && sign != -1) || natom < 1 || natom > 4096) return IB_ERR_ARG;
+  if (naux == 0) return IB_OK;
+  if (!quartets || !qidx || !aux_off || !shell_l || !fofs || !shell_atom || !P || !blocks || !force)
+    return IB_ERR_ARG;
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return IB_ERR_NODEVICE;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = sizeof(double) * 3 * (size_t)natom;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(ib_jk_force_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return IB_ERR_CUDA;
+  const int threads = 256, wpb = threads / 32;
+  int blocks_n = (naux + wpb - 1) / wpb;
+  if (blocks_n > nsm * 8) blocks_n = nsm * 8;
+  ib_jk_force_kernel<<<blocks_n, threads, smem, static_cast<cudaStream_t>(stream)>>>(
+      quartets, qidx, aux_off, naux, pos, sign, shell_l, fofs, shell_atom, P, nbf, natom, blocks, force);
+  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+}
