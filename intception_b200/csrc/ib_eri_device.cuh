@@ -66,8 +66,9 @@ typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch
 typedef int (*IbOccFn)(int variant);
 struct IbClassEntry {
   int cid;
-  IbLaunchFn launch;
+  IbLaunchFn launch;    // null: no unrolled kernel (the generic kernel serves the class)
   IbOccFn occupancy;
+  int kind;             // 1: FP64 variants only, 2: FP64 and FP32 variants
 };
 
 __host__ __device__ inline constexpr double ib_two_pi52() { return 34.98683665524972497; }  // 2 pi^(5/2)

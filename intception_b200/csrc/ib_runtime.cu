@@ -43,7 +43,7 @@ constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 cop
 constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
 constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
 constexpr int kNRanges = 4 * IB_NCLASS + 4;
-constexpr int kKeyBits = 23;                    // skip(1) fp32(1) class(9) Kab(6) Kcd(6)
+constexpr int kKeyBits = 24;                    // skip(1) generic(1) fp32(1) class(9) Kab(6) Kcd(6)
 constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
 
 thread_local int tl_status = IB_OK;
@@ -107,6 +107,7 @@ struct Context {
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;                                             // FP32 rejections of the last mixed batch
+  DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
   DevBuf d_stage, d_cart, d_res;
   HostBuf h_stage, h_res;
   IbClassEntry table[IB_NCLASS] = {};
@@ -145,8 +146,8 @@ __device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
 
 __global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
                             const int* __restrict__ shell_k, int nq, int lmax, const double* __restrict__ bounds,
-                            double skip_below, double thr, int mixed, int n_emit, unsigned* __restrict__ keys,
-                            int* __restrict__ vals, int* status) {
+                            double skip_below, double thr, int mixed, const int* __restrict__ kind,
+                            unsigned* __restrict__ keys, int* __restrict__ vals, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], st[4] = {0, 0, 0, 0};
     bool bad = false;
@@ -164,17 +165,19 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int cid = pb * (pb + 1) / 2 + pk;
     const int kab = min(shell_k[s[0]] * shell_k[s[1]], 63), kcd = min(shell_k[s[2]] * shell_k[s[3]], 63);
     const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
-    const int fp32 = (!skip && mixed && cid < n_emit && bounds[q] < thr) ? 1 : 0;
-    keys[q] = (unsigned(skip) << 22) | (unsigned(fp32) << 21) | (unsigned(cid) << 12) | (unsigned(kab) << 6) |
-              unsigned(kcd);
+    const int k = kind[cid];
+    const int gen = (!skip && k == 0) ? 1 : 0;
+    const int fp32 = (!skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
+    keys[q] = (unsigned(skip) << 23) | (unsigned(gen) << 22) | (unsigned(fp32) << 21) | (unsigned(cid) << 12) |
+              (unsigned(kab) << 6) | unsigned(kcd);
     vals[q] = q;
   }
 }
 
 __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __restrict__ order, int nq,
                                const int* __restrict__ quartets, const int* __restrict__ shell_l,
-                               const long long* __restrict__ out_off, int spherical, int n_emit,
-                               IbItem* __restrict__ items, int* __restrict__ ranges) {
+                               const long long* __restrict__ out_off, int spherical, IbItem* __restrict__ items,
+                               int* __restrict__ ranges) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
     const int q = order[p];
     int s[4], l[4], n[4];
@@ -193,23 +196,23 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     it.off = out_off[q];
     items[p] = it;
     const unsigned key = keys[p];
-    const int slot = (int)(key >> 12);  // skip bit * 1024 + fp32 bit * 512 + cid
+    const int slot = (int)(key >> 12);  // skip*2048 + generic*1024 + fp32*512 + cid
     const int prev = p > 0 ? (int)(keys[p - 1] >> 12) : -1;
     const int next = p + 1 < nq ? (int)(keys[p + 1] >> 12) : -1;
-    if (slot >> 10) {  // screened out: one range for all of them, sorted last
-      if (prev < 0 || !(prev >> 10)) ranges[kSlotSkip] = p;
+    if (slot >> 11) {  // screened out: one range for all of them, sorted last
+      if (prev < 0 || !(prev >> 11)) ranges[kSlotSkip] = p;
       if (next < 0) ranges[kSlotSkip + 1] = p + 1;
+      continue;
+    }
+    if ((slot >> 10) & 1) {  // no unrolled kernel: one contiguous range for the generic kernel
+      if (prev < 0 || !((prev >> 10) & 1)) ranges[kSlotGeneric] = p;
+      if (next < 0 || ((next >> 10) & 3) != 1) ranges[kSlotGeneric + 1] = p + 1;
       continue;
     }
     const int cid = slot & 511, fp32 = (slot >> 9) & 1;
     const int rs = 2 * (cid + fp32 * IB_NCLASS);
     if (prev != slot) ranges[rs] = p;
     if (next != slot) ranges[rs + 1] = p + 1;
-    const bool gen = (fp32 == 0 && cid >= n_emit);
-    const bool gprev = p > 0 && ((prev >> 9) == 0) && ((prev & 511) >= n_emit);
-    const bool gnext = p + 1 < nq && ((next >> 9) == 0) && ((next & 511) >= n_emit);
-    if (gen && !gprev) ranges[kSlotGeneric] = p;
-    if (gen && !gnext) ranges[kSlotGeneric + 1] = p + 1;
   }
 }
 
@@ -358,10 +361,14 @@ int get_context(Context** out) {
     IB_CUDA(c->status.ensure(sizeof(int)));
     IB_CUDA(cudaMemset(c->status.p, 0, sizeof(int)));
     ib_register_emitted_classes(c->table);
-    for (int cid = 0; cid < ib_n_emitted_classes; ++cid)
-      for (int v = 0; v < 4; ++v) {
-        c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
-      }
+    std::vector<int> kind(IB_NCLASS, 0);
+    for (int cid = 0; cid < IB_NCLASS; ++cid) {
+      if (!c->table[cid].launch) continue;
+      kind[cid] = c->table[cid].kind;
+      for (int v = 0; v < 4; ++v) c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
+    }
+    IB_CUDA(c->kind.ensure(IB_NCLASS * sizeof(int)));
+    IB_CUDA(cudaMemcpy(c->kind.p, kind.data(), IB_NCLASS * sizeof(int), cudaMemcpyHostToDevice));
     IB_CUDA(cudaGetLastError());
     g_ctx[dev] = c;
   }
@@ -404,7 +411,9 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     if (prec == 1) ap.ranges = a.ranges + kSlotFp32;
     const int variant = prec * 2 + (sph ? 1 : 0);
     // heaviest classes first so they start early on their streams
-    for (int cid = ib_n_emitted_classes - 1; cid >= 0; --cid) {
+    for (int cid = IB_NCLASS - 1; cid >= 0; --cid) {
+      if (!c->table[cid].launch) continue;
+      if (prec == 1 && c->table[cid].kind != 2) continue;
       const int grid = c->nsm * c->occ[cid][variant];
       cudaStream_t ss = c->side[k % kNSide];
       c->table[cid].launch(variant, grid, ss, ap);
@@ -555,7 +564,7 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
           hit[b] = it;
         }
   std::memset(hrg, 0, kNRanges * sizeof(int));
-  const bool emitted = cid < ib_n_emitted_classes;
+  const bool emitted = c->table[cid].launch != nullptr;
   if (emitted) {
     hrg[2 * cid] = 0;
     hrg[2 * cid + 1] = nblk;
@@ -758,14 +767,14 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   const bool use_bounds = bounds != nullptr && (precision == IB_PREC_MIXED || skip_below > 0.0);
   ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, nq, basis->lmax,
                                    use_bounds ? bounds : nullptr, skip_below, fp32_below,
-                                   precision == IB_PREC_MIXED ? 1 : 0, ib_n_emitted_classes, c->keys.as<unsigned>(),
+                                   precision == IB_PREC_MIXED ? 1 : 0, c->kind.as<int>(), c->keys.as<unsigned>(),
                                    c->vals.as<int>(), c->status.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());
   IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
                                           c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
   ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
-                                      out_off, spherical ? 1 : 0, ib_n_emitted_classes, c->items.as<IbItem>(),
+                                      out_off, spherical ? 1 : 0, c->items.as<IbItem>(),
                                       c->ranges.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());

@@ -406,23 +406,37 @@ class Emitter:
         return '\n'.join(src), stats
 
 
-def emit_all(outdir, lmax=LMAX_EMIT, ngroups=6):
+def emitted_classes():
+    """Canonical classes with an unrolled kernel: every class with l <= 2, and
+    the classes with one f shell and the rest <= d (FP64 only), which the
+    nuclear-gradient batches of an l <= 2 basis reach."""
+    out = [(c, True) for c in canonical_classes(LMAX_EMIT)]
+    pairs = [(a, b) for a in range(3) for b in range(a + 1)]
+    for lb in range(3):
+        for (lc, ld) in pairs:
+            out.append(((3, lb, lc, ld), False))
+    out.sort(key=lambda x: class_id(*x[0]))
+    return out
+
+
+def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
     """Write the class translation units and the dispatch table into outdir.
     Returns the list of per-class statistics."""
     os.makedirs(outdir, exist_ok=True)
-    classes = canonical_classes(lmax)
+    classes = emitted_classes()
     # balance translation units by emitted size (largest classes first)
     from .group_emitter import GroupEmitter, orientation
     bodies = []
-    for c in classes:
+    for c, fp32 in classes:
         # the one-thread schedule's counts are the algorithmic work of the class
         tbody, st = Emitter(*c).kernel()
         if orientation(*c) is not None and c not in THREAD_CLASSES:
-            body, gst = GroupEmitter(*c).kernel()
+            body, gst = GroupEmitter(*c).kernel(fp32=fp32)
             st.update(kind='group', G=gst['G'], orient=gst['orient'], lane_flops=gst['lane_flops'])
         else:
             body = tbody
             st['kind'] = 'thread'
+        st['fp32'] = fp32
         bodies.append((c, body, st))
     order = sorted(bodies, key=lambda x: -len(x[1]))
     groups = [[] for _ in range(ngroups)]
@@ -442,8 +456,8 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=6):
             regs.append(st)
         parts.append('void ib_register_group_%d(IbClassEntry* table) {' % g)
         for st in regs:
-            parts.append('  table[%d] = IbClassEntry{%d, &ib_launch_%s, &ib_occupancy_%s};'
-                         % (st['cid'], st['cid'], st['tag'], st['tag']))
+            parts.append('  table[%d] = IbClassEntry{%d, &ib_launch_%s, &ib_occupancy_%s, %d};'
+                         % (st['cid'], st['cid'], st['tag'], st['tag'], 2 if st['fp32'] else 1))
         parts.append('}')
         _write_if_changed(path, '\n'.join(parts) + '\n')
         written.append(path)

@@ -431,7 +431,9 @@ class GroupEmitter:
         return ' * '.join(parts + ['(SPH ? %.17g : 1.0)' % sph])
 
     # -------------------------------------------------------------- kernel
-    def kernel(self):
+    def kernel(self, fp32=True):
+        """CUDA source of the class kernel and its launcher; fp32=False
+        instantiates the FP64 variants only (FP32 requests run in FP64)."""
         chain, NT = self.emit_chain()
         epi_cart, sm_cart = self.emit_epilogue(False)
         epi_sph, sm_sph = self.emit_epilogue(True)
@@ -649,14 +651,17 @@ class GroupEmitter:
         src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
         src.append('  const size_t smem = ib_smem_%s();' % t)
         src.append('  switch (variant) {')
-        for v, (R, S) in enumerate((('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))):
+        variants = (('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))
+        if not fp32:
+            variants = variants[:2] * 2
+        for v, (R, S) in enumerate(variants):
             src.append('    case %d: ib_eri_%s<%s, %s><<<grid, IB_BLOCK, smem, s>>>(a); break;' % (v, t, R, S))
         src.append('  }')
         src.append('}')
         src.append('static int ib_occupancy_%s(int variant) {' % t)
         src.append('  int n = 0; const size_t smem = ib_smem_%s();' % t)
         src.append('  switch (variant) {')
-        for v, (R, S) in enumerate((('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))):
+        for v, (R, S) in enumerate(variants):
             src.append('    case %d: cudaFuncSetAttribute(ib_eri_%s<%s, %s>, cudaFuncAttributeMaxDynamicSharedMemorySize, '
                        '(int)smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ib_eri_%s<%s, %s>, IB_BLOCK, '
                        'smem); break;' % (v, t, R, S, t, R, S))
