@@ -135,6 +135,20 @@ int intception_b200_eri_batch(const intception_b200_basis *basis, const int *qua
                               int nq, int spherical, int precision, const double *bounds, double skip_below,
                               double fp32_below, double mixed_tol, double *out, void *stream);
 
+/* CUDA graph of one intception_b200_eri_batch call (same arguments, fixed
+ * device pointers and sizes): the class sort, item build and every class kernel
+ * with its side-stream fork/join are captured once and replayed with a single
+ * launch.  create runs the batch once eagerly (sizing the work buffers, so the
+ * capture allocates nothing) and once under capture; launch replays it on
+ * stream; replays read the inputs' current contents.  The graph uses the
+ * library's shared work buffers: do not run it concurrently with other batches. */
+int intception_b200_eri_graph_create(const intception_b200_basis *basis, const int *quartets,
+                                     const long long *out_off, int nq, int spherical, int precision,
+                                     const double *bounds, double skip_below, double fp32_below, double mixed_tol,
+                                     double *out, void **handle);
+int intception_b200_eri_graph_launch(void *handle, void *stream);
+int intception_b200_eri_graph_destroy(void *handle);
+
 /* Schwarz factors q[p] = sqrt(max_ij |(ij|ij)|) of the shell pairs
  * pairs[2p], pairs[2p+1] (device pointers), so that |(ab|cd)| <= q_ab q_cd for
  * every function of the quartet; spherical selects the function set the

@@ -16,6 +16,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -38,7 +39,7 @@ __global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double
 
 namespace {
 
-constexpr int kNSide = 8;                       // side streams for concurrent class kernels
+constexpr int kNSideMax = 64;                   // side streams for concurrent class kernels (upper limit)
 constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 copies
 constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
 constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
@@ -102,8 +103,9 @@ struct Context {
   int device = -1;
   int nsm = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t side[kNSide] = {};
-  cudaEvent_t fork = nullptr, join[kNSide] = {};
+  int nside = 40;  // INTCEPTION_B200_STREAMS, 1..64: enough for every class kernel to run concurrently
+  cudaStream_t side[kNSideMax] = {};
+  cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;                                             // FP32 rejections of the last mixed batch
@@ -168,8 +170,9 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int k = kind[cid];
     const int gen = (!skip && k == 0) ? 1 : 0;
     const int fp32 = (!skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
+    // primitive-pair counts descending inside a class: the longest quartets start first
     keys[q] = (unsigned(skip) << 23) | (unsigned(gen) << 22) | (unsigned(fp32) << 21) | (unsigned(cid) << 12) |
-              (unsigned(kab) << 6) | unsigned(kcd);
+              (unsigned(63 - kab) << 6) | unsigned(63 - kcd);
     vals[q] = q;
   }
 }
@@ -346,7 +349,8 @@ int get_context(Context** out) {
     c->device = dev;
     IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    for (int i = 0; i < kNSide; ++i) {
+    if (const char* env = std::getenv("INTCEPTION_B200_STREAMS")) c->nside = std::max(1, std::min(kNSideMax, std::atoi(env)));
+    for (int i = 0; i < c->nside; ++i) {
       IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
       IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
     }
@@ -401,10 +405,15 @@ long long generic_slice(int lmax) {
 // Launch the emitted kernels for the given variants and the generic kernel;
 // items/ranges already on the device.  Returns the number of kernels launched.
 int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
-             int lmax, int* nlaunch) {
+             int lmax, int* nlaunch, const int* zero_fill_shell_l = nullptr) {
   IB_CUDA(cudaEventRecord(c->fork, s));
-  for (int i = 0; i < kNSide; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
+  for (int i = 0; i < c->nside; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
   int k = 0;
+  if (zero_fill_shell_l) {  // screened quartets: zero blocks, concurrent with the class kernels
+    ib_zero_blocks<<<c->nsm * 4, 256, 0, c->side[c->nside - 1]>>>(a.items, a.ranges, zero_fill_shell_l, sph ? 1 : 0,
+                                                                   a.out);
+    ++*nlaunch;
+  }
   for (int prec = 0; prec < 2; ++prec) {
     if ((prec == 0 && !fp64_present) || (prec == 1 && !fp32_present)) continue;
     IbLaunch ap = a;
@@ -415,7 +424,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       if (!c->table[cid].launch) continue;
       if (prec == 1 && c->table[cid].kind != 2) continue;
       const int grid = c->nsm * c->occ[cid][variant];
-      cudaStream_t ss = c->side[k % kNSide];
+      cudaStream_t ss = c->side[k % c->nside];
       c->table[cid].launch(variant, grid, ss, ap);
       ++k;
       if (prec == 1) {
@@ -434,12 +443,12 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
     nblk = std::max<long long>(nblk, 1);
     IB_CUDA(c->scratch.ensure((size_t)nblk * slice * sizeof(double)));
-    ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, c->side[k % kNSide]>>>(a, kSlotGeneric, sph ? 1 : 0,
+    ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, c->side[k % c->nside]>>>(a, kSlotGeneric, sph ? 1 : 0,
                                                                          c->scratch.as<double>(), slice);
     ++k;
   }
   IB_CUDA(cudaGetLastError());
-  for (int i = 0; i < kNSide; ++i) {
+  for (int i = 0; i < c->nside; ++i) {
     IB_CUDA(cudaEventRecord(c->join[i], c->side[i]));
     IB_CUDA(cudaStreamWaitEvent(s, c->join[i], 0));
   }
@@ -794,12 +803,8 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
     a.flags = c->flags.as<int>();
     a.mixed_tol = mixed_tol;
   }
-  if (use_bounds && skip_below > 0.0) {
-    ib_zero_blocks<<<c->nsm * 4, 256, 0, s>>>(a.items, a.ranges, basis->shell_l, spherical ? 1 : 0, out);
-    ++*nl;
-    IB_CUDA(cudaGetLastError());
-  }
-  return dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, nl);
+  return dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, nl,
+                  use_bounds && skip_below > 0.0 ? basis->shell_l : nullptr);
 }
 }  // namespace
 
@@ -976,6 +981,76 @@ int intception_b200_schwarz(const intception_b200_basis* basis, const int* pairs
                                      c->sw_off.as<long long>(), c->sw_blocks.as<double>(), q + p0);
     IB_CUDA(cudaGetLastError());
   }
+  return set_status(IB_OK, "");
+}
+
+// ---------------------------------------------------------------- CUDA graphs
+struct IbGraph {
+  Context* ctx;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  int launches;
+};
+
+int intception_b200_eri_graph_create(const intception_b200_basis* basis, const int* quartets, const long long* out_off,
+                                     int nq, int spherical, int precision, const double* bounds, double skip_below,
+                                     double fp32_below, double mixed_tol, double* out, void** handle) {
+  if (!handle) return set_status(IB_ERR_ARG, "graph_create: null handle");
+  *handle = nullptr;
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t s = nullptr;
+  IB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  // eager pass: sizes every work buffer, so the captured pass allocates nothing
+  int nl = 0;
+  st = batch_impl(c, basis, quartets, out_off, nq, spherical, precision, bounds, skip_below, fp32_below, mixed_tol,
+                  out, s, &nl);
+  if (st) {
+    cudaStreamDestroy(s);
+    return st;
+  }
+  IB_CUDA(cudaStreamSynchronize(s));
+  IbGraph* g = new IbGraph{c, nullptr, nullptr, 0};
+  IB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  nl = 0;
+  st = batch_impl(c, basis, quartets, out_off, nq, spherical, precision, bounds, skip_below, fp32_below, mixed_tol,
+                  out, s, &nl);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+  cudaStreamDestroy(s);
+  if (st || ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    delete g;
+    return st ? st : set_status(IB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+  }
+  g->graph = graph;
+  g->launches = nl;
+  const cudaError_t ei = cudaGraphInstantiate(&g->exec, graph, 0);
+  if (ei != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    delete g;
+    return set_status(IB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
+  *handle = g;
+  return set_status(IB_OK, "");
+}
+
+int intception_b200_eri_graph_launch(void* handle, void* stream) {
+  IbGraph* g = static_cast<IbGraph*>(handle);
+  if (!g) return set_status(IB_ERR_ARG, "graph_launch: null handle");
+  tl_launches = g->launches;
+  IB_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+  return set_status(IB_OK, "");
+}
+
+int intception_b200_eri_graph_destroy(void* handle) {
+  IbGraph* g = static_cast<IbGraph*>(handle);
+  if (!g) return set_status(IB_OK, "");
+  cudaGraphExecDestroy(g->exec);
+  cudaGraphDestroy(g->graph);
+  delete g;
   return set_status(IB_OK, "");
 }
 

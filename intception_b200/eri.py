@@ -92,6 +92,14 @@ def load():
     lib.intception_b200_schwarz.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                             C.c_void_p]
     lib.intception_b200_schwarz.restype = C.c_int
+    lib.intception_b200_eri_graph_create.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                     C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                                     C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.intception_b200_eri_graph_create.restype = C.c_int
+    lib.intception_b200_eri_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+    lib.intception_b200_eri_graph_launch.restype = C.c_int
+    lib.intception_b200_eri_graph_destroy.argtypes = [C.c_void_p]
+    lib.intception_b200_eri_graph_destroy.restype = C.c_int
     lib.intception_b200_eri_batch_noalloc.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int,
                                                       C.c_int, C.c_void_p, C.c_void_p]
     lib.intception_b200_eri_batch_noalloc.restype = C.c_int
@@ -228,6 +236,16 @@ class EriEngine:
         _check(st)
         return out
 
+    def graph(self, out, precision=PREC_FP64, bounds=None, skip_below=0.0, fp32_below=0.0, mixed_tol=5e-11):
+        """CUDA graph replaying compute(out=out, ...) with one launch; returns
+        an EriGraph (call .launch(stream), .close())."""
+        h = C.c_void_p()
+        _check(load().intception_b200_eri_graph_create(
+            C.byref(self._basis), self.quartets.data_ptr(), self.out_off.data_ptr(), self.nq,
+            1 if self.spherical else 0, precision, bounds.data_ptr() if bounds is not None else None,
+            float(skip_below), float(fp32_below), float(mixed_tol), out.data_ptr(), C.byref(h)))
+        return EriGraph(h, self)
+
     def schwarz(self, pairs, stream=None):
         """sqrt(max |(ij|ij)|) for shell pairs (torch int32 [n, 2], device)."""
         torch = self.torch
@@ -257,6 +275,30 @@ class EriEngine:
     @staticmethod
     def device_status():
         return load().intception_b200_batch_status()
+
+
+class EriGraph:
+    """A captured batch (intception_b200_eri_graph_*)."""
+
+    def __init__(self, handle, engine):
+        self.h = handle
+        self.engine = engine  # keeps the device inputs alive
+
+    def launch(self, stream=None):
+        torch = self.engine.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.engine.device)
+        _check(load().intception_b200_eri_graph_launch(self.h, C.c_void_p(s.cuda_stream)))
+
+    def close(self):
+        if self.h:
+            load().intception_b200_eri_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def batch_reference_layout(batch):

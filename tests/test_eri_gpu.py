@@ -184,3 +184,25 @@ def test_screened_and_mixed_paths_meet_error_bar():
     assert np.abs(mix.cpu().numpy() - r).max() <= 1e-10
     kept = (bounds >= 1e-12).double().mean().item()
     assert 0.0 < kept < 1.0
+
+
+def test_cuda_graph_replay_matches_direct_batch():
+    """The captured pipeline (sort, items, every class kernel, side-stream
+    fork/join) replays to the same blocks, also after the inputs change."""
+    import torch
+    b = basis.config_mixed_l2(nq=20000, seed=61, spherical=True)
+    eng = eri.EriEngine(b)
+    ref = eng.compute().clone()
+    out = torch.full_like(ref, float('nan'))
+    g = eng.graph(out)
+    g.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+    # replay reads the current inputs: move every shell and compare again
+    eng.shell_xyz.add_(0.25)
+    ref2 = eng.compute().clone()
+    out.fill_(float('nan'))
+    g.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref2)
+    g.close()
