@@ -79,6 +79,37 @@ int intception_integral_eri_abcd_m_cont_sph_work_array_size(
  * intception_b200_boys_batch. */
 void intception_boys(double *f, const int ifskip, const int nmin, const int nmax, const double x);
 
+/* Two-index primitive Cartesian classes of the reference's example input
+ * script (examples/example_input.py:83-107, generated with contracted=False;
+ * argument list: generator/callables/main_source_algorithms/primitive_general.py:31-97,
+ * output copy: primitive_general.py:929).  Host pointers, synchronous.
+ * output_array[ia*iskipa + ib*iskipb] for the na = (la+1)(la+2)/2 and
+ * nb = (lb+1)(lb+2)/2 components (na, nb must equal those counts;
+ * intception_b200_last_status() reports IB_ERR_ARG otherwise); 0 <= l <= 6;
+ * exponents > 0; work_array is accepted and not touched. */
+
+/* Replaces intception_integral_overlap_2idx_ab_prim_cart_main: (a|b) overlap. */
+void intception_integral_overlap_2idx_ab_prim_cart_main(
+    const double xa, const double cA[3], const int la, const int na, const int iskipa,
+    const double xb, const double cB[3], const int lb, const int nb, const int iskipb,
+    double *work_array, double *output_array);
+
+/* Replaces intception_integral_overlap_2idx_ab_prim_cart_work_array_size
+ * (primitive_vrr_only_no_auxiliary.py:126-165): ncum(la) * ncum(lb),
+ * ncum(l) = (l+1)(l+2)(l+3)/6. */
+int intception_integral_overlap_2idx_ab_prim_cart_work_array_size(const int la, const int lb);
+
+/* Replaces intception_integral_nuclear_2idx_ab_m_cC_prim_cart_main: attraction
+ * (a| 1/|r-C| |b) to the unit point charge at cC. */
+void intception_integral_nuclear_2idx_ab_m_cC_prim_cart_main(
+    const double xa, const double cA[3], const int la, const int na, const int iskipa,
+    const double xb, const double cB[3], const int lb, const int nb, const int iskipb,
+    const double cC[3], double *work_array, double *output_array);
+
+/* Replaces intception_integral_nuclear_2idx_ab_m_cC_prim_cart_work_array_size
+ * (primitive_vrr_only_with_auxiliary.py:191-230): 2 (ncum(lb) ncum(la) + la + lb + 1). */
+int intception_integral_nuclear_2idx_ab_m_cC_prim_cart_work_array_size(const int la, const int lb);
+
 /* ----------------------------------------------------------------------------
  * Status
  * ------------------------------------------------------------------------- */
@@ -205,6 +236,20 @@ int intception_b200_jk_energy(const int *quartets, const long long *out_off, int
 int intception_b200_jk_force(const int *quartets, const int *qidx, const long long *aux_off, int naux, int pos,
                              int sign, const int *shell_l, const int *fofs, const int *shell_atom, const double *P,
                              int nbf, int natom, const double *blocks, double *force, void *stream);
+
+/* Batched two-index primitive integrals (no counterpart in the reference,
+ * which emits one call per pair): pair i of n has exponents xa[i], xb[i],
+ * centres ca[3i..], cb[3i..], angular momenta la[i], lb[i] <= lmax <= 6 and,
+ * for IB_TWOIDX_NUCLEAR, the charge position cc[3i..] (cc may be NULL for
+ * overlap).  Its block goes to out + off[i], a fastest
+ * (out[off[i] + ia + na*ib]).  Device pointers; asynchronous on stream (NULL =
+ * legacy default).  A pair with l outside [0, lmax] or an exponent <= 0 is
+ * skipped and IB_ERR_ARG is stored in *status (a device int, may be NULL). */
+#define IB_TWOIDX_OVERLAP 0
+#define IB_TWOIDX_NUCLEAR 1
+int intception_b200_twoidx_batch(int kind, int n, int lmax, const double *xa, const double *ca, const int *la,
+                                 const double *xb, const double *cb, const int *lb, const double *cc,
+                                 const long long *off, double *out, int *status, void *stream);
 
 /* The library's Cartesian->spherical matrix for l (host memory,
  * T[icart + isph*ncart], ncart x (2l+1)). */

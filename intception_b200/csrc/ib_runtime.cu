@@ -742,6 +742,10 @@ void build_sph_host(std::vector<double>& out) {
   for (int l = 0; l <= IB_LMAX; ++l) sph_matrix_host(l, out.data() + ib_sph_offset(l));
 }
 
+// Sets the calling thread's status word (intception_b200_last_status/_last_error)
+// for entry points defined in other translation units.
+int ib_runtime_set_status(int st, const char* msg) { return set_status(st, msg ? msg : ""); }
+
 namespace {
 // The caller's stream; NULL is the legacy default stream (CUDA's convention).
 int resolve_stream(Context* c, void* stream, cudaStream_t* s) {

@@ -481,3 +481,160 @@ void oracle_eri_batch(int nq, const int *quartets, const int *shell_l, const int
                     out + out_off[q]);
   }
 }
+
+/* ---------------------------------------------------------------------------
+ * Two-index classes of the reference's example script (examples/example_input.py:58-110),
+ * primitive Cartesian: overlap_2idx (base sqrt(pi^3/p^3) exp(-xi R_AB^2), vrr1 on a,
+ * vrr2 on b) and nuclear_2idx (base 2 pi/p exp(-xi R_AB^2) F_m(p R_PC^2), vrr1 on b,
+ * vrr2 on a, both with the auxiliary m).  Tables over cumulative components.
+ * ------------------------------------------------------------------------- */
+static void oracle_2idx(int kind, double xa, const double *A, int la, int na, int iskipa, double xb,
+                        const double *B, int lb, int nb, int iskipb, const double *Cn, double *out) {
+  init_comp_tab();
+  const double p = xa + xb, op = 1.0 / p, o2p = 0.5 * op, xi = xa * xb * op;
+  double PA[3], PB[3], PC[3], AB2 = 0.0, PC2 = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    const double P = (xa * A[i] + xb * B[i]) * op;
+    PA[i] = P - A[i];
+    PB[i] = P - B[i];
+    PC[i] = kind ? P - Cn[i] : 0.0;
+    AB2 += (A[i] - B[i]) * (A[i] - B[i]);
+    PC2 += PC[i] * PC[i];
+  }
+  const int L = kind ? la + lb : 0;
+  const int nA = ncum(la), nB = ncum(lb);
+  double *V = calloc((size_t)(L + 2) * nA * nB, sizeof(double));
+#define V2(m, a, b) V[((size_t)(m) * nA + (a)) * nB + (b)]
+  double F[4 * OR_LMAX + 2];
+  if (kind == 0) {
+    V2(0, 0, 0) = sqrt(31.006276680299816 * op * op * op) * exp(-xi * AB2);
+    /* vrr1: [a+1i|0] = PA_i [a|0] + a_i/2p [a-1i|0] */
+    for (int ia = 1; ia < nA; ++ia) {
+      const int *e = comp_tab[ia];
+      const int i = first_dir(e);
+      int em[3] = {e[0], e[1], e[2]};
+      em[i] -= 1;
+      double v = PA[i] * V2(0, cidx(em[0], em[1], em[2]), 0);
+      if (em[i] > 0) {
+        int e2[3] = {em[0], em[1], em[2]};
+        e2[i] -= 1;
+        v += o2p * em[i] * V2(0, cidx(e2[0], e2[1], e2[2]), 0);
+      }
+      V2(0, ia, 0) = v;
+    }
+    /* vrr2: [a|b+1i] = PB_i [a|b] + b_i/2p [a|b-1i] + a_i/2p [a-1i|b] */
+    for (int ib = 1; ib < nB; ++ib) {
+      const int *f = comp_tab[ib];
+      const int i = first_dir(f);
+      int fm[3] = {f[0], f[1], f[2]};
+      fm[i] -= 1;
+      const int b1 = cidx(fm[0], fm[1], fm[2]);
+      int b2 = -1;
+      if (fm[i] > 0) {
+        int f2[3] = {fm[0], fm[1], fm[2]};
+        f2[i] -= 1;
+        b2 = cidx(f2[0], f2[1], f2[2]);
+      }
+      for (int ia = 0; ia < nA; ++ia) {
+        const int *e = comp_tab[ia];
+        double v = PB[i] * V2(0, ia, b1);
+        if (b2 >= 0) v += o2p * fm[i] * V2(0, ia, b2);
+        if (e[i] > 0) {
+          int em[3] = {e[0], e[1], e[2]};
+          em[i] -= 1;
+          v += o2p * e[i] * V2(0, cidx(em[0], em[1], em[2]), b1);
+        }
+        V2(0, ia, ib) = v;
+      }
+    }
+  } else {
+    oracle_boys(F, 1, 0, L, p * PC2);
+    const double pref = 2.0 * 3.141592653589793 * op * exp(-xi * AB2);
+    for (int m = 0; m <= L; ++m) V2(m, 0, 0) = pref * F[m];
+    /* vrr1 on b: [0|b+1i]^(m) = PB_i [..]^(m) - PC_i [..]^(m+1) + b_i/2p ([b-1i]^(m) - [b-1i]^(m+1)) */
+    for (int ib = 1; ib < nB; ++ib) {
+      const int *f = comp_tab[ib];
+      const int lf = f[0] + f[1] + f[2];
+      const int i = first_dir(f);
+      int fm[3] = {f[0], f[1], f[2]};
+      fm[i] -= 1;
+      const int b1 = cidx(fm[0], fm[1], fm[2]);
+      int b2 = -1;
+      if (fm[i] > 0) {
+        int f2[3] = {fm[0], fm[1], fm[2]};
+        f2[i] -= 1;
+        b2 = cidx(f2[0], f2[1], f2[2]);
+      }
+      for (int m = 0; m + lf <= L; ++m) {
+        double v = PB[i] * V2(m, 0, b1) - PC[i] * V2(m + 1, 0, b1);
+        if (b2 >= 0) v += o2p * fm[i] * (V2(m, 0, b2) - V2(m + 1, 0, b2));
+        V2(m, 0, ib) = v;
+      }
+    }
+    /* vrr2 on a: [a+1i|b]^(m) = PA_i [a|b]^(m) - PC_i [a|b]^(m+1) + b_i/2p ([a|b-1i] - ..^(m+1))
+     *                          + a_i/2p ([a-1i|b] - ..^(m+1)) */
+    for (int ia = 1; ia < nA; ++ia) {
+      const int *e = comp_tab[ia];
+      const int le = e[0] + e[1] + e[2];
+      const int i = first_dir(e);
+      int em[3] = {e[0], e[1], e[2]};
+      em[i] -= 1;
+      const int a1 = cidx(em[0], em[1], em[2]);
+      int a2 = -1;
+      if (em[i] > 0) {
+        int e2[3] = {em[0], em[1], em[2]};
+        e2[i] -= 1;
+        a2 = cidx(e2[0], e2[1], e2[2]);
+      }
+      for (int ib = 0; ib < nB; ++ib) {
+        const int *f = comp_tab[ib];
+        const int lf = f[0] + f[1] + f[2];
+        int b1 = -1;
+        if (f[i] > 0) {
+          int fm[3] = {f[0], f[1], f[2]};
+          fm[i] -= 1;
+          b1 = cidx(fm[0], fm[1], fm[2]);
+        }
+        for (int m = 0; m + le + lf <= L; ++m) {
+          double v = PA[i] * V2(m, a1, ib) - PC[i] * V2(m + 1, a1, ib);
+          if (b1 >= 0) v += o2p * f[i] * (V2(m, a1, b1) - V2(m + 1, a1, b1));
+          if (a2 >= 0) v += o2p * em[i] * (V2(m, a2, ib) - V2(m + 1, a2, ib));
+          V2(m, ia, ib) = v;
+        }
+      }
+    }
+  }
+  const int a0 = ncum(la - 1), b0 = ncum(lb - 1);
+  for (int ib = 0; ib < nb; ++ib)
+    for (int ia = 0; ia < na; ++ia) out[(size_t)ia * iskipa + (size_t)ib * iskipb] = V2(0, a0 + ia, b0 + ib);
+#undef V2
+  free(V);
+}
+
+/* Same argument lists as the emitted example functions */
+void oracle_overlap_2idx_ab_prim_cart_main(double xa, const double cA[3], int la, int na, int iskipa, double xb,
+                                           const double cB[3], int lb, int nb, int iskipb, double *work, double *out) {
+  (void)work;
+  oracle_2idx(0, xa, cA, la, na, iskipa, xb, cB, lb, nb, iskipb, NULL, out);
+}
+
+void oracle_nuclear_2idx_ab_m_cC_prim_cart_main(double xa, const double cA[3], int la, int na, int iskipa, double xb,
+                                                const double cB[3], int lb, int nb, int iskipb, const double cC[3],
+                                                double *work, double *out) {
+  (void)work;
+  oracle_2idx(1, xa, cA, la, na, iskipa, xb, cB, lb, nb, iskipb, cC, out);
+}
+
+/* work-array sizes as emitted (examples/example_input.py classes) */
+int oracle_2idx_work_array_size(int kind, int la, int lb) {
+  return kind == 0 ? ncum(la) * ncum(lb) : 2 * (ncum(lb) * ncum(la) + la + lb + 1);
+}
+
+void oracle_2idx_batch(int kind, int n, const double *xa, const double *ca, const int *la, const double *xb,
+                       const double *cb, const int *lb, const double *cc, const long long *off, double *out) {
+  for (int p = 0; p < n; ++p) {
+    const int na = nc_l(la[p]), nb = nc_l(lb[p]);
+    oracle_2idx(kind, xa[p], ca + 3 * p, la[p], na, 1, xb[p], cb + 3 * p, lb[p], nb, na, kind ? cc + 3 * p : NULL,
+                out + off[p]);
+  }
+}

@@ -59,6 +59,30 @@ def compile_variant(outdir, variant):
     return so
 
 
+def build_example(reference):
+    """The reference's own example script (2-index overlap and nuclear
+    attraction, primitive Cartesian), run from oracle/_ref/gen_2idx so that its
+    output_directory './output' lands there, compiled with ref_batch_2idx.c."""
+    work = os.path.join(REF_OUT, 'gen_2idx')
+    outdir = os.path.join(work, 'output')
+    os.makedirs(outdir, exist_ok=True)
+    shim = ("import sys, time, runpy; time.clock = time.perf_counter; "
+            "sys.path.insert(0, %r); runpy.run_path(%r, run_name='__main__')"
+            % (os.path.join(reference, 'src'), os.path.join(reference, 'examples', 'example_input.py')))
+    subprocess.run([sys.executable, '-c', shim], check=True, cwd=work, stdout=subprocess.DEVNULL)
+    srcs = sorted(f for f in os.listdir(outdir) if f.endswith('.c') and f != 'unity.c')
+    unity = os.path.join(outdir, 'unity.c')
+    with open(unity, 'w') as fh:
+        fh.write('#include <math.h>\n')
+        for s in srcs:
+            fh.write('#include "%s"\n' % s)
+        fh.write('#include "%s"\n' % os.path.join(HERE, 'ref_batch_2idx.c'))
+    so = os.path.join(REF_OUT, 'libref_2idx.so')
+    subprocess.run(['gcc', '-std=gnu99', '-O2', '-fPIC', '-shared', '-w', '-I', outdir, unity, '-o', so, '-lm'],
+                   check=True)
+    return so
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default='/root/reference')
@@ -71,6 +95,7 @@ def main():
     for variant in ('cart', 'sph'):
         outdir = generate(args.reference, variant, args.lmax)
         print(compile_variant(outdir, variant))
+    print(build_example(args.reference))
     return 0
 
 

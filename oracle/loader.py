@@ -8,6 +8,8 @@ CPU-baseline leg.  The product (intception_b200) never imports this module.
 * ``_ref/libref_eri_{cart,sph}.so`` (built by oracle/gen_ref.py where the
   reference tree exists) is the reference generator's own emitted C99 plus an
   OpenMP batch driver.  It may be absent; callers must handle ``None``.
+* ``_ref/libref_2idx.so`` (also gen_ref.py) is the reference's emitted C99 of
+  its example script's two-index classes (overlap, nuclear attraction).
 """
 import ctypes as C
 import os
@@ -50,6 +52,15 @@ def load_oracle():
         lib.oracle_eri_cont_cart_main.restype = None
         lib.oracle_eri_cont_sph_main.argtypes = per_sph * 4 + [_dp, _dp]
         lib.oracle_eri_cont_sph_main.restype = None
+        lib.oracle_2idx_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _ip, _dp, _dp, _ip, _dp, _lp, _dp]
+        lib.oracle_2idx_batch.restype = None
+        lib.oracle_2idx_work_array_size.argtypes = [C.c_int] * 3
+        lib.oracle_2idx_work_array_size.restype = C.c_int
+        pair = [C.c_double, _dp, C.c_int, C.c_int, C.c_int] * 2
+        lib.oracle_overlap_2idx_ab_prim_cart_main.argtypes = pair + [_dp, _dp]
+        lib.oracle_overlap_2idx_ab_prim_cart_main.restype = None
+        lib.oracle_nuclear_2idx_ab_m_cC_prim_cart_main.argtypes = pair + [_dp, _dp, _dp]
+        lib.oracle_nuclear_2idx_ab_m_cC_prim_cart_main.restype = None
         _oracle = lib
     return _oracle
 
@@ -76,6 +87,40 @@ def load_ref(variant):
             lib.intception_boys.restype = None
             _ref[variant] = lib
     return _ref[variant]
+
+
+_REF_2IDX_SO = os.path.join(HERE, '_ref', 'libref_2idx.so')
+_ref2 = []
+
+
+def load_ref_2idx():
+    """The reference-emitted two-index classes (ref_2idx_batch), or None."""
+    if not _ref2:
+        if not os.path.exists(_REF_2IDX_SO):
+            _ref2.append(None)
+        else:
+            lib = C.CDLL(_REF_2IDX_SO)
+            lib.ref_2idx_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _ip, _dp, _dp, _ip, _dp, _lp, _dp]
+            lib.ref_2idx_batch.restype = None
+            lib.ref_2idx_work_array_size.argtypes = [C.c_int] * 3
+            lib.ref_2idx_work_array_size.restype = C.c_int
+            _ref2.append(lib)
+    return _ref2[0]
+
+
+def twoidx_batch(kind, pairs, lib=None):
+    """Two-index primitive blocks of a pair set (dict with xa, ca, la, xb, cb,
+    lb, cc, off, size; kind 0 overlap, 1 nuclear) with the C restatement, or
+    with the reference's emitted C99 when lib is load_ref_2idx()."""
+    lib = lib or load_oracle()
+    fn = lib.oracle_2idx_batch if hasattr(lib, 'oracle_2idx_batch') else lib.ref_2idx_batch
+    a = {k: np.ascontiguousarray(pairs[k], dtype=np.int32 if k in ('la', 'lb') else
+                                 (np.int64 if k == 'off' else np.float64))
+         for k in ('xa', 'ca', 'la', 'xb', 'cb', 'lb', 'cc', 'off')}
+    out = np.zeros(int(pairs['size']))
+    fn(int(kind), len(a['xa']), _ptr(a['xa']), _ptr(a['ca']), _ptr(a['la'], _ip), _ptr(a['xb']), _ptr(a['cb']),
+       _ptr(a['lb'], _ip), _ptr(a['cc']), _ptr(a['off'], _lp), _ptr(out))
+    return out
 
 
 def boys(nmax, x, lib=None):

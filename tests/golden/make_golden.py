@@ -2,6 +2,7 @@
 
 Run in a container that has the reference tree (it builds oracle/_ref first):
     python oracle/gen_ref.py && python tests/golden/make_golden.py
+(``make_golden.py twoidx`` writes only twoidx.npz.)
 
 Every fixture stores seeded inputs (shell table, quartets, spherical matrices)
 and the outputs of intception_integral_eri_abcd_m_cont_{cart,sph}_main as
@@ -173,5 +174,58 @@ def main():
     print('work_array_size.npz', len(rows), 'rows')
 
 
+def twoidx_pairs(seed, n, lmax):
+    """Seeded pair set for the two-index classes: random pairs over every
+    (la, lb) <= lmax, then hand-built edges (A = B, A = B = C so T = 0, a far
+    charge with T above the Boys table, tight and diffuse exponents)."""
+    rng = np.random.default_rng(seed)
+    la = rng.integers(0, lmax + 1, n)
+    lb = rng.integers(0, lmax + 1, n)
+    xa = np.exp(rng.uniform(np.log(0.05), np.log(200.0), n))
+    xb = np.exp(rng.uniform(np.log(0.05), np.log(200.0), n))
+    ca = rng.uniform(0.0, 3.0, (n, 3))
+    cb = rng.uniform(0.0, 3.0, (n, 3))
+    cc = rng.uniform(0.0, 3.0, (n, 3))
+    edges = []
+    for l1 in range(lmax + 1):
+        for l2 in range(lmax + 1):
+            c0 = rng.uniform(0, 1, 3)
+            edges.append((l1, l2, 0.8, 1.3, c0, c0, c0 + 0.4))             # A = B
+            edges.append((l1, l2, 2.0, 0.7, c0, c0, c0))                   # A = B = C: T = 0
+            edges.append((l1, l2, 1.5, 2.5, c0, c0 + 0.2, c0 + 30.0))      # T >= 36
+            edges.append((l1, l2, 5e3, 0.02, c0, c0 + 1.0, c0 - 0.5))      # tight with diffuse
+    la = np.concatenate([la, [e[0] for e in edges]]).astype(np.int32)
+    lb = np.concatenate([lb, [e[1] for e in edges]]).astype(np.int32)
+    xa = np.concatenate([xa, [e[2] for e in edges]])
+    xb = np.concatenate([xb, [e[3] for e in edges]])
+    ca = np.concatenate([ca, [e[4] for e in edges]])
+    cb = np.concatenate([cb, [e[5] for e in edges]])
+    cc = np.concatenate([cc, [e[6] for e in edges]])
+    sizes = ((la + 1) * (la + 2) // 2) * ((lb + 1) * (lb + 2) // 2)
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    return dict(xa=xa, ca=ca.ravel(), la=la, xb=xb, cb=cb.ravel(), lb=lb, cc=cc.ravel(), off=off,
+                size=np.int64(sizes.sum()))
+
+
+def twoidx():
+    """twoidx.npz: the reference-emitted overlap_2idx and nuclear_2idx of its
+    example script over a seeded pair set, and their work-array sizes."""
+    lib = loader.load_ref_2idx()
+    assert lib is not None, 'oracle/_ref/libref_2idx.so not built (python oracle/gen_ref.py)'
+    pairs = twoidx_pairs(21, 250, 6)
+    ov = loader.twoidx_batch(0, pairs, lib)
+    nu = loader.twoidx_batch(1, pairs, lib)
+    rows = [[k, la, lb, lib.ref_2idx_work_array_size(k, la, lb)] for k in (0, 1) for la in range(7)
+            for lb in range(7)]
+    np.savez_compressed(os.path.join(HERE, 'twoidx.npz'), overlap=ov, nuclear=nu,
+                        work_array_size=np.array(rows, np.int64), **pairs)
+    print('twoidx.npz', len(pairs['xa']), 'pairs, max |S| = %.3e, max |V| = %.3e'
+          % (np.abs(ov).max(), np.abs(nu).max()))
+
+
 if __name__ == '__main__':
-    main()
+    if sys.argv[1:] == ['twoidx']:
+        twoidx()
+    else:
+        main()
+        twoidx()
