@@ -7,6 +7,9 @@ Workload (one step = one pass of the ERI path over one batch):
   uniform in a 30-bohr cube, spherical output, seed 1 (rank r uses seed 1+r).
   Synthetic data with the shapes of that configuration.
 
+--workload nuclear_2idx | overlap_2idx times the reference example script's
+two-index classes instead (4e6 primitive pairs, l <= 2; one launch per step).
+
 Arms:
   default          : this library, FP64 path and mixed-precision path
   --impl reference : the reference's own CPU implementation of the path (the
@@ -52,6 +55,9 @@ def parse():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx'],
+                    help='eri: the headline; *_2idx: the example script\'s two-index classes')
+    ap.add_argument('--npairs', type=int, default=4_000_000)
     return ap.parse_args()
 
 
@@ -240,9 +246,157 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+TWOIDX_METRIC = 'primitive %s pair blocks/s (example_input.py class, l<=2)'
+TWOIDX_WORKLOAD = ('%d primitive pairs%s, la and lb uniform in 0..2, alpha log-uniform [0.05,1e4], A in a 30-bohr '
+                   'cube, B%s within 2 bohr of A, seed 1')
+
+
+def twoidx_cpu(kind, pairs, seconds, step_index=0):
+    """The reference's emitted C99 of the example classes (oracle/_ref,
+    OpenMP) -- or the oracle port when it was not built -- over a bounded
+    random sample of the pairs.  Returns (pairs/s, kind, cores, sample)."""
+    from intception_b200 import twoidx
+    from oracle import loader
+    lib = loader.load_ref_2idx()
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(77 + step_index)
+    n_all = len(pairs['la'])
+
+    def run(n):
+        idx = np.sort(rng.choice(n_all, n, replace=False))
+        sub = {k: np.asarray(pairs[k])[idx] for k in ('xa', 'ca', 'la', 'xb', 'cb', 'lb', 'cc')}
+        sub['off'], sub['size'] = twoidx.block_offsets(sub['la'], sub['lb'])
+        t0 = time.perf_counter()
+        loader.twoidx_batch(kind, sub, lib)
+        return time.perf_counter() - t0
+
+    n = 20000
+    dt = run(n)
+    n2 = int(min(n_all, max(n, n * seconds / max(dt, 1e-3))))
+    dt2 = run(n2)
+    return (n2 / dt2, 'reference' if lib is not None else 'port', cores if lib is not None else 1,
+            '%d random pairs of the workload (uniform sample)' % n2)
+
+
+def run_twoidx(args, rank, world, local):
+    """Two-index workload: one step = one launch over every pair."""
+    import torch
+    from intception_b200 import eri, twoidx
+    kind = twoidx.NUCLEAR if args.workload == 'nuclear_2idx' else twoidx.OVERLAP
+    name = 'nuclear-attraction' if kind == twoidx.NUCLEAR else 'overlap'
+    workload = TWOIDX_WORKLOAD % (args.npairs, ' x one point charge' if kind == twoidx.NUCLEAR else '',
+                                  ' and the charge' if kind == twoidx.NUCLEAR else '')
+    pairs = twoidx.make_pairs(args.npairs, 2, seed=1 + rank)
+    if args.impl == 'reference':
+        if rank != 0:
+            return
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, ckind, cores, sample = twoidx_cpu(kind, pairs, max(2.0, args.cpu_seconds / 3), i)
+            if i >= args.warmup:
+                vals.append(v)
+        v = float(np.median(vals))
+        line = {'metric': TWOIDX_METRIC % name, 'value': v, 'unit': 'pairs/s', 'n_gpus': args.gpus,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * args.npairs / v,
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic', 'config': {'workload': workload, 'parallelism': 'openmp host cores'},
+                'impl': 'reference',
+                'cpu_baseline': {'value': v, 'unit': 'pairs/s', 'cores': cores, 'kind': ckind, 'sample': sample},
+                'e2e': {'value': v, 'unit': 'pairs/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line), flush=True)
+        return
+    batch = twoidx.TwoIndexBatch(pairs)
+    out = torch.empty(batch.size, dtype=torch.float64, device='cuda')
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        assert batch.device_status() == 0
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+
+    clk = ClockSampler(local).__enter__()
+    ms = timed(lambda: batch.compute(kind, out=out))
+    value = args.npairs * world / (ms * 1e-3)
+    # roofline: algorithmic bytes and flops of the step, against measured HBM and FP64 peaks
+    cost = {(a, b): twoidx.algorithmic_cost(kind, a, b) for a in range(3) for b in range(3)}
+    cls = pairs['la'].astype(np.int64) * 3 + pairs['lb']
+    counts = np.bincount(cls, minlength=9)
+    flops = float(sum(counts[a * 3 + b] * cost[(a, b)][0] for a in range(3) for b in range(3)))
+    nbytes = float(sum(counts[a * 3 + b] * cost[(a, b)][1] for a in range(3) for b in range(3)))
+    with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+        hbm = json.load(fh)['hbm_gbs'] * 1e9
+    peak64 = eri.fma_peak(True) if rank == 0 else 0.0
+    t_hbm, t_fp = nbytes / hbm, flops / peak64 if peak64 else 0.0
+    bound = 'hbm' if t_hbm >= t_fp else 'fp64'
+    achieved = (nbytes if bound == 'hbm' else flops) / (ms * 1e-3)
+    peak = hbm if bound == 'hbm' else peak64
+    roofline = {'bound': bound, 'achieved': achieved / (1e9 if bound == 'hbm' else 1e12),
+                'peak': peak / (1e9 if bound == 'hbm' else 1e12), 'unit': 'GB/s' if bound == 'hbm' else 'TFLOP/s',
+                'frac': achieved / peak, 'traffic': None,
+                'peak_source': 'hbm: MEASURED_PEAKS.json hbm_gbs; fp64: intception_b200_fma_peak this run',
+                'kernel': 'ib2_%s_kernel' % ('nuclear' if kind == twoidx.NUCLEAR else 'overlap'),
+                'alg_bytes_per_step': nbytes, 'alg_flops_per_step': flops,
+                'fp64_frac': (flops / (ms * 1e-3)) / peak64 if peak64 else None}
+    prof = os.path.join(ROOT, 'profiles', 'traffic_%s.json' % args.workload)
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            roofline['traffic'] = json.load(fh).get('bytes_per_step')
+    # e2e: host inputs -> device, the launch, the blocks back to host
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_in = [pin(batch.xa.cpu()), pin(batch.ca.cpu()), pin(batch.la.cpu()), pin(batch.xb.cpu()),
+            pin(batch.cb.cpu()), pin(batch.lb.cpu()), pin(batch.off.cpu())]
+    d_in = [batch.xa, batch.ca, batch.la, batch.xb, batch.cb, batch.lb, batch.off]
+    if kind == twoidx.NUCLEAR:
+        h_in.append(pin(batch.cc.cpu()))
+        d_in.append(batch.cc)
+    h_out = torch.empty(batch.size, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        for h, d in zip(h_in, d_in):
+            d.copy_(h, non_blocking=True)
+        batch.compute(kind, out=out)
+        h_out.copy_(out, non_blocking=True)
+
+    mse = timed(e2e_step)
+    e2e = {'value': args.npairs * world / (mse * 1e-3), 'unit': 'pairs/s',
+           'h2d_bytes_per_step': sum(t.numel() * t.element_size() for t in h_in),
+           'd2h_bytes_per_step': h_out.numel() * 8, 'ms_per_step': mse}
+    clk.__exit__(None, None, None)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, ckind, cores, sample = twoidx_cpu(kind, pairs, args.cpu_seconds)
+        cpu = {'value': v, 'unit': 'pairs/s', 'cores': cores, 'kind': ckind, 'sample': sample}
+    if rank == 0:
+        line = {'metric': TWOIDX_METRIC % name, 'value': value, 'unit': 'pairs/s', 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': workload, 'npairs_per_gpu': args.npairs,
+                           'l2': 'inputs+outputs %.0f MB per step, larger than L2; no flush' % (nbytes / 1e6)},
+                'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
+                'gpu_launches': args.steps, 'gpu_launches_per_step': 1, 'clocks': clk.summary()}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_init(args.gpus)
+    if args.workload != 'eri':
+        run_twoidx(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == 'reference':
         run_reference_arm(args, rank, world)
         return

@@ -57,6 +57,7 @@ struct Ib2Args {
   double* out;
   const double* boys;
   int* status;
+  int lthr;  // lane-group kernels: pairs with max(la, lb) <= lthr belong to the thread-per-pair kernels
 };
 
 __host__ __device__ __forceinline__ int ib2_ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -64,9 +65,12 @@ __host__ __device__ __forceinline__ int ib2_ncum(int l) { return (l + 1) * (l + 
 __device__ __forceinline__ int ib2_cidx(int y, int z) { return z + (y + z) * (y + z + 1) / 2; }
 
 // Offset of level n in the VRR table of total L: sum_{n'<n} ncart(n') (L - n' + 1).
-__host__ __device__ __forceinline__ int ib2_vrr_off(int n, int L) {
+__host__ __device__ constexpr int ib2_vrr_off(int n, int L) {
   return (L + 1) * n * (n + 1) * (n + 2) / 6 - (n - 1) * n * (n + 1) * (n + 2) / 8;
 }
+__host__ __device__ constexpr int ib2_ncart_c(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int ib2_ncum_c(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
+__host__ __device__ constexpr int ib2_cidx_c(int y, int z) { return z + (y + z) * (y + z + 1) / 2; }
 
 // (x, y, z) of every component of levels 0..12 in the reference's order
 // (cumulative index ncum(n-1) + k; within a level z + (y+z)(y+z+1)/2 = k).
@@ -118,6 +122,7 @@ __global__ void __launch_bounds__(IB2_BLOCK) ib2_overlap_kernel(const Ib2Args a)
       if (lane == 0 && a.status) atomicExch(a.status, IB_ERR_ARG);
       continue;
     }
+    if (max(la, lb) <= a.lthr) continue;  // done by the thread-per-pair kernel
     const double op = 1.0 / (xa + xb), o2p = 0.5 * op, xi = xa * xb * op;
     const int nj = lb + 1;
     if (lane < 3) {
@@ -180,6 +185,7 @@ __global__ void __launch_bounds__(IB2_BLOCK) ib2_nuclear_kernel(const Ib2Args a,
       if (lane == 0 && a.status) atomicExch(a.status, IB_ERR_ARG);
       continue;
     }
+    if (max(la0, lb0) <= a.lthr) continue;  // done by the thread-per-pair kernel
     const bool swap = la0 < lb0;  // recur on the larger side
     const int la = swap ? lb0 : la0, lb = swap ? la0 : lb0, L = la + lb;
     const double* pa = swap ? a.cb + 3 * p : a.ca + 3 * p;
@@ -260,6 +266,309 @@ __global__ void __launch_bounds__(IB2_BLOCK) ib2_nuclear_kernel(const Ib2Args a,
       o[t] = lb == 0 ? V[vo + k * (L - la + 1)] : R[k * nbs + fk];
     }
     __syncwarp(mask);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-pair kernels for max(la, lb) <= IB2_LT: the recurrences of one
+// class fully unrolled at compile time (every table index a constant, the
+// tables in registers); the class is picked per thread by a switch.
+#define IB2_LT 2
+
+// Largest HRR level table, (ncum(L-j) - ncum(LA-1)) ncart(j) over j = 1..LB.
+__host__ __device__ constexpr int ib2_hrr_max(int LA, int LB) {
+  int h = 1;
+  for (int j = 1; j <= LB; ++j) {
+    const int t = (ib2_ncum_c(LA + LB - j) - ib2_ncum_c(LA - 1)) * ib2_ncart_c(j);
+    h = t > h ? t : h;
+  }
+  return h;
+}
+
+// F_m(T), m = 0..L, reading the global table (no staging; L is a constant).
+template <int L>
+__device__ __forceinline__ void ib2_boys_f(double T, const double* __restrict__ tab, double* F) {
+  if (T < IB_BOYS_TMAX) {
+    const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
+    const double dx = (double)i * (1.0 / IB_BOYS_H_INV) - T;
+    const double* r = tab + i * IB_BOYS_NCOL + L;
+    double f = __ldg(r + 6) * (1.0 / 720.0);
+    f = fma(f, dx, __ldg(r + 5) * (1.0 / 120.0));
+    f = fma(f, dx, __ldg(r + 4) * (1.0 / 24.0));
+    f = fma(f, dx, __ldg(r + 3) * (1.0 / 6.0));
+    f = fma(f, dx, __ldg(r + 2) * 0.5);
+    f = fma(f, dx, __ldg(r + 1));
+    F[L] = fma(f, dx, __ldg(r));
+    if (L > 0) {
+      const double e = exp(-T), t2 = T + T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    const double oT = 1.0 / T;
+    F[0] = sqrt(0.78539816339744830962 * oT);  // (1/2) sqrt(pi/T)
+    if (L > 0) {
+      const double he = 0.5 * exp(-T);
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = fma((double)m + 0.5, F[m], -he) * oT;
+    }
+  }
+}
+
+// Nuclear attraction of one pair, LA >= LB; element (k of LA, f of LB) to o[k*sa + f*sb].
+template <int LA, int LB>
+__device__ __forceinline__ void ib2_nuclear_pair(double xa, const double* __restrict__ pa, double xb,
+                                                 const double* __restrict__ pb, const double* __restrict__ pc,
+                                                 const double* __restrict__ boys, double* __restrict__ o, int sa,
+                                                 int sb) {
+  constexpr int L = LA + LB;
+  const double op = 1.0 / (xa + xb), o2p = 0.5 * op, xi = xa * xb * op;
+  double AB[3], PA[3], PC[3], ab2 = 0.0, pc2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double A = pa[d], B = pb[d], C = pc[d];
+    AB[d] = A - B;
+    PA[d] = -xb * op * AB[d];
+    PC[d] = (xa * (A - C) + xb * (B - C)) * op;
+    ab2 = fma(AB[d], AB[d], ab2);
+    pc2 = fma(PC[d], PC[d], pc2);
+  }
+  double V[ib2_vrr_off(L + 1, L)];
+  ib2_boys_f<L>((xa + xb) * pc2, boys, V);
+  const double pref = 6.283185307179586477 * op * exp(-xi * ab2);
+#pragma unroll
+  for (int m = 0; m <= L; ++m) V[m] *= pref;
+  // VRR: [e]^(m) = PA_i [e-1i]^(m) - PC_i [e-1i]^(m+1) + (e_i-1)/2p ([e-2i]^(m) - [e-2i]^(m+1))
+#pragma unroll
+  for (int n = 1; n <= L; ++n) {
+    const int M = L - n + 1;
+#pragma unroll
+    for (int s = 0; s <= n; ++s)
+#pragma unroll
+      for (int z = 0; z <= s; ++z) {
+        const int y = s - z, x = n - s, k = z + s * (s + 1) / 2;
+        const int i = x ? 0 : (y ? 1 : 2);
+        const int ei = i == 0 ? x : (i == 1 ? y : z);
+        const int y1 = y - (i == 1), z1 = z - (i == 2);
+        const int r1 = ib2_vrr_off(n - 1, L) + ib2_cidx_c(y1, z1) * (M + 1);
+        const int r2 = n >= 2 ? ib2_vrr_off(n - 2, L) + ib2_cidx_c(y1 - (i == 1), z1 - (i == 2)) * (M + 2) : 0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          double v = PA[i] * V[r1 + m] - PC[i] * V[r1 + m + 1];
+          if (ei >= 2) v = fma((double)(ei - 1) * o2p, V[r2 + m] - V[r2 + m + 1], v);
+          V[ib2_vrr_off(n, L) + k * M + m] = v;
+        }
+      }
+  }
+  if (LB == 0) {
+#pragma unroll
+    for (int k = 0; k < ib2_ncart_c(LA); ++k) o[k * sa] = V[ib2_vrr_off(LA, L) + k * (L - LA + 1)];
+    return;
+  }
+  // HRR: (e|f+1i) = (e+1i|f) + AB_i (e|f); H[(e - first e of level LA)*ncart(j) + f]
+  constexpr int base = ib2_ncum_c(LA - 1);
+  constexpr int NH = ib2_hrr_max(LA, LB);
+  double H[2][NH];  // level j in H[j & 1]
+#pragma unroll
+  for (int j = 1; j <= LB; ++j) {
+    double* Hn = H[j & 1];
+    const double* Hp = H[(j - 1) & 1];
+    const int nf = ib2_ncart_c(j), nfp = ib2_ncart_c(j - 1);
+#pragma unroll
+    for (int n = LA; n <= L - j; ++n)
+#pragma unroll
+      for (int s = 0; s <= n; ++s)
+#pragma unroll
+        for (int z = 0; z <= s; ++z) {
+          const int y = s - z, k0 = z + s * (s + 1) / 2;
+#pragma unroll
+          for (int fs = 0; fs <= j; ++fs)
+#pragma unroll
+            for (int fz = 0; fz <= fs; ++fz) {
+              const int fy = fs - fz, fx = j - fs, fk = fz + fs * (fs + 1) / 2;
+              const int i = fx ? 0 : (fy ? 1 : 2);
+              const int fkp = ib2_cidx_c(fy - (i == 1), fz - (i == 2));
+              const int k1 = ib2_cidx_c(y + (i == 1), z + (i == 2));
+              double h0, h1;
+              if (j == 1) {
+                h0 = V[ib2_vrr_off(n, L) + k0 * (L - n + 1)];
+                h1 = V[ib2_vrr_off(n + 1, L) + k1 * (L - n)];
+              } else {
+                h0 = Hp[(ib2_ncum_c(n - 1) - base + k0) * nfp + fkp];
+                h1 = Hp[(ib2_ncum_c(n) - base + k1) * nfp + fkp];
+              }
+              Hn[(ib2_ncum_c(n - 1) - base + k0) * nf + fk] = fma(AB[i], h0, h1);
+            }
+        }
+  }
+#pragma unroll
+  for (int k = 0; k < ib2_ncart_c(LA); ++k)
+#pragma unroll
+    for (int f = 0; f < ib2_ncart_c(LB); ++f) o[k * sa + f * sb] = H[LB & 1][k * ib2_ncart_c(LB) + f];
+}
+
+template <int LA, int LB>
+__device__ __forceinline__ void ib2_overlap_pair(double xa, const double* __restrict__ pa, double xb,
+                                                 const double* __restrict__ pb, double* __restrict__ o) {
+  const double op = 1.0 / (xa + xb), o2p = 0.5 * op, xi = xa * xb * op;
+  double S[3][LA + 1][LB + 1];
+  double ab2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double AB = pa[d] - pb[d], PA = -xb * op * AB, PB = xa * op * AB;
+    ab2 = fma(AB, AB, ab2);
+    S[d][0][0] = 1.0;
+#pragma unroll
+    for (int i = 1; i <= LA; ++i) {
+      double v = PA * S[d][i - 1][0];
+      if (i >= 2) v = fma((double)(i - 1) * o2p, S[d][i - 2][0], v);
+      S[d][i][0] = v;
+    }
+#pragma unroll
+    for (int j = 1; j <= LB; ++j)
+#pragma unroll
+      for (int i = 0; i <= LA; ++i) {
+        double v = PB * S[d][i][j - 1];
+        if (j >= 2) v = fma((double)(j - 1) * o2p, S[d][i][j - 2], v);
+        if (i >= 1) v = fma((double)i * o2p, S[d][i - 1][j - 1], v);
+        S[d][i][j] = v;
+      }
+  }
+  const double pref = sqrt(31.006276680299820175 * op * op * op) * exp(-xi * ab2);  // pi^3 / p^3
+#pragma unroll
+  for (int fs = 0; fs <= LB; ++fs)
+#pragma unroll
+    for (int fz = 0; fz <= fs; ++fz)
+#pragma unroll
+      for (int es = 0; es <= LA; ++es)
+#pragma unroll
+        for (int ez = 0; ez <= es; ++ez) {
+          const int ex = LA - es, ey = es - ez, fx = LB - fs, fy = fs - fz;
+          const int ia = ez + es * (es + 1) / 2, ib = fz + fs * (fs + 1) / 2;
+          o[ia + ib2_ncart_c(LA) * ib] = pref * S[0][ex][fx] * S[1][ey][fy] * S[2][ez][fz];
+        }
+}
+
+// Block-cooperative chunks: a block stages IB2_CHUNK pairs' inputs in shared
+// memory (coalesced, each input byte read once), counting-sorts them by class
+// there, and its warps run the sorted list, so the 32 lanes of a warp execute
+// the same unrolled class code.  Pairs of the lane-group kernel and refused
+// pairs are left out of the list.
+#define IB2_CHUNK 512
+#define IB2_TPB 128
+
+template <int KIND>
+struct Ib2Stage {
+  double xa[IB2_CHUNK], xb[IB2_CHUNK];
+  double ca[3 * IB2_CHUNK], cb[3 * IB2_CHUNK];
+  double cc[KIND == 1 ? 3 * IB2_CHUNK : 1];
+  long long off[IB2_CHUNK];
+  short order[IB2_CHUNK];     // chunk-local pair index, sorted by class
+  unsigned char cls[IB2_CHUNK];
+  unsigned char swp[IB2_CHUNK];
+  int count[16], start[16];
+};
+
+template <int KIND>
+__device__ __forceinline__ void ib2_thread_pair(const Ib2Stage<KIND>& st, int c, int j, const double* boys,
+                                                double* out) {
+  if (KIND == 0) {
+    const double* pa = st.ca + 3 * j;
+    const double* pb = st.cb + 3 * j;
+    double* o = out + st.off[j];
+    const double xa = st.xa[j], xb = st.xb[j];
+    switch (c) {
+      case 0: ib2_overlap_pair<0, 0>(xa, pa, xb, pb, o); break;
+      case 1: ib2_overlap_pair<0, 1>(xa, pa, xb, pb, o); break;
+      case 2: ib2_overlap_pair<0, 2>(xa, pa, xb, pb, o); break;
+      case 3: ib2_overlap_pair<1, 0>(xa, pa, xb, pb, o); break;
+      case 4: ib2_overlap_pair<1, 1>(xa, pa, xb, pb, o); break;
+      case 5: ib2_overlap_pair<1, 2>(xa, pa, xb, pb, o); break;
+      case 6: ib2_overlap_pair<2, 0>(xa, pa, xb, pb, o); break;
+      case 7: ib2_overlap_pair<2, 1>(xa, pa, xb, pb, o); break;
+      default: ib2_overlap_pair<2, 2>(xa, pa, xb, pb, o); break;
+    }
+  } else {
+    const bool swap = st.swp[j];
+    const double* pa = swap ? st.cb + 3 * j : st.ca + 3 * j;
+    const double* pb = swap ? st.ca + 3 * j : st.cb + 3 * j;
+    const double xa = swap ? st.xb[j] : st.xa[j], xb = swap ? st.xa[j] : st.xb[j];
+    double* o = out + st.off[j];
+    const double* pc = st.cc + 3 * j;
+#define IB2_NU(A_, B_)                                                                                      \
+  ib2_nuclear_pair<A_, B_>(xa, pa, xb, pb, pc, boys, o, swap ? ib2_ncart_c(B_) : 1, swap ? 1 : ib2_ncart_c(A_)); \
+  break;
+    switch (c) {
+      case 0: IB2_NU(0, 0)
+      case 1: IB2_NU(1, 0)
+      case 2: IB2_NU(1, 1)
+      case 3: IB2_NU(2, 0)
+      case 4: IB2_NU(2, 1)
+      default: IB2_NU(2, 2)
+    }
+#undef IB2_NU
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(IB2_TPB, 4) ib2_thread_kernel(const Ib2Args a) {
+  constexpr int kClasses = KIND == 0 ? (IB2_LT + 1) * (IB2_LT + 1) : (IB2_LT + 1) * (IB2_LT + 2) / 2;
+  extern __shared__ __align__(16) unsigned char ib2_raw[];
+  Ib2Stage<KIND>& st = *reinterpret_cast<Ib2Stage<KIND>*>(ib2_raw);
+  const long long nchunk = ((long long)a.n + IB2_CHUNK - 1) / IB2_CHUNK;
+  for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    const int p0 = (int)(ch * IB2_CHUNK);
+    const int np = min(IB2_CHUNK, a.n - p0);
+    if (threadIdx.x < 16) st.count[threadIdx.x] = 0;
+    for (int t = threadIdx.x; t < np; t += IB2_TPB) {
+      st.xa[t] = __ldg(a.xa + p0 + t);
+      st.xb[t] = __ldg(a.xb + p0 + t);
+      st.off[t] = __ldg(a.off + p0 + t);
+    }
+    for (int t = threadIdx.x; t < 3 * np; t += IB2_TPB) {
+      st.ca[t] = __ldg(a.ca + 3LL * p0 + t);
+      st.cb[t] = __ldg(a.cb + 3LL * p0 + t);
+      if (KIND == 1) st.cc[t] = __ldg(a.cc + 3LL * p0 + t);
+    }
+    __syncthreads();
+    // class of every staged pair; per-class counts
+    for (int t = threadIdx.x; t < np; t += IB2_TPB) {
+      const int la = __ldg(a.la + p0 + t), lb = __ldg(a.lb + p0 + t);
+      int c = 255;
+      if (ib2_bad(la, lb, a.lmax, st.xa[t], st.xb[t])) {
+        if (a.status) atomicExch(a.status, IB_ERR_ARG);
+      } else if (KIND == 0) {
+        if (la <= IB2_LT && lb <= IB2_LT) c = la * (IB2_LT + 1) + lb;
+      } else {
+        const int hi = max(la, lb), lo = min(la, lb);
+        if (hi <= IB2_LT) c = hi * (hi + 1) / 2 + lo;
+        st.swp[t] = la < lb;
+      }
+      st.cls[t] = (unsigned char)c;
+      if (c != 255) atomicAdd(&st.count[c], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int c = 0; c < kClasses; ++c) {
+        st.start[c] = acc;
+        acc += st.count[c];
+      }
+      st.start[kClasses] = acc;
+      for (int c = 0; c < kClasses; ++c) st.count[c] = st.start[c];  // running insert positions
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < np; t += IB2_TPB) {
+      const int c = st.cls[t];
+      if (c != 255) st.order[atomicAdd(&st.count[c], 1)] = (short)t;
+    }
+    __syncthreads();
+    const int total = st.start[kClasses];
+    for (int i = threadIdx.x; i < total; i += IB2_TPB) {
+      const int j = st.order[i];
+      ib2_thread_pair<KIND>(st, st.cls[j], j, a.boys, a.out);
+    }
+    __syncthreads();  // the stage is reused by the next chunk
   }
 }
 
@@ -348,6 +657,8 @@ int twoidx_setup(TwoIdxDevice** out) {
     ok = ok && cudaGetSymbolAddress((void**)&d.single, ib2_single) == cudaSuccess;
     ok = ok && cudaGetSymbolAddress((void**)&d.single_out, ib2_single_out) == cudaSuccess;
     ok = ok && cudaGetSymbolAddress((void**)&d.single_status, ib2_single_status) == cudaSuccess;
+    ok = ok && allow_smem(ib2_thread_kernel<0>, sizeof(Ib2Stage<0>)) == cudaSuccess;
+    ok = ok && allow_smem(ib2_thread_kernel<1>, sizeof(Ib2Stage<1>)) == cudaSuccess;
     // each group size serves the lmax values pick_group maps to it
     ok = ok && allow_smem(ib2_nuclear_kernel<32>, smem_bytes(1, 32, IB2_LMAX)) == cudaSuccess;
     ok = ok && allow_smem(ib2_nuclear_kernel<16>, smem_bytes(1, 16, 2)) == cudaSuccess;
@@ -370,7 +681,22 @@ int grid_for(K kernel, size_t smem, int n, int groups, int nsm) {
   return (int)std::max(1LL, std::min<long long>(need, (long long)per_sm * nsm));
 }
 
-int launch(int kind, const Ib2Args& a, int nsm, cudaStream_t s) {
+int launch(int kind, const Ib2Args& a0, int nsm, cudaStream_t s) {
+  // every pair passes the thread-per-pair kernel (which also flags invalid
+  // pairs); pairs with max(la, lb) > IB2_LT then take the lane-group kernel
+  {
+    const long long chunks = ((long long)a0.n + IB2_CHUNK - 1) / IB2_CHUNK;
+    const int grid = (int)std::max(1LL, std::min<long long>(chunks, 4LL * nsm));
+    if (kind == 0)
+      ib2_thread_kernel<0><<<grid, IB2_TPB, sizeof(Ib2Stage<0>), s>>>(a0);
+    else
+      ib2_thread_kernel<1><<<grid, IB2_TPB, sizeof(Ib2Stage<1>), s>>>(a0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return IB_ERR_CUDA;
+  }
+  if (a0.lmax <= IB2_LT) return IB_OK;
+  Ib2Args a = a0;
+  a.lthr = IB2_LT;
   const int G = pick_group(kind, a.lmax);
   const size_t smem = smem_bytes(kind, G, a.lmax);
   const int groups = IB2_BLOCK / G;
@@ -443,6 +769,7 @@ void single_pair(int kind, double xa, const double* cA, int la, int na, int iski
   h.l[1] = lb;
   h.off = 0;
   Ib2Args a;
+  a.lthr = -1;
   a.n = 1;
   a.lmax = std::max(la, lb);
   a.xa = d->single->d;
@@ -528,6 +855,7 @@ int intception_b200_twoidx_batch(int kind, int n, int lmax, const double* xa, co
   int st = twoidx_setup(&d);
   if (st) return st;
   Ib2Args a;
+  a.lthr = -1;
   a.n = n;
   a.lmax = lmax;
   a.xa = xa;

@@ -145,3 +145,46 @@ class TwoIndexBatch:
     def device_status(self):
         """The device status word (0 = every pair evaluated); synchronises."""
         return int(self.status.item())
+
+
+def make_pairs(n, lmax=2, seed=1, box=30.0):
+    """Synthetic pair set: la, lb uniform in 0..lmax, exponents log-uniform in
+    [0.05, 1e4], A uniform in a box, B and the charge C within 2 bohr of A
+    (pairs and charges near each other, as in a molecule)."""
+    rng = np.random.default_rng(seed)
+    la = rng.integers(0, lmax + 1, n).astype(np.int32)
+    lb = rng.integers(0, lmax + 1, n).astype(np.int32)
+    xa = np.exp(rng.uniform(np.log(0.05), np.log(1e4), n))
+    xb = np.exp(rng.uniform(np.log(0.05), np.log(1e4), n))
+    ca = rng.uniform(0.0, box, (n, 3))
+    cb = ca + rng.uniform(-2.0, 2.0, (n, 3))
+    cc = ca + rng.uniform(-2.0, 2.0, (n, 3))
+    return dict(xa=xa, ca=ca, la=la, xb=xb, cb=cb, lb=lb, cc=cc)
+
+
+def algorithmic_cost(kind, la, lb):
+    """(FP64 flops, bytes) per pair of the recurrences as the kernels run them:
+    nuclear -- VRR entries (3 flops, 7 with the two-back term), HRR entries
+    (2), Boys (Taylor, downward recursion) and setup; overlap -- the three 1D
+    tables and 3 multiplies per output.  Bytes: the pair's inputs and its
+    output block."""
+    na, nb = ncart(la), ncart(lb)
+    nbytes = 8 * na * nb + 8 * 2 + 8 * 6 + 4 * 2 + 8 + (24 if kind == NUCLEAR else 0)
+    if kind == OVERLAP:
+        return 3 * 5 * (la + 1) * (lb + 1) + 3 * na * nb + 30, nbytes
+    hi, lo = max(la, lb), min(la, lb)
+    L = hi + lo
+    flops = 40 + 14 + 3 * L + (L + 1)
+    for n in range(1, L + 1):
+        for k in range(ncart(n)):
+            s = 0
+            while (s + 1) * (s + 2) // 2 <= k:
+                s += 1
+            z = k - s * (s + 1) // 2
+            e = (n - s, s - z, z)
+            ei = next(v for v in e if v > 0)
+            flops += (L - n + 1) * (7 if ei >= 2 else 3)
+    ncum = lambda l: (l + 1) * (l + 2) * (l + 3) // 6  # noqa: E731
+    for j in range(1, lo + 1):
+        flops += 2 * (ncum(L - j) - ncum(hi - 1)) * ncart(j)
+    return flops, nbytes

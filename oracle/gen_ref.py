@@ -78,8 +78,8 @@ def build_example(reference):
             fh.write('#include "%s"\n' % s)
         fh.write('#include "%s"\n' % os.path.join(HERE, 'ref_batch_2idx.c'))
     so = os.path.join(REF_OUT, 'libref_2idx.so')
-    subprocess.run(['gcc', '-std=gnu99', '-O2', '-fPIC', '-shared', '-w', '-I', outdir, unity, '-o', so, '-lm'],
-                   check=True)
+    subprocess.run(['gcc', '-std=gnu99', '-O3', '-march=native', '-fPIC', '-shared', '-fopenmp', '-w', '-I', outdir,
+                    unity, '-o', so, '-lm'], check=True)
     return so
 
 

@@ -11,9 +11,10 @@
 
 static int rb2_ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
-/* kind 0: overlap, 1: nuclear attraction to the point cC[3*p] */
+/* kind 0: overlap, 1: nuclear attraction to the point cC[3*p]; OpenMP over pairs */
 void ref_2idx_batch(int kind, int n, const double *xa, const double *ca, const int *la, const double *xb,
                     const double *cb, const int *lb, const double *cc, const long long *off, double *out) {
+#pragma omp parallel for schedule(dynamic, 256)
   for (int p = 0; p < n; ++p) {
     int na = rb2_ncart(la[p]), nb = rb2_ncart(lb[p]);
     int nw = kind == 0 ? intception_integral_overlap_2idx_ab_prim_cart_work_array_size(la[p], lb[p])
