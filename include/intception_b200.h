@@ -195,6 +195,13 @@ int intception_b200_last_launch_count(void);
  * batch had their FP32 result rejected by the error bound and recomputed in FP64. */
 int intception_b200_last_fp32_rejections(void);
 
+/* Tuning: at most cap lane groups (a power of two; 0 = no cap) share one
+ * contracted quartet in the kernel of canonical class cid (cid < 0: every
+ * class).  The kernels spread a quartet's primitive quartets over more groups
+ * when a class has fewer quartets than the grid has groups; results agree to
+ * rounding for every cap.  New: the reference's functions have no such knob. */
+int intception_b200_set_slice_cap(int cid, int cap);
+
 /* Waits for the device and returns the device status word of the last batch
  * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
 int intception_b200_batch_status(void);

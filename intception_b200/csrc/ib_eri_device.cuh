@@ -46,21 +46,54 @@ struct IbLaunch {
   int* flags;              // per sorted item: 1 = FP32 result rejected, recompute in FP64
   int recheck;             // FP64 kernels: evaluate only flagged items
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
+  int max_slices;          // class kernels: cap on lane groups sharing one quartet (0: lane groups per block)
 };
 
-// Per-lane constants of a lane-group kernel: the lane's Cartesian component,
-// its base-chain path (direction and the exponent before each step), and the
-// lanes owning component - 1x, - 1y, - 1z inside the group.
-struct IbLaneInfo {
-  unsigned char c[3];
-  unsigned char len;
-  unsigned char dir[8];
-  unsigned char nb[8];
-  unsigned char src[3];
+// Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
+// path, 5 bits per step (direction 0..2, or 3 for an identity step that pads
+// shorter paths at the front; then the exponent before the step); misc: the
+// lane's Cartesian component (4 bits per axis) and the lanes owning
+// component - 1x, - 1y, - 1z inside the group (6 bits each).
+struct IbLaneCode {
+  unsigned steps;
+  unsigned misc;
 };
+
+// An opaque register copy: the compiler keeps the value in a register (or
+// spills it) instead of re-loading it where it is used.
+__device__ __forceinline__ unsigned ib_pin(unsigned x) {
+  unsigned y;
+  asm volatile("mov.b32 %0, %1;" : "=r"(y) : "r"(x));
+  return y;
+}
 
 // Barrier over the 64 threads of two-warp group g of the block (named barrier g+1).
 __device__ __forceinline__ void ib_group_bar(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
+
+// Slices per quartet of a class kernel: the largest power of two W <= gpb
+// (and <= cap when cap > 0) with n * W <= the grid's lane groups, so that a
+// class with fewer quartets than lane groups spreads each quartet's primitive
+// quartets over W groups.  Uniform over the grid (n, gridDim, cap are).
+__device__ __forceinline__ int ib_slices(int n, int gpb, int cap) {
+  const int wmax = cap > 0 ? min(cap, gpb) : gpb;
+  const long long groups = (long long)gridDim.x * gpb;
+  int w = 1;
+  while (2 * w <= wmax && (long long)n * (2 * w) <= groups) w *= 2;
+  return w;
+}
+
+// Barrier over the sg-th quartet slot of the block (SG lanes): a warp-level
+// sync inside a warp, named barrier sg+1 for two warps, the block barrier for
+// the whole block.  Every lane of the slot calls it the same number of times.
+__device__ __forceinline__ void ib_sg_sync(int SG, int sg, unsigned mask) {
+  if (SG <= 32) {
+    __syncwarp(mask);
+  } else if (SG < IB_BLOCK) {
+    asm volatile("bar.sync %0, %1;" ::"r"(sg + 1), "r"(SG) : "memory");
+  } else {
+    __syncthreads();
+  }
+}
 
 typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch& a);
 typedef int (*IbOccFn)(int variant);

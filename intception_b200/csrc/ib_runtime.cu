@@ -104,6 +104,7 @@ struct Context {
   int nsm = 0;
   cudaStream_t stream = nullptr;
   int nside = 40;  // INTCEPTION_B200_STREAMS, 1..64: enough for every class kernel to run concurrently
+  int slice_cap[IB_NCLASS] = {};  // per class: cap on lane groups per quartet (0: no cap; INTCEPTION_B200_MAX_SLICES)
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
@@ -350,6 +351,8 @@ int get_context(Context** out) {
     IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     if (const char* env = std::getenv("INTCEPTION_B200_STREAMS")) c->nside = std::max(1, std::min(kNSideMax, std::atoi(env)));
+    if (const char* env = std::getenv("INTCEPTION_B200_MAX_SLICES"))
+      for (int cid = 0; cid < IB_NCLASS; ++cid) c->slice_cap[cid] = std::max(0, std::atoi(env));
     for (int i = 0; i < c->nside; ++i) {
       IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
       IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
@@ -425,6 +428,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       if (prec == 1 && c->table[cid].kind != 2) continue;
       const int grid = c->nsm * c->occ[cid][variant];
       cudaStream_t ss = c->side[k % c->nside];
+      ap.max_slices = c->slice_cap[cid];
       c->table[cid].launch(variant, grid, ss, ap);
       ++k;
       if (prec == 1) {
@@ -1071,6 +1075,18 @@ int intception_b200_last_fp32_rejections(void) {
   int k = 0;
   for (int v : h) k += v != 0;
   return k;
+}
+
+// Cap on the lane groups that share one quartet in the class kernels, per
+// canonical class id (cid < 0: every class); 0 removes the cap.
+int intception_b200_set_slice_cap(int cid, int cap) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  if (cid >= IB_NCLASS || cap < 0) return set_status(IB_ERR_ARG, "set_slice_cap: class id or cap out of range");
+  for (int k = 0; k < IB_NCLASS; ++k)
+    if (cid < 0 || k == cid) c->slice_cap[k] = cap;
+  return set_status(IB_OK, "");
 }
 
 // Device status word of the last batch (reads it synchronously).

@@ -355,9 +355,9 @@ class GroupEmitter:
         nd = (2 * ld + 1) if sph else len(D)
         L = []
         # bra HRR, lanes over f
-        L.append('    for (int t = j; t < %d; t += %d) {' % (NF, self.G))
+        L.append('    for (int t = r; t < %d; t += SG) {' % NF)
         for e in range(NE):
-            L.append('      const double q%d = sb[%d * %d + t];' % (e, e, NFP))
+            L.append('      const double q%d = sb0[%d * %d + t];' % (e, e, NFP))
         cnt = [0]
         body = []
         res = self._hrr(A, B, lambda a: 'q%d' % e_index[a], 'AB', 'h', body, cnt)
@@ -371,14 +371,14 @@ class GroupEmitter:
         else:
             outs = [res[(a, b)] for a in A for b in B]
         for u, name in enumerate(outs):
-            L.append('      sb[%d * %d + t] = %s;' % (u, NFP, name))
+            L.append('      sb0[%d * %d + t] = %s;' % (u, NFP, name))
         L.append('    }')
-        L.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        L.append('    ib_sg_sync(SG, sg, sgmask);')
         # ket HRR, lanes over ab
         NAB = na * nb
-        L.append('    for (int u = j; u < %d; u += %d) {' % (NAB, self.G))
+        L.append('    for (int u = r; u < %d; u += SG) {' % NAB)
         for f in range(NF):
-            L.append('      const double w%d = sb[u * %d + %d];' % (f, NFP, f))
+            L.append('      const double w%d = sb0[u * %d + %d];' % (f, NFP, f))
         body = []
         cnt = [0]
         res = self._hrr(Cc, D, lambda c: 'w%d' % f_index[c], 'CD', 'k', body, cnt)
@@ -452,38 +452,62 @@ class GroupEmitter:
                    ' %d chain nodes, %d chain flops/primitive quartet/lane'
                    % (self.la, self.lb, self.lc, self.ld, 'bra' if bra else 'ket', self.G, self.QPW, self.nvar,
                       self.flops))
-        src.append('__constant__ IbLaneInfo ib_lane_%s[%d] = {' % (t, self.G))
+        # per lane: the base-chain steps padded at the front with identity
+        # steps to S_hi (5 bits each: direction 0..2 or 3 = identity, then the
+        # exponent before the step), and the component with the lanes owning
+        # s - 1x, s - 1y, s - 1z (4 + 4 + 4 + 6 + 6 + 6 bits)
+        assert self.S_hi <= 6 and self.G <= 64
+        src.append('__constant__ IbLaneCode ib_lane_%s[%d] = {' % (t, self.G))
         for (c, dirs, nbs, sr) in rows:
-            dd = list(dirs) + [0] * (8 - len(dirs))
-            nn = list(nbs) + [0] * (8 - len(nbs))
-            src.append('  {{%d, %d, %d}, %d, {%s}, {%s}, {%d, %d, %d}},'
-                       % (c[0], c[1], c[2], len(dirs), ', '.join(map(str, dd)), ', '.join(map(str, nn)),
-                          sr[0], sr[1], sr[2]))
+            pad = self.S_hi - len(dirs)
+            steps = [(3, 0)] * pad + list(zip(dirs, nbs))
+            code = 0
+            for k, (d, nb) in enumerate(steps):
+                assert nb < 8
+                code |= (d | (nb << 2)) << (5 * k)
+            assert max(c) < 16
+            misc = c[0] | (c[1] << 4) | (c[2] << 8) | (sr[0] << 12) | (sr[1] << 18) | (sr[2] << 24)
+            src.append('  {0x%08xu, 0x%08xu},' % (code, misc))
         src.append('};')
         src.append('template <typename R, bool SPH>')
         src.append('__global__ void __launch_bounds__(IB_BLOCK) ib_eri_%s(const IbLaunch a) {' % t)
         src.append('  extern __shared__ double ib_smem[];')
-        if self.wide:
-            src.append('  constexpr int QPB = IB_BLOCK / 64;')
-        else:
-            src.append('  constexpr int QPB = (IB_BLOCK / 32) * %d;' % self.QPW)
+        # Slices: W lane groups (W a power of two, chosen per launch) share one
+        # contracted quartet, each sweeping every W-th chunk of its primitive
+        # quartets; the W partial accumulator tables are summed in shared memory
+        # before the HRR.  W grows while the class's quartets cannot fill the
+        # grid's groups, so a class with few (or very long) quartets still uses
+        # the whole device.  W = 1 is the plain one-group-per-quartet kernel.
+        gpb = 'IB_BLOCK / 64' if self.wide else '(IB_BLOCK / 32) * %d' % self.QPW
+        src.append('  constexpr int GPB = %s;  // lane groups per block' % gpb)
         src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (self.cid, self.cid))
-        src.append('  if (beg + (int)blockIdx.x * QPB >= end) return;  // block-uniform')
+        src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices);')
+        src.append('  const int SPB = GPB / W;  // quartets in flight per block')
+        src.append('  if (beg + (int)blockIdx.x * SPB >= end) return;  // block-uniform')
         src.append('  ib_stage_boys(ib_smem, a.boys_tab, %d);' % self.L)
         src.append('  __syncthreads();')
         if self.wide:
             src.append('  const int gid = threadIdx.x / 64, j = threadIdx.x % 64;')
             src.append('  const unsigned gmask = 0xffffffffu;')
+            src.append('  const unsigned sgmask = 0xffffffffu;')
         else:
             src.append('  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;')
             src.append('  const int gq = lane / %d, j = lane %% %d;' % (self.G, self.G))
             src.append('  const int gid = warp * %d + gq;' % self.QPW)
             src.append('  const unsigned gmask = %s;' % ('0xffffffffu' if self.G == 32 else
                                                        '(((1u << %d) - 1u) << (gq * %d))' % (self.G, self.G)))
-        src.append('  (void)gmask;')
+            src.append('  const unsigned sgmask = W * %d >= 32 ? 0xffffffffu : '
+                       '(((1u << (W * %d)) - 1u) << ((gq / W) * W * %d));' % (self.G, self.G, self.G))
+        src.append('  (void)gmask; (void)sgmask;')
+        src.append('  const int sg = gid / W, w = gid - sg * W;  // quartet slot in the block, slice in the quartet')
+        src.append('  const int SG = W * %d, r = w * %d + j;  // lanes per quartet, this lane among them'
+                   % (self.G, self.G))
         nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
         per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
+        per_group += 1  # this slice's FP32 error bound, summed over the slices
         src.append('  double* __restrict__ sb = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + gid * %d;' % per_group)
+        src.append('  double* __restrict__ sb0 = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + sg * W * %d;  // slice 0'
+                   % per_group)
         if self.wide:
             src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb + %d);' % smem_group)
             src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * 64))
@@ -493,11 +517,18 @@ class GroupEmitter:
                        % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0)))
             src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);'
                        % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (17 + self.L + 1) * self.G))
-        src.append('  const IbLaneInfo li = ib_lane_%s[j];' % t)
-        src.append('  const int src0 = li.src[0], src1 = li.src[1], src2 = li.src[2];')
-        src.append('  (void)src0; (void)src1; (void)src2;')
-        src.append('  for (int p = beg + (int)blockIdx.x * QPB + gid; p < end; p += (int)gridDim.x * QPB) {')
-        src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // group-uniform')
+        self.per_group = per_group
+        # lane constants read once and pinned in registers: a divergent
+        # constant-bank load re-issued inside the primitive loop would be
+        # serialised per distinct lane address
+        src.append('  const unsigned lsteps = ib_pin(ib_lane_%s[j].steps), lmisc = ib_pin(ib_lane_%s[j].misc);'
+                   % (t, t))
+        src.append('  const int src0 = (lmisc >> 12) & 63, src1 = (lmisc >> 18) & 63, src2 = (lmisc >> 24) & 63;')
+        src.append('  const double lcx = (double)(lmisc & 15), lcy = (double)((lmisc >> 4) & 15), '
+                   'lcz = (double)((lmisc >> 8) & 15);')
+        src.append('  (void)src0; (void)src1; (void)src2; (void)lsteps; (void)lcx; (void)lcy; (void)lcz;')
+        src.append('  for (int p = beg + (int)blockIdx.x * SPB + sg; p < end; p += (int)gridDim.x * SPB) {')
+        src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // uniform over the quartet\'s lanes')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
         src.append('    double acc[%d];' % NT)
@@ -512,14 +543,25 @@ class GroupEmitter:
                  'o2z', 'roz', 'o2e', 'roe', 'o2zpe']
         self.nfield = len(fields) + L + 1
         if self.G == 1:
-            # one lane per quartet: set up each primitive quartet in registers
-            src.append('    for (int ia = 0; ia < g.k[0]; ++ia)')
-            src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
-            src.append('      IbBraPair bp;')
-            src.append('      ib_bra_pair(a, g, ia, ib, bp);')
-            src.append('      if (bp.K == 0.0) continue;  // every primitive quartet of this pair is zero')
-            src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
-            src.append('      for (int id = 0; id < g.k[3]; ++id) {')
+            # one lane per slice: the slice's primitive quartets (every W-th of
+            # the flattened (ab, cd) range) are set up in registers; the bra
+            # pair is reused while ab does not change
+            src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
+            src.append('    const int kcd = g.k[2] * kd_, np = g.k[0] * kb_ * kcd;')
+            src.append('    // exact small-integer quotients: (x + 0.5) / k is >= 1/128 away from an integer')
+            src.append('    const float rkb = 1.0f / (float)kb_, rkd = 1.0f / (float)kd_;')
+            src.append('    int ab = 0, cd = w - W, ab_last = -1;')
+            src.append('    IbBraPair bp;')
+            src.append('    for (int u = w; u < np; u += W) {')
+            src.append('        cd += W;')
+            src.append('        while (cd >= kcd) { cd -= kcd; ++ab; }')
+            src.append('        if (ab != ab_last) {')
+            src.append('          const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
+            src.append('          ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('          ab_last = ab;')
+            src.append('        }')
+            src.append('        if (bp.K == 0.0) continue;  // every primitive quartet of this pair is zero')
+            src.append('        const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
             src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq)) continue;' % L)
@@ -534,7 +576,7 @@ class GroupEmitter:
             sync = 'ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'
             src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
             src.append('    const int kcd = g.k[2] * kd_, np = g.k[0] * kb_ * kcd;')
-            src.append('    for (int q0 = 0; q0 < np; q0 += %d) {' % self.G)
+            src.append('    for (int q0 = w * %d; q0 < np; q0 += W * %d) {' % (self.G, self.G))
             src.append('      {')
             src.append('        const int q = q0 + j;')
             src.append('        if (q < np) {')
@@ -574,18 +616,22 @@ class GroupEmitter:
             src.append('        const R so2 = o2e, sro = roe;')
             src.append('        const R CXx = PAx, CXy = PAy, CXz = PAz, CWx = WPx, CWy = WPy, CWz = WPz;')
             src.append('        const R co2 = o2z, cro = roz;')
-        src.append('        const R tfx = (R)li.c[0] * o2zpe, tfy = (R)li.c[1] * o2zpe, tfz = (R)li.c[2] * o2zpe;')
+        src.append('        const R tfx = (R)lcx * o2zpe, tfy = (R)lcy * o2zpe, tfz = (R)lcz * o2zpe;')
         src.append('        (void)tfx; (void)tfy; (void)tfz; (void)SXx; (void)SXy; (void)SXz; (void)SWx; (void)SWy;')
         src.append('        (void)SWz; (void)so2; (void)sro; (void)CXx; (void)CXy; (void)CXz; (void)CWx; (void)CWy;')
         src.append('        (void)CWz; (void)co2; (void)cro;')
         for m in range(L + 1):
             src.append('        R c1_%d = f%d, c2_%d = (R)0;' % (m, m, m))
+        # base chain, the same S_hi steps on every lane (identity steps first
+        # on lanes of a lower level: px = 1, wx = 0, nb = 0 keeps c1); the
+        # first real step of a path has nb = 0, so the c2 it sees is unused
         for k in range(1, self.S_hi + 1):
-            src.append('        if (%d <= li.len) {' % k)
-            src.append('          const int d = li.dir[%d];' % (k - 1))
-            src.append('          const R px = d == 0 ? SXx : (d == 1 ? SXy : SXz);')
-            src.append('          const R wx = d == 0 ? SWx : (d == 1 ? SWy : SWz);')
-            src.append('          const R nb = (R)li.nb[%d] * so2;' % (k - 1))
+            src.append('        {')
+            src.append('          const unsigned st = lsteps >> %d;' % (5 * (k - 1)))
+            src.append('          const int d = (int)(st & 3u);')
+            src.append('          const R px = d == 0 ? SXx : (d == 1 ? SXy : (d == 2 ? SXz : (R)1));')
+            src.append('          const R wx = d == 0 ? SWx : (d == 1 ? SWy : (d == 2 ? SWz : (R)0));')
+            src.append('          const R nb = (R)(int)((st >> 2) & 7u) * so2;')
             for m in range(L - k + 1):
                 src.append('          const R t%d = px * c1_%d + wx * c1_%d + nb * (c2_%d - sro * c2_%d);'
                            % (m, m, m + 1, m, m + 1))
@@ -596,7 +642,6 @@ class GroupEmitter:
             src.append('        const R b%d = c1_%d;' % (m, m))
         src += chain
         if self.G == 1:
-            src.append('      }')
             src.append('    }')
         else:
             src.append('      }')
@@ -614,9 +659,17 @@ class GroupEmitter:
             src.append('      ib_group_bar(gid);')
             src.append('      est = sb[0] + sb[1];')
             src.append('      ib_group_bar(gid);')
+        pg = self.per_group
+        src.append('      if (W > 1) {  // sum over the slices')
+        src.append('        ib_sg_sync(SG, sg, sgmask);')
+        src.append('        if (j == 0) sb[%d] = est;' % (pg - 1))
+        src.append('        ib_sg_sync(SG, sg, sgmask);')
+        src.append('        est = 0.0;')
+        src.append('        for (int v = 0; v < W; ++v) est += sb0[v * %d + %d];' % (pg, pg - 1))
+        src.append('      }')
         src.append('      if (est * %s > a.mixed_tol) {' % self.amp_expr())
-        src.append('        if (j == 0) a.flags[p] = 1;')
-        src.append('        continue;  // group-uniform: the FP64 pass recomputes and stores this quartet')
+        src.append('        if (r == 0) a.flags[p] = 1;')
+        src.append('        continue;  // uniform over the quartet: the FP64 pass recomputes and stores it')
         src.append('      }')
         src.append('    }')
         # accumulators -> shared [e][f]
@@ -629,7 +682,16 @@ class GroupEmitter:
             for tt in range(NT):
                 src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NFP, s_lo_idx, tt))
         src.append('    }')
-        src.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        src.append('    ib_sg_sync(SG, sg, sgmask);')
+        src.append('    if (W > 1) {  // slice 0 table += the other slices tables')
+        src.append('      for (int x = r; x < %d; x += SG) {' % (NE * NF))
+        src.append('        const int o = (x / %d) * %d + x %% %d;' % (NF, NFP, NF))
+        src.append('        double s = sb0[o];')
+        src.append('        for (int v = 1; v < W; ++v) s += sb0[v * %d + o];' % self.per_group)
+        src.append('        sb0[o] = s;')
+        src.append('      }')
+        src.append('      ib_sg_sync(SG, sg, sgmask);')
+        src.append('    }')
         src.append('    const double ABx = g.AB[0], ABy = g.AB[1], ABz = g.AB[2];')
         src.append('    const double CDx = g.CD[0], CDy = g.CD[1], CDz = g.CD[2];')
         src.append('    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;')
@@ -639,7 +701,7 @@ class GroupEmitter:
         src.append('    } else {')
         src += ['  ' + s for s in epi_cart]
         src.append('    }')
-        src.append('    %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+        src.append('    ib_sg_sync(SG, sg, sgmask);')
         src.append('  }')
         src.append('}')
         src.append('')

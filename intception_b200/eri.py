@@ -105,6 +105,8 @@ def load():
     lib.intception_b200_eri_batch_noalloc.restype = C.c_int
     lib.intception_b200_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
     lib.intception_b200_fma_peak.restype = C.c_int
+    lib.intception_b200_set_slice_cap.argtypes = [C.c_int, C.c_int]
+    lib.intception_b200_set_slice_cap.restype = C.c_int
     _lib = lib
     return lib
 
@@ -125,6 +127,26 @@ def fma_peak(fp64=True, iters=4096):
     v = C.c_double(0.0)
     _check(load().intception_b200_fma_peak(1 if fp64 else 0, iters, C.byref(v)))
     return v.value
+
+
+def class_id(la, lb, lc, ld):
+    """Canonical class id of (la lb|lc ld): la >= lb, lc >= ld, bra pair >= ket
+    pair (the id the batch kernels are registered under)."""
+    if la < lb:
+        la, lb = lb, la
+    if lc < ld:
+        lc, ld = ld, lc
+    pb, pk = la * (la + 1) // 2 + lb, lc * (lc + 1) // 2 + ld
+    if pb < pk:
+        pb, pk = pk, pb
+    return pb * (pb + 1) // 2 + pk
+
+
+def set_slice_cap(cap, cls=None):
+    """At most cap lane groups (power of two, 0 = no cap) share one quartet
+    in the class kernels: every class, or the canonical class (la,lb,lc,ld)."""
+    cid = -1 if cls is None else class_id(*cls)
+    _check(load().intception_b200_set_slice_cap(cid, int(cap)))
 
 
 def sph_matrix(l):
@@ -307,4 +329,4 @@ def batch_reference_layout(batch):
 
 
 __all__ = ['IntceptionError', 'load', 'lmax', 'sph_matrix', 'work_array_size', 'cont_cart_main', 'cont_sph_main',
-           'boys', 'EriEngine', 'header_functions', '_basis']
+           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap']

@@ -35,6 +35,63 @@ def test_dropin_matches_reference_golden(k):
     assert np.abs(out - ref).max() <= tolerance(ref)
 
 
+def _all_l2_orderings(seed, sph, kmax=4, copies=1, box=3.0):
+    """copies x the 81 (la,lb,lc,ld) orderings with l <= 2, fresh shells each."""
+    rng = np.random.default_rng(seed)
+    quartets = []
+    ls = []
+    for _ in range(copies):
+        for la in range(3):
+            for lb in range(3):
+                for lc in range(3):
+                    for ld in range(3):
+                        base = len(ls)
+                        ls += [la, lb, lc, ld]
+                        quartets.append([base, base + 1, base + 2, base + 3])
+    ks = rng.integers(1, kmax + 1, len(ls)).astype(np.int32)
+    l_, k_, p_, xyz, e, c = basis.make_shells(rng, np.array(ls, np.int32), ks, 0.1, 40.0, box)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    return basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
+
+
+@pytest.mark.parametrize('cap', [1, 2, 4, 8, 16, 32, 64, 0])
+@pytest.mark.parametrize('sph', [False, True])
+def test_slices_every_l2_class_vs_oracle(cap, sph):
+    """Every slice count (lane groups sharing one quartet, forced by the cap;
+    0 = as many as the grid allows, up to a whole block) gives the oracle's
+    blocks: 3 x 81 orderings, K up to 6 so that slices get uneven shares of
+    the primitive quartets."""
+    b = _all_l2_orderings(71 + sph, sph, kmax=6, copies=3)
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    eri.set_slice_cap(cap)
+    try:
+        out = run_batch(b)
+    finally:
+        eri.set_slice_cap(0)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
+@pytest.mark.parametrize('cap', [1, 4, 0])
+def test_slices_mixed_tier_meets_error_bar(cap):
+    """The FP32 tier sums its rounding-error bound over the slices: the
+    rejected quartets are redone in FP64, the rest stay within 1e-10."""
+    import torch
+    b = _all_l2_orderings(81, True, kmax=6, copies=4, box=2.0)
+    eng = eri.EriEngine(b)
+    eri.set_slice_cap(cap)
+    try:
+        ref = eng.compute().clone()
+        bounds = eng.quartet_bounds()
+        mix = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, skip_below=1e-14, fp32_below=1e-2,
+                          mixed_tol=5e-11).clone()
+        torch.cuda.synchronize()
+    finally:
+        eri.set_slice_cap(0)
+    assert eng.device_status() == 0
+    assert np.abs(mix.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-10
+
+
 @pytest.mark.parametrize('sph', [False, True])
 def test_every_l2_class_vs_oracle(sph):
     """All 81 (la,lb,lc,ld) orderings with l <= 2, i.e. every canonical class
