@@ -202,6 +202,13 @@ int intception_b200_last_fp32_rejections(void);
  * rounding for every cap.  New: the reference's functions have no such knob. */
 int intception_b200_set_slice_cap(int cid, int cap);
 
+/* Tuning: register budget of the kernel of canonical class cid for variant v4
+ * (0 FP64 Cartesian, 1 FP64 spherical, 2 FP32 Cartesian, 3 FP32 spherical):
+ * the kernel compiled for minb (1, 3, 4 or 5) resident blocks per SM; 0
+ * restores the default, the autotuner's table built into the library.  New: the
+ * reference has no counterpart. */
+int intception_b200_set_class_minb(int cid, int v4, int minb);
+
 /* Waits for the device and returns the device status word of the last batch
  * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
 int intception_b200_batch_status(void);

@@ -1,0 +1,114 @@
+"""Autotuner for the class kernels (run on the GPU the library will serve).
+
+For every canonical class with l <= 2 it builds a batch of quartets of that
+class with the headline workload's distribution (K uniform in 1..6 per shell,
+exponents log-uniform [0.05, 1e4], centres in a 30-bohr cube, coefficients
+normalised), times the batch with each register budget the library was
+compiled with (``__launch_bounds__(IB_BLOCK, minb)``, minb in 1, 3, 4, 5 resident
+blocks per SM) for each of the four variants (FP64/FP32 VRR x Cartesian/
+spherical), and keeps the fastest.  The FP32 variants are timed with every
+quartet in the FP32 tier and every result accepted, so that the FP32 kernel
+itself is what is measured.
+
+Output: ``intception_b200/tuning.json`` -- per class the chosen budget index
+per variant (``minb``, indexes into (1, 3, 4, 5)) and the measured times.
+``python -m intception_b200.build`` bakes it into the library as the default;
+``eri.set_class_minb`` overrides it at run time.
+
+    python -m intception_b200.autotune [--nq 40000] [--reps 5] [--out PATH]
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+MINB_VALUES = (1, 3, 4, 5)
+VARIANTS = ('fp64_cart', 'fp64_sph', 'fp32_cart', 'fp32_sph')
+
+
+def class_batch(cls, nq, seed, spherical):
+    """nq quartets of the shell-l pattern cls, each over four fresh shells."""
+    from . import basis
+    rng = np.random.default_rng(seed)
+    ls = np.tile(np.asarray(cls, np.int32), nq)
+    ks = rng.integers(1, 7, 4 * nq).astype(np.int32)
+    l, k, ptr, xyz, e, c = basis.make_shells(rng, ls, ks, 0.05, 1.0e4, 30.0)
+    q = np.arange(4 * nq, dtype=np.int32).reshape(nq, 4)
+    off, total = basis.packed_offsets(l, q, spherical)
+    return basis.ShellBatch(l, k, ptr, xyz, e, c, q, off, spherical, total)
+
+
+def time_variant(eng, out, precision, reps, warmup=2):
+    import torch
+    from . import eri
+    kw = {}
+    if precision == eri.PREC_MIXED:
+        kw = dict(bounds=eng._tune_bounds, skip_below=0.0, fp32_below=2.0, mixed_tol=1e300)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(warmup):
+        eng.compute(out=out, precision=precision, **kw)
+    ts = []
+    for _ in range(reps):
+        ev[0].record()
+        eng.compute(out=out, precision=precision, **kw)
+        ev[1].record()
+        torch.cuda.synchronize()
+        ts.append(ev[0].elapsed_time(ev[1]))
+    assert eng.device_status() == 0
+    return float(np.median(ts))
+
+
+def tune(nq=40000, reps=5, classes=None, log=print):
+    import torch
+    from . import eri
+    from .emit.eri_emitter import canonical_classes
+    torch.cuda.set_device(0)
+    classes = classes or canonical_classes(2)
+    result = {}
+    for cls in classes:
+        tag = '%d%d%d%d' % tuple(cls)
+        ent = {'minb': [0, 0, 0, 0], 'ms': {}}
+        for sph in (False, True):
+            b = class_batch(cls, nq, seed=1000 + eri.class_id(*cls), spherical=sph)
+            eng = eri.EriEngine(b)
+            eng._tune_bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+            out = torch.empty(b.out_size, dtype=torch.float64, device='cuda')
+            for prec in (eri.PREC_FP64, eri.PREC_MIXED):
+                v4 = (2 if prec == eri.PREC_MIXED else 0) + (1 if sph else 0)
+                times = []
+                for mi, mb in enumerate(MINB_VALUES):
+                    eri.set_class_minb(cls, v4, mb)
+                    times.append(time_variant(eng, out, prec, reps))
+                best = int(np.argmin(times))
+                eri.set_class_minb(cls, v4, MINB_VALUES[best])
+                ent['minb'][v4] = best
+                ent['ms'][VARIANTS[v4]] = [round(t, 4) for t in times]
+            del eng, out
+        result[tag] = ent
+        log('%s %s' % (tag, ' '.join('%s:%s' % (VARIANTS[v], MINB_VALUES[ent['minb'][v]]) for v in range(4))))
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--nq', type=int, default=40000)
+    ap.add_argument('--reps', type=int, default=5)
+    ap.add_argument('--out', default=os.path.join(PKG, 'tuning.json'))
+    a = ap.parse_args()
+    import torch
+    t0 = time.time()
+    res = tune(a.nq, a.reps)
+    meta = {'device': torch.cuda.get_device_name(0), 'nq_per_class': a.nq, 'reps': a.reps,
+            'minb_values': list(MINB_VALUES), 'variants': list(VARIANTS),
+            'workload': 'per class: K uniform 1..6, alpha log-uniform [0.05,1e4], 30-bohr cube, seed 1000+cid',
+            'seconds': round(time.time() - t0, 1)}
+    with open(a.out, 'w') as fh:
+        json.dump({'meta': meta, 'classes': res}, fh, indent=1)
+    print('wrote', a.out)
+
+
+if __name__ == '__main__':
+    main()

@@ -7,7 +7,7 @@
 //   items [n] IbItem: the four shells of one quartet after canonical permutation
 //   and the output strides that undo it.
 // Boys: F_L(T) by 7-term Taylor about the nearest point of a 1/16 grid (the
-// seven columns L..L+6, divided by k!, staged in shared memory per block),
+// seven columns L..L+6 of the table row, read through the read-only cache),
 // downward recursion to F_0; T >= 36 uses the asymptotic F_0 and upward
 // recursion (the scheme of generator_boys_function.py:98-205 on a finer grid).
 #pragma once
@@ -95,6 +95,12 @@ __device__ __forceinline__ void ib_sg_sync(int SG, int sg, unsigned mask) {
   }
 }
 
+// Register budgets of the class kernels: variant v4 + 4 * mi is launched with
+// __launch_bounds__(IB_BLOCK, IB_MINB_VALUES[mi]) (minimum resident blocks per
+// SM; 1 = no register cap).  The autotuner picks mi per class and variant.
+#define IB_NMINB 4
+__host__ __device__ inline constexpr int ib_minb_value(int mi) { return mi == 0 ? 1 : mi + 2; }  // 1, 3, 4, 5
+
 typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch& a);
 typedef int (*IbOccFn)(int variant);
 struct IbClassEntry {
@@ -106,35 +112,23 @@ struct IbClassEntry {
 
 __host__ __device__ inline constexpr double ib_two_pi52() { return 34.98683665524972497; }  // 2 pi^(5/2)
 
-__host__ inline size_t ib_boys_smem_bytes() {
-  return sizeof(double) * IB_BOYS_NPTS * IB_BOYS_TAYLOR;
-}
-
-// 1/k! for k = 0..6 without a local array (a runtime-indexed array would live on the stack).
-__device__ __forceinline__ double ib_invfact(int k) {
-  double r = 1.0;
-  for (int i = 2; i <= k; ++i) r /= (double)i;
-  return r;
-}
-
-// Stage the Taylor coefficients g_k = F_{L+k}(T_i)/k! for k = 0..6 of every grid point.
-__device__ __forceinline__ void ib_stage_boys(double* __restrict__ s, const double* __restrict__ tab, int L) {
-  for (int idx = threadIdx.x; idx < IB_BOYS_NPTS * IB_BOYS_TAYLOR; idx += blockDim.x) {
-    const int i = idx / IB_BOYS_TAYLOR, k = idx - i * IB_BOYS_TAYLOR;
-    s[idx] = __ldg(tab + i * IB_BOYS_NCOL + L + k) * ib_invfact(k);
-  }
-}
-
-// F_m(T), m = 0..L, into F[] (compile-time L so the recursion unrolls).
+// F_m(T), m = 0..L, into F[] (compile-time L so the recursion unrolls), from
+// the global table (rows of IB_BOYS_NCOL values F_n(T_i); the seven columns
+// L..L+6 of one row are read through the read-only cache, which keeps the
+// class's 578 x 7 working set resident next to the kernel's shared memory).
 template <int L>
-__device__ __forceinline__ void ib_boys(double T, const double* __restrict__ s, double* F) {
+__device__ __forceinline__ void ib_boys(double T, const double* __restrict__ tab, double* F) {
   if (T < IB_BOYS_TMAX) {
     const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
     const double dx = (double)i * (1.0 / IB_BOYS_H_INV) - T;
-    const double* r = s + i * IB_BOYS_TAYLOR;
-    double f = r[6];
-#pragma unroll
-    for (int k = 5; k >= 0; --k) f = fma(f, dx, r[k]);
+    const double* r = tab + i * IB_BOYS_NCOL + L;
+    double f = __ldg(r + 6) * (1.0 / 720.0);
+    f = fma(f, dx, __ldg(r + 5) * (1.0 / 120.0));
+    f = fma(f, dx, __ldg(r + 4) * (1.0 / 24.0));
+    f = fma(f, dx, __ldg(r + 3) * (1.0 / 6.0));
+    f = fma(f, dx, __ldg(r + 2) * 0.5);
+    f = fma(f, dx, __ldg(r + 1));
+    f = fma(f, dx, __ldg(r));
     F[L] = f;
     if (L > 0) {
       const double e = exp(-T), t2 = T + T;
@@ -260,7 +254,7 @@ struct IbPrimQuartet {
 // skipping it leaves the contracted sums bit-identical.
 template <typename R, int L>
 __device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuartet& g, const IbBraPair& bp, int ic,
-                                                int id, const double* __restrict__ boys_s, double* F,
+                                                int id, const double* __restrict__ boys_tab, double* F,
                                                 IbPrimQuartet<R>& pq) {
   const double xc = __ldg(a.prim_exp + g.ptr[2] + ic), cc = __ldg(a.prim_coef + g.ptr[2] + ic);
   const double xd = __ldg(a.prim_exp + g.ptr[3] + id), cd = __ldg(a.prim_coef + g.ptr[3] + id);
@@ -276,7 +270,7 @@ __device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuart
     PQ[d] = bp.P[d] - Q[d];
   }
   const double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
-  ib_boys<L>(rho * RPQ2, boys_s, F);
+  ib_boys<L>(rho * RPQ2, boys_tab, F);
   const double pref = ib_two_pi52() * bp.oz * oe * sqrt(ozpe) * bp.K * Kcd;
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;

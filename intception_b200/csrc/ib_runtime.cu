@@ -35,6 +35,8 @@ void ib_register_emitted_classes(IbClassEntry* table);
 void build_sph_host(std::vector<double>& out);
 extern const int ib_n_emitted_classes;
 extern const int ib_lmax_emitted;
+extern const int ib_tuned_minb[IB_NCLASS][4];
+extern const int ib_tuned_slice_cap[IB_NCLASS];
 __global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double* scratch, long long slice);
 
 namespace {
@@ -114,7 +116,8 @@ struct Context {
   DevBuf d_stage, d_cart, d_res;
   HostBuf h_stage, h_res;
   IbClassEntry table[IB_NCLASS] = {};
-  int occ[IB_NCLASS][4] = {};
+  int occ[IB_NCLASS][4 * IB_NMINB] = {};
+  int minb_idx[IB_NCLASS][4] = {};  // register budget chosen per class and variant (autotuned defaults)
   std::mutex mu;
 };
 
@@ -351,8 +354,6 @@ int get_context(Context** out) {
     IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     if (const char* env = std::getenv("INTCEPTION_B200_STREAMS")) c->nside = std::max(1, std::min(kNSideMax, std::atoi(env)));
-    if (const char* env = std::getenv("INTCEPTION_B200_MAX_SLICES"))
-      for (int cid = 0; cid < IB_NCLASS; ++cid) c->slice_cap[cid] = std::max(0, std::atoi(env));
     for (int i = 0; i < c->nside; ++i) {
       IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
       IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
@@ -372,8 +373,12 @@ int get_context(Context** out) {
     for (int cid = 0; cid < IB_NCLASS; ++cid) {
       if (!c->table[cid].launch) continue;
       kind[cid] = c->table[cid].kind;
-      for (int v = 0; v < 4; ++v) c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
+      for (int v = 0; v < 4 * IB_NMINB; ++v) c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
+      for (int v = 0; v < 4; ++v) c->minb_idx[cid][v] = std::min(std::max(ib_tuned_minb[cid][v], 0), IB_NMINB - 1);
+      c->slice_cap[cid] = ib_tuned_slice_cap[cid];
     }
+    if (const char* env = std::getenv("INTCEPTION_B200_MAX_SLICES"))
+      for (int cid = 0; cid < IB_NCLASS; ++cid) c->slice_cap[cid] = std::max(0, std::atoi(env));
     IB_CUDA(c->kind.ensure(IB_NCLASS * sizeof(int)));
     IB_CUDA(cudaMemcpy(c->kind.p, kind.data(), IB_NCLASS * sizeof(int), cudaMemcpyHostToDevice));
     IB_CUDA(cudaGetLastError());
@@ -426,10 +431,11 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     for (int cid = IB_NCLASS - 1; cid >= 0; --cid) {
       if (!c->table[cid].launch) continue;
       if (prec == 1 && c->table[cid].kind != 2) continue;
-      const int grid = c->nsm * c->occ[cid][variant];
+      const int vt = variant + 4 * c->minb_idx[cid][variant];
+      const int grid = c->nsm * c->occ[cid][vt];
       cudaStream_t ss = c->side[k % c->nside];
       ap.max_slices = c->slice_cap[cid];
-      c->table[cid].launch(variant, grid, ss, ap);
+      c->table[cid].launch(vt, grid, ss, ap);
       ++k;
       if (prec == 1) {
         // FP64 pass over the same items: recomputes the quartets the FP32
@@ -437,7 +443,8 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
         IbLaunch ar = ap;
         ar.recheck = 1;
         const int v64 = sph ? 1 : 0;
-        c->table[cid].launch(v64, c->nsm * c->occ[cid][v64], ss, ar);
+        const int vt64 = v64 + 4 * c->minb_idx[cid][v64];
+        c->table[cid].launch(vt64, c->nsm * c->occ[cid][vt64], ss, ar);
         ++k;
       }
     }
@@ -605,8 +612,9 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
   a.out = c->d_cart.as<double>();
   IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
   if (emitted) {
-    const int grid = std::max(1, std::min(c->nsm * c->occ[cid][0], (nblk + IB_BLOCK - 1) / IB_BLOCK));
-    c->table[cid].launch(0, grid, s, a);
+    const int vt = 4 * c->minb_idx[cid][0];
+    const int grid = std::max(1, std::min(c->nsm * c->occ[cid][vt], (nblk + IB_BLOCK - 1) / IB_BLOCK));
+    c->table[cid].launch(vt, grid, s, a);
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
     long long nb = std::min<long long>({(long long)nblk, 2LL * c->nsm,
@@ -1086,6 +1094,25 @@ int intception_b200_set_slice_cap(int cid, int cap) {
   if (cid >= IB_NCLASS || cap < 0) return set_status(IB_ERR_ARG, "set_slice_cap: class id or cap out of range");
   for (int k = 0; k < IB_NCLASS; ++k)
     if (cid < 0 || k == cid) c->slice_cap[k] = cap;
+  return set_status(IB_OK, "");
+}
+
+// Register budget of the kernel of canonical class cid for variant v4
+// (0 FP64 Cartesian, 1 FP64 spherical, 2 FP32 Cartesian, 3 FP32 spherical):
+// minb = minimum resident blocks per SM it was compiled for (1, 3, 4, 5);
+// 0 restores the built-in (autotuned) default.
+int intception_b200_set_class_minb(int cid, int v4, int minb) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  int mi = -1;
+  for (int k = 0; k < IB_NMINB; ++k)
+    if (ib_minb_value(k) == minb) mi = k;
+  if (minb == 0 && cid >= 0 && cid < IB_NCLASS && v4 >= 0 && v4 <= 3)
+    mi = std::min(std::max(ib_tuned_minb[cid][v4], 0), IB_NMINB - 1);  // back to the built-in default
+  if (cid < 0 || cid >= IB_NCLASS || v4 < 0 || v4 > 3 || mi < 0 || !c->table[cid].launch)
+    return set_status(IB_ERR_ARG, "set_class_minb: class, variant or budget not available");
+  c->minb_idx[cid][v4] = mi;
   return set_status(IB_OK, "");
 }
 

@@ -40,6 +40,8 @@ LMAX_EMIT = 2  # classes with every l <= LMAX_EMIT get an unrolled kernel
 THREAD_CLASSES = set()
 
 DIRS = 'xyz'
+NPAIR_TOTAL = 7 * 8 // 2                       # shell pairs with l <= 6 (IB_NPAIR)
+NCLASS_TOTAL = NPAIR_TOTAL * (NPAIR_TOTAL + 1) // 2  # canonical classes (IB_NCLASS)
 
 
 def comps(l):
@@ -331,11 +333,8 @@ class Emitter:
                    % (self.la, self.lb, self.lc, self.ld, self.nvar, self.flops, self.hrr_flops))
         src.append('template <typename R, bool SPH>')
         src.append('__global__ void __launch_bounds__(IB_BLOCK) ib_eri_%s(const IbLaunch a) {' % t)
-        src.append('  extern __shared__ double ib_boys_s[];')
         src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (cid, cid))
         src.append('  if (beg + (int)(blockIdx.x * blockDim.x) >= end) return;  // block-uniform')
-        src.append('  ib_stage_boys(ib_boys_s, a.boys_tab, %d);' % L)
-        src.append('  __syncthreads();')
         src.append('  for (int p = beg + blockIdx.x * blockDim.x + threadIdx.x; p < end; p += gridDim.x * blockDim.x) {')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
@@ -351,7 +350,7 @@ class Emitter:
         src.append('      for (int id = 0; id < g.k[3]; ++id) {')
         src.append('      IbPrimQuartet<R> pq;')
         src.append('      double F[%d];' % (L + 1))
-        src.append('      if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_boys_s, F, pq)) continue;' % L)
+        src.append('      if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq)) continue;' % L)
         for m in range(L + 1):
             src.append('      const R s%d = (R)F[%d];' % (m, m))
         src.append('      const R PAx = pq.PA[0], PAy = pq.PA[1], PAz = pq.PA[2];')
@@ -382,7 +381,7 @@ class Emitter:
         src.append('')
         # host-side launcher and occupancy query for this class
         src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
-        src.append('  const size_t smem = ib_boys_smem_bytes();')
+        src.append('  const size_t smem = 0;')
         src.append('  switch (variant) {')
         src.append('    case 0: ib_eri_%s<double, false><<<grid, IB_BLOCK, smem, s>>>(a); break;' % t)
         src.append('    case 1: ib_eri_%s<double, true><<<grid, IB_BLOCK, smem, s>>>(a); break;' % t)
@@ -391,7 +390,7 @@ class Emitter:
         src.append('  }')
         src.append('}')
         src.append('static int ib_occupancy_%s(int variant) {' % t)
-        src.append('  int n = 0; const size_t smem = ib_boys_smem_bytes();')
+        src.append('  int n = 0; const size_t smem = 0;')
         src.append('  switch (variant) {')
         src.append('    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ib_eri_%s<double, false>, IB_BLOCK, smem); break;' % t)
         src.append('    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ib_eri_%s<double, true>, IB_BLOCK, smem); break;' % t)
@@ -469,6 +468,23 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
     for g in range(ngroups):
         disp.append('  ib_register_group_%d(table);' % g)
     disp.append('}')
+    # autotuned defaults (intception_b200/tuning.json, written by
+    # python -m intception_b200.autotune on a GPU): per class and variant the
+    # register-budget index, per class the slice cap
+    minb = [[0] * 4 for _ in range(NCLASS_TOTAL)]
+    scap = [0] * NCLASS_TOTAL
+    tpath = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'tuning.json')
+    if os.path.exists(tpath):
+        import json
+        with open(tpath) as fh:
+            tun = json.load(fh)
+        for tag, ent in tun.get('classes', {}).items():
+            cid = class_id(*(int(ch) for ch in tag))
+            minb[cid] = [int(x) for x in ent.get('minb', [0, 0, 0, 0])]
+            scap[cid] = int(ent.get('slice_cap', 0))
+    disp.append('extern const int ib_tuned_minb[%d][4] = {%s};'
+                % (NCLASS_TOTAL, ', '.join('{%s}' % ', '.join(map(str, r)) for r in minb)))
+    disp.append('extern const int ib_tuned_slice_cap[%d] = {%s};' % (NCLASS_TOTAL, ', '.join(map(str, scap))))
     disp.append('extern const int ib_n_emitted_classes = %d;' % len(classes))
     disp.append('extern const int ib_lmax_emitted = %d;' % lmax)
     _write_if_changed(os.path.join(outdir, 'eri_dispatch.cu'), '\n'.join(disp) + '\n')

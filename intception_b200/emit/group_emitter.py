@@ -71,10 +71,18 @@ def group_size(n):
     return g
 
 
+# register budgets offered to the autotuner: __launch_bounds__(IB_BLOCK, MINB)
+# asks for MINB resident blocks per SM (1: no register cap); must match
+# IB_MINB_VALUES in ib_eri_device.cuh
+MINB_VALUES = (1, 3, 4, 5)
+
+
 class GroupEmitter:
-    def __init__(self, la, lb, lc, ld):
+    def __init__(self, la, lb, lc, ld, tuned=None):
         self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
         self.L = la + lb + lc + ld
+        # every register budget is instantiated for the l <= 2 classes
+        self.tuned = max(la, lb, lc, ld) <= 2 if tuned is None else tuned
         self.E, self.F = la + lb, lc + ld
         self.orient = orientation(la, lb, lc, ld)
         assert self.orient is not None
@@ -469,8 +477,8 @@ class GroupEmitter:
             misc = c[0] | (c[1] << 4) | (c[2] << 8) | (sr[0] << 12) | (sr[1] << 18) | (sr[2] << 24)
             src.append('  {0x%08xu, 0x%08xu},' % (code, misc))
         src.append('};')
-        src.append('template <typename R, bool SPH>')
-        src.append('__global__ void __launch_bounds__(IB_BLOCK) ib_eri_%s(const IbLaunch a) {' % t)
+        src.append('template <typename R, bool SPH, int MINB>')
+        src.append('__global__ void __launch_bounds__(IB_BLOCK, MINB) ib_eri_%s(const IbLaunch a) {' % t)
         src.append('  extern __shared__ double ib_smem[];')
         # Slices: W lane groups (W a power of two, chosen per launch) share one
         # contracted quartet, each sweeping every W-th chunk of its primitive
@@ -484,8 +492,6 @@ class GroupEmitter:
         src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices);')
         src.append('  const int SPB = GPB / W;  // quartets in flight per block')
         src.append('  if (beg + (int)blockIdx.x * SPB >= end) return;  // block-uniform')
-        src.append('  ib_stage_boys(ib_smem, a.boys_tab, %d);' % self.L)
-        src.append('  __syncthreads();')
         if self.wide:
             src.append('  const int gid = threadIdx.x / 64, j = threadIdx.x % 64;')
             src.append('  const unsigned gmask = 0xffffffffu;')
@@ -505,8 +511,8 @@ class GroupEmitter:
         nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
         per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
         per_group += 1  # this slice's FP32 error bound, summed over the slices
-        src.append('  double* __restrict__ sb = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + gid * %d;' % per_group)
-        src.append('  double* __restrict__ sb0 = ib_smem + IB_BOYS_NPTS * IB_BOYS_TAYLOR + sg * W * %d;  // slice 0'
+        src.append('  double* __restrict__ sb = ib_smem + gid * %d;' % per_group)
+        src.append('  double* __restrict__ sb0 = ib_smem + sg * W * %d;  // slice 0'
                    % per_group)
         if self.wide:
             src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb + %d);' % smem_group)
@@ -564,7 +570,7 @@ class GroupEmitter:
             src.append('        const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
-            src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq)) continue;' % L)
+            src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq)) continue;' % L)
             src.append('        if (sizeof(R) == 4) est += %s;' % self.err_expr())
             for f, nm in zip(fields, names):
                 src.append('        const R %s = pq.%s;' % (nm, f))
@@ -587,7 +593,7 @@ class GroupEmitter:
             src.append('          ib_bra_pair(a, g, ia, ib, bp);')
             src.append('          IbPrimQuartet<R> pq;')
             src.append('          double F[%d];' % (L + 1))
-            src.append('          const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, ib_smem, F, pq);' % L)
+            src.append('          const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
             src.append('          if (live) {')
             for k, f in enumerate(fields):
                 src.append('            ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
@@ -706,27 +712,37 @@ class GroupEmitter:
         src.append('}')
         src.append('')
         if self.wide:
-            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 64) * %d)' % per_group
+            smem_bytes = '(sizeof(double) * (IB_BLOCK / 64) * %d)' % per_group
         else:
-            smem_bytes = '(ib_boys_smem_bytes() + sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, per_group)
+            smem_bytes = '(sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, per_group)
         src.append('static size_t ib_smem_%s() { return %s; }' % (t, smem_bytes))
-        src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
-        src.append('  const size_t smem = ib_smem_%s();' % t)
-        src.append('  switch (variant) {')
+        # variant = v4 + 4 * mi: v4 = precision x output (FP64/FP32 x Cartesian/
+        # spherical), mi indexes the register budget IB_MINB[mi] (minimum
+        # resident blocks per SM); classes outside the tuned set instantiate
+        # mi = 0 only
         variants = (('double', 'false'), ('double', 'true'), ('float', 'false'), ('float', 'true'))
         if not fp32:
             variants = variants[:2] * 2
-        for v, (R, S) in enumerate(variants):
-            src.append('    case %d: ib_eri_%s<%s, %s><<<grid, IB_BLOCK, smem, s>>>(a); break;' % (v, t, R, S))
+        minbs = list(range(len(MINB_VALUES))) if self.tuned else [0]
+        cases = []
+        for mi in range(len(MINB_VALUES)):
+            for v, (R, S) in enumerate(variants):
+                use = mi if mi in minbs else 0
+                cases.append((v + 4 * mi, 'ib_eri_%s<%s, %s, %d>' % (t, R, S, MINB_VALUES[use])))
+        src.append('static void ib_launch_%s(int variant, int grid, cudaStream_t s, const IbLaunch& a) {' % t)
+        src.append('  const size_t smem = ib_smem_%s();' % t)
+        src.append('  switch (variant) {')
+        for v, fn in cases:
+            src.append('    case %d: %s<<<grid, IB_BLOCK, smem, s>>>(a); break;' % (v, fn))
         src.append('  }')
         src.append('}')
         src.append('static int ib_occupancy_%s(int variant) {' % t)
         src.append('  int n = 0; const size_t smem = ib_smem_%s();' % t)
         src.append('  switch (variant) {')
-        for v, (R, S) in enumerate(variants):
-            src.append('    case %d: cudaFuncSetAttribute(ib_eri_%s<%s, %s>, cudaFuncAttributeMaxDynamicSharedMemorySize, '
-                       '(int)smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ib_eri_%s<%s, %s>, IB_BLOCK, '
-                       'smem); break;' % (v, t, R, S, t, R, S))
+        for v, fn in cases:
+            src.append('    case %d: cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicSharedMemorySize, '
+                       '(int)smem); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, %s, IB_BLOCK, '
+                       'smem); break;' % (v, fn, fn))
         src.append('  }')
         src.append('  return n;')
         src.append('}')

@@ -107,6 +107,8 @@ def load():
     lib.intception_b200_fma_peak.restype = C.c_int
     lib.intception_b200_set_slice_cap.argtypes = [C.c_int, C.c_int]
     lib.intception_b200_set_slice_cap.restype = C.c_int
+    lib.intception_b200_set_class_minb.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.intception_b200_set_class_minb.restype = C.c_int
     _lib = lib
     return lib
 
@@ -147,6 +149,13 @@ def set_slice_cap(cap, cls=None):
     in the class kernels: every class, or the canonical class (la,lb,lc,ld)."""
     cid = -1 if cls is None else class_id(*cls)
     _check(load().intception_b200_set_slice_cap(cid, int(cap)))
+
+
+def set_class_minb(cls, variant, minb):
+    """Register budget of canonical class cls = (la,lb,lc,ld) for variant
+    0..3 (FP64 cart, FP64 sph, FP32 cart, FP32 sph): the kernel compiled for
+    minb in (1, 3, 4, 5) resident blocks per SM; 0 restores the default."""
+    _check(load().intception_b200_set_class_minb(class_id(*cls), int(variant), int(minb)))
 
 
 def sph_matrix(l):
@@ -329,4 +338,4 @@ def batch_reference_layout(batch):
 
 
 __all__ = ['IntceptionError', 'load', 'lmax', 'sph_matrix', 'work_array_size', 'cont_cart_main', 'cont_sph_main',
-           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap']
+           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap', 'set_class_minb']

@@ -72,6 +72,35 @@ def test_slices_every_l2_class_vs_oracle(cap, sph):
     assert np.abs(out - ref).max() <= tolerance(ref)
 
 
+@pytest.mark.parametrize('minb', [1, 3, 4, 5])
+def test_every_register_budget_vs_oracle(minb):
+    """Each register budget the class kernels are compiled with (minimum
+    resident blocks per SM) gives the oracle's blocks, FP64 Cartesian and
+    spherical, and the FP32 tier stays within 1e-10 of FP64."""
+    import torch
+    from intception_b200.emit.eri_emitter import canonical_classes
+    classes = canonical_classes(2)
+    try:
+        for cls in classes:
+            for v4 in range(4):
+                eri.set_class_minb(cls, v4, minb)
+        for sph in (False, True):
+            b = _all_l2_orderings(91 + sph, sph, kmax=5, copies=2)
+            ref = loader.oracle_batch(b, basis.sph_matrices(6))
+            eng = eri.EriEngine(b)
+            out = eng.compute()
+            bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+            mix = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, fp32_below=2.0, mixed_tol=5e-11)
+            torch.cuda.synchronize()
+            assert eng.device_status() == 0
+            assert np.abs(out.cpu().numpy() - ref).max() <= tolerance(ref)
+            assert np.abs(mix.cpu().numpy() - ref).max() <= 1e-10
+    finally:
+        for cls in classes:
+            for v4 in range(4):
+                eri.set_class_minb(cls, v4, 0)
+
+
 @pytest.mark.parametrize('cap', [1, 4, 0])
 def test_slices_mixed_tier_meets_error_bar(cap):
     """The FP32 tier sums its rounding-error bound over the slices: the
