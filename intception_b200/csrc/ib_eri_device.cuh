@@ -82,6 +82,14 @@ __device__ __forceinline__ int ib_slices(int n, int gpb, int cap) {
   return w;
 }
 
+// Slices for kernels with three lane groups per warp: 3 (one warp per
+// quartet) when the class's quartets fill at most a third of the grid's groups
+// and the cap allows it, else 1.
+__device__ __forceinline__ int ib_slices_in_threes(int n, int gpb, int cap) {
+  const long long groups = (long long)gridDim.x * gpb;
+  return ((cap == 0 || cap >= 3) && (long long)n * 3 <= groups) ? 3 : 1;
+}
+
 // Barrier over the sg-th quartet slot of the block (SG lanes): a warp-level
 // sync inside a warp, named barrier sg+1 for two warps, the block barrier for
 // the whole block.  Every lane of the slot calls it the same number of times.

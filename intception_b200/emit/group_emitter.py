@@ -71,6 +71,9 @@ def group_size(n):
     return g
 
 
+# pack ten-lane groups three to a warp (False: pad them to 16 lanes, two per warp)
+PACK_TEN = True
+
 # register budgets offered to the autotuner: __launch_bounds__(IB_BLOCK, MINB)
 # asks for MINB resident blocks per SM (1: no register cap); must match
 # IB_MINB_VALUES in ib_eri_device.cuh
@@ -92,6 +95,12 @@ class GroupEmitter:
             self.S_lo, self.S_hi, self.C_lo, self.C_hi = lc, self.F, la, self.E
         self.NL = ncum(self.S_hi)
         self.G = group_size(self.NL)
+        # ten lane-side components: three 10-lane groups per warp (lanes 30
+        # and 31 idle) instead of two padded 16-lane groups; shuffles then
+        # address absolute lanes and slices come in threes (one warp)
+        self.packed = PACK_TEN and self.NL == 10
+        if self.packed:
+            self.G = 10
         # G = 64: two warps per quartet; transfer operands go through shared
         # memory, one named barrier per recurrence level
         self.wide = self.G > 32
@@ -180,6 +189,13 @@ class GroupEmitter:
             self.shuffles[key] = ('x%d' % len(self.shuffles), level)
         return self.shuffles[key][0]
 
+    def _shfl_call(self, name, i):
+        """Read register `name` of the lane owning s - 1i (src0..2 hold group-
+        relative lanes for power-of-two groups, absolute lanes when packed)."""
+        if self.packed:
+            return '__shfl_sync(gmask, %s, src%d)' % (name, i)
+        return '__shfl_sync(gmask, %s, src%d, %d)' % (name, i, self.G)
+
     def slot_index(self, c, m):
         """Position of chain node (c, m), m >= 1, in its level's transfer buffer."""
         k = sum(c)
@@ -258,7 +274,7 @@ class GroupEmitter:
         for ln in body:
             for var in re.findall(r'\bx\d+\b', ln):
                 src_name, i = shuf[var]
-                ln = re.sub(r'\b%s\b' % var, '__shfl_sync(gmask, %s, src%d, %d)' % (src_name, i, self.G), ln)
+                ln = re.sub(r'\b%s\b' % var, self._shfl_call(src_name, i), ln)
             out.append(ln)
         defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
         return defs + out, len(targets)
@@ -283,7 +299,7 @@ class GroupEmitter:
         shuf_by_level = {}
         for (src_name, i), (var, lvl) in self.shuffles.items():
             shuf_by_level.setdefault(lvl + 1, []).append(
-                '        const R %s = __shfl_sync(gmask, %s, src%d, %d);' % (var, src_name, i, self.G))
+                '        const R %s = %s;' % (var, self._shfl_call(src_name, i)))
         t_index = {c: t for t, c in enumerate(targets)}
         out = []
         if ZERO in t_index:
@@ -489,7 +505,10 @@ class GroupEmitter:
         gpb = 'IB_BLOCK / 64' if self.wide else '(IB_BLOCK / 32) * %d' % self.QPW
         src.append('  constexpr int GPB = %s;  // lane groups per block' % gpb)
         src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (self.cid, self.cid))
-        src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices);')
+        if self.packed:
+            src.append('  const int W = ib_slices_in_threes(end - beg, GPB, a.max_slices);')
+        else:
+            src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices);')
         src.append('  const int SPB = GPB / W;  // quartets in flight per block')
         src.append('  if (beg + (int)blockIdx.x * SPB >= end) return;  // block-uniform')
         if self.wide:
@@ -499,6 +518,10 @@ class GroupEmitter:
         else:
             src.append('  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;')
             src.append('  const int gq = lane / %d, j = lane %% %d;' % (self.G, self.G))
+            if self.packed:
+                # lanes past the last group of the warp take no part: slices stay
+                # inside a warp (W = 1 or 3), so no barrier needs them
+                src.append('  if (gq >= %d) return;' % self.QPW)
             src.append('  const int gid = warp * %d + gq;' % self.QPW)
             src.append('  const unsigned gmask = %s;' % ('0xffffffffu' if self.G == 32 else
                                                        '(((1u << %d) - 1u) << (gq * %d))' % (self.G, self.G)))
@@ -529,7 +552,11 @@ class GroupEmitter:
         # serialised per distinct lane address
         src.append('  const unsigned lsteps = ib_pin(ib_lane_%s[j].steps), lmisc = ib_pin(ib_lane_%s[j].misc);'
                    % (t, t))
-        src.append('  const int src0 = (lmisc >> 12) & 63, src1 = (lmisc >> 18) & 63, src2 = (lmisc >> 24) & 63;')
+        if self.packed:
+            src.append('  const int src0 = gq * %d + ((lmisc >> 12) & 63), src1 = gq * %d + ((lmisc >> 18) & 63), '
+                       'src2 = gq * %d + ((lmisc >> 24) & 63);' % (self.G, self.G, self.G))
+        else:
+            src.append('  const int src0 = (lmisc >> 12) & 63, src1 = (lmisc >> 18) & 63, src2 = (lmisc >> 24) & 63;')
         src.append('  const double lcx = (double)(lmisc & 15), lcy = (double)((lmisc >> 4) & 15), '
                    'lcz = (double)((lmisc >> 8) & 15);')
         src.append('  (void)src0; (void)src1; (void)src2; (void)lsteps; (void)lcx; (void)lcy; (void)lcz;')
@@ -655,7 +682,13 @@ class GroupEmitter:
             src.append('    }')
         # FP32: sum the error bound over the group, reject the quartet if too large
         src.append('    if (sizeof(R) == 4) {')
-        if self.G > 1 and not self.wide:
+        if self.packed:  # not a power of two: through the group's table area, still unused
+            src.append('      sb[j] = est;')
+            src.append('      __syncwarp(gmask);')
+            src.append('      est = 0.0;')
+            src.append('      for (int v = 0; v < %d; ++v) est += sb[v];' % self.G)
+            src.append('      __syncwarp(gmask);')
+        elif self.G > 1 and not self.wide:
             src.append('      for (int o = %d; o > 0; o >>= 1) est += __shfl_xor_sync(gmask, est, o, %d);'
                        % (self.G // 2, self.G))
         elif self.wide:
