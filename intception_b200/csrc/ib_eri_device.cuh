@@ -237,17 +237,52 @@ struct IbBraPair {
   double P[3], PA[3];
 };
 
+// Prefactor c_a c_b exp(-xa xb/(xa+xb) R^2) of a primitive pair: the one
+// expression every pair evaluation uses, so that a pair culled for a zero
+// prefactor is exactly a pair whose primitive quartets would all be zero.
+__device__ __forceinline__ double ib_pair_factor(double xa, double ca, double xb, double cb, double oz, double r2) {
+  return ca * cb * exp(-xa * xb * oz * r2);
+}
+
 __device__ __forceinline__ void ib_bra_pair(const IbLaunch& a, const IbQuartet& g, int ia, int ib, IbBraPair& bp) {
   const double xa = __ldg(a.prim_exp + g.ptr[0] + ia), ca = __ldg(a.prim_coef + g.ptr[0] + ia);
   const double xb = __ldg(a.prim_exp + g.ptr[1] + ib), cb = __ldg(a.prim_coef + g.ptr[1] + ib);
   bp.zeta = xa + xb;
   bp.oz = 1.0 / bp.zeta;
-  bp.K = ca * cb * exp(-xa * xb * bp.oz * g.RAB2);
+  bp.K = ib_pair_factor(xa, ca, xb, cb, bp.oz, g.RAB2);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     bp.P[d] = (xa * g.A[d] + xb * g.B[d]) * bp.oz;
     bp.PA[d] = bp.P[d] - g.A[d];
   }
+}
+
+// Live primitive pairs of one side of the quartet (side 0: shells a, b; 1: c, d)
+// within the tile of pair indices [p0, p0 + n), n <= 64: the offsets t (pair
+// p0 + t, pair index = i0 * K1 + i1) whose prefactor is not zero, in
+// increasing order, into lst[]; returns their number.  Run by nb <= 32
+// builder lanes of one warp (b = this lane's rank, bmask their lanes, bbase
+// the lane of rank 0); every builder returns the same count.
+__device__ __forceinline__ int ib_live_pairs(const IbLaunch& a, const IbQuartet& g, int side, int p0, int n,
+                                             unsigned char* __restrict__ lst, int b, int nb, unsigned bmask,
+                                             int bbase) {
+  const int ptr0 = g.ptr[2 * side], ptr1 = g.ptr[2 * side + 1], k1 = g.k[2 * side + 1];
+  const double r2 = side ? g.RCD2 : g.RAB2;
+  int cnt = 0;
+  for (int t0 = 0; t0 < n; t0 += nb) {
+    const int t = t0 + b;
+    bool live = false;
+    if (t < n) {
+      const int p = p0 + t, i0 = p / k1, i1 = p - i0 * k1;
+      const double x0 = __ldg(a.prim_exp + ptr0 + i0), c0 = __ldg(a.prim_coef + ptr0 + i0);
+      const double x1 = __ldg(a.prim_exp + ptr1 + i1), c1 = __ldg(a.prim_coef + ptr1 + i1);
+      live = ib_pair_factor(x0, c0, x1, c1, 1.0 / (x0 + x1), r2) != 0.0;
+    }
+    const unsigned bal = __ballot_sync(bmask, live) >> bbase;
+    if (live) lst[cnt + __popc(bal & ((1u << b) - 1u))] = (unsigned char)t;
+    cnt += __popc(bal);
+  }
+  return cnt;
 }
 
 template <typename R>
@@ -267,7 +302,7 @@ __device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuart
   const double xc = __ldg(a.prim_exp + g.ptr[2] + ic), cc = __ldg(a.prim_coef + g.ptr[2] + ic);
   const double xd = __ldg(a.prim_exp + g.ptr[3] + id), cd = __ldg(a.prim_coef + g.ptr[3] + id);
   const double eta = xc + xd, oe = 1.0 / eta;
-  const double Kcd = cc * cd * exp(-xc * xd * oe * g.RCD2);
+  const double Kcd = ib_pair_factor(xc, cc, xd, cd, oe, g.RCD2);
   if (bp.K * Kcd == 0.0) return false;
   const double ozpe = 1.0 / (bp.zeta + eta);
   const double rho = bp.zeta * eta * ozpe;

@@ -533,6 +533,8 @@ class GroupEmitter:
                    % (self.G, self.G))
         nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
         per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
+        self.list_off = per_group
+        per_group += 17  # live-pair lists of the quartet's current tile (2 x 64 bytes) and their counts
         per_group += 1  # this slice's FP32 error bound, summed over the slices
         src.append('  double* __restrict__ sb = ib_smem + gid * %d;' % per_group)
         src.append('  double* __restrict__ sb0 = ib_smem + sg * W * %d;  // slice 0'
@@ -547,6 +549,8 @@ class GroupEmitter:
             src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);'
                        % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (17 + self.L + 1) * self.G))
         self.per_group = per_group
+        src.append('  unsigned char* __restrict__ lst = reinterpret_cast<unsigned char*>(sb0 + %d);' % self.list_off)
+        src.append('  int* __restrict__ lcnt = reinterpret_cast<int*>(sb0 + %d);' % (self.list_off + 16))
         # lane constants read once and pinned in registers: a divergent
         # constant-bank load re-issued inside the primitive loop would be
         # serialised per distinct lane address
@@ -575,25 +579,44 @@ class GroupEmitter:
         names = ['PAx', 'PAy', 'PAz', 'WPx', 'WPy', 'WPz', 'QCx', 'QCy', 'QCz', 'WQx', 'WQy', 'WQz',
                  'o2z', 'roz', 'o2e', 'roe', 'o2zpe']
         self.nfield = len(fields) + L + 1
+        # Pair tiles of at most 64 x 64 primitive pairs; in each, the first
+        # min(SG, 32) lanes of the quartet list the pairs whose prefactor is
+        # not zero (ib_live_pairs), and the slices run over live x live
+        # primitive quartets only (the others are exactly zero)
+        src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
+        src.append('    const int kab = g.k[0] * kb_, kcd = g.k[2] * kd_;')
+        src.append('    // exact small-integer quotients: (x + 0.5) / k is >= 1/128 away from an integer')
+        src.append('    const float rkb = 1.0f / (float)kb_, rkd = 1.0f / (float)kd_;')
+        src.append('    for (int ab0 = 0; ab0 < kab; ab0 += 64)')
+        src.append('    for (int cd0 = 0; cd0 < kcd; cd0 += 64) {')
+        src.append('      if (r < 32) {')
+        src.append('        const int nbld = min(SG, 32);')
+        if self.wide:
+            src.append('        const unsigned bmask = 0xffffffffu;')
+            src.append('        const int bbase = 0;')
+        else:
+            src.append('        const unsigned bmask = SG >= 32 ? 0xffffffffu : sgmask;')
+            src.append('        const int bbase = SG >= 32 ? 0 : lane - r;')
+        src.append('        const int n0 = ib_live_pairs(a, g, 0, ab0, min(64, kab - ab0), lst, r, nbld, bmask, bbase);')
+        src.append('        const int n1 = ib_live_pairs(a, g, 1, cd0, min(64, kcd - cd0), lst + 64, r, nbld, bmask, bbase);')
+        src.append('        if (r == 0) { lcnt[0] = n0; lcnt[1] = n1; }')
+        src.append('      }')
+        src.append('      ib_sg_sync(SG, sg, sgmask);')
+        src.append('      const int nl1 = lcnt[1], npl = lcnt[0] * nl1;')
+        src.append('      const float rn1 = 1.0f / (float)max(nl1, 1);')
         if self.G == 1:
-            # one lane per slice: the slice's primitive quartets (every W-th of
-            # the flattened (ab, cd) range) are set up in registers; the bra
-            # pair is reused while ab does not change
-            src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
-            src.append('    const int kcd = g.k[2] * kd_, np = g.k[0] * kb_ * kcd;')
-            src.append('    // exact small-integer quotients: (x + 0.5) / k is >= 1/128 away from an integer')
-            src.append('    const float rkb = 1.0f / (float)kb_, rkd = 1.0f / (float)kd_;')
-            src.append('    int ab = 0, cd = w - W, ab_last = -1;')
-            src.append('    IbBraPair bp;')
-            src.append('    for (int u = w; u < np; u += W) {')
-            src.append('        cd += W;')
-            src.append('        while (cd >= kcd) { cd -= kcd; ++ab; }')
+            # one lane per slice: every W-th live primitive quartet, set up in
+            # registers; the bra pair is reused while it does not change
+            src.append('      int ab_last = -1;')
+            src.append('      IbBraPair bp;')
+            src.append('      for (int u = w; u < npl; u += W) {')
+            src.append('        const int qa = (int)(((float)u + 0.5f) * rn1), qc = u - qa * nl1;')
+            src.append('        const int ab = ab0 + lst[qa], cd = cd0 + lst[64 + qc];')
             src.append('        if (ab != ab_last) {')
             src.append('          const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
             src.append('          ib_bra_pair(a, g, ia, ib, bp);')
             src.append('          ab_last = ab;')
             src.append('        }')
-            src.append('        if (bp.K == 0.0) continue;  // every primitive quartet of this pair is zero')
             src.append('        const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
@@ -604,39 +627,38 @@ class GroupEmitter:
             for m in range(L + 1):
                 src.append('        const R f%d = (R)F[%d];' % (m, m))
         else:
-            # lane j sets up primitive quartet q0 + j of the chunk; the group
-            # then sweeps the chunk reading the shared values (broadcast)
+            # lane j sets up live primitive quartet q0 + j of the chunk; the
+            # group then sweeps the chunk reading the shared values (broadcast)
             sync = 'ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'
-            src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
-            src.append('    const int kcd = g.k[2] * kd_, np = g.k[0] * kb_ * kcd;')
-            src.append('    for (int q0 = w * %d; q0 < np; q0 += W * %d) {' % (self.G, self.G))
-            src.append('      {')
-            src.append('        const int q = q0 + j;')
-            src.append('        if (q < np) {')
-            src.append('          const int ab = q / kcd, cd = q - ab * kcd;')
-            src.append('          const int ia = ab / kb_, ib = ab - ia * kb_;')
-            src.append('          const int ic = cd / kd_, id = cd - ic * kd_;')
-            src.append('          IbBraPair bp;')
-            src.append('          ib_bra_pair(a, g, ia, ib, bp);')
-            src.append('          IbPrimQuartet<R> pq;')
-            src.append('          double F[%d];' % (L + 1))
-            src.append('          const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
-            src.append('          if (live) {')
+            src.append('      for (int q0 = w * %d; q0 < npl; q0 += W * %d) {' % (self.G, self.G))
+            src.append('        {')
+            src.append('          const int q = q0 + j;')
+            src.append('          if (q < npl) {')
+            src.append('            const int qa = (int)(((float)q + 0.5f) * rn1), qc = q - qa * nl1;')
+            src.append('            const int ab = ab0 + lst[qa], cd = cd0 + lst[64 + qc];')
+            src.append('            const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
+            src.append('            const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
+            src.append('            IbBraPair bp;')
+            src.append('            ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('            IbPrimQuartet<R> pq;')
+            src.append('            double F[%d];' % (L + 1))
+            src.append('            const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
+            src.append('            if (live) {')
             for k, f in enumerate(fields):
-                src.append('            ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
+                src.append('              ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
             for m in range(L + 1):
-                src.append('            ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
-            src.append('            if (sizeof(R) == 4) est += %s;' % self.err_expr())
+                src.append('              ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
+            src.append('              if (sizeof(R) == 4) est += %s;' % self.err_expr())
+            src.append('            }')
+            src.append('            pz[j] = live ? 1 : 0;  // 0 only where the two pair prefactors multiply to zero')
             src.append('          }')
-            src.append('          pz[j] = live ? 1 : 0;')
             src.append('        }')
-            src.append('      }')
-            src.append('      %s;' % sync)
-            src.append('      const int nu = min(%d, np - q0);' % self.G)
-            src.append('      for (int u = 0; u < nu; ++u) {')
-            src.append('        if (!pz[u]) continue;  // group-uniform: exact-zero primitive quartet')
+            src.append('        %s;' % sync)
+            src.append('        const int nu = min(%d, npl - q0);' % self.G)
+            src.append('        for (int u = 0; u < nu; ++u) {')
+            src.append('          if (!pz[u]) continue;  // group-uniform: exact-zero primitive quartet')
             for k, nm in enumerate(names):
-                src.append('        const R %s = ps[%d * %d + u];' % (nm, k, self.G))
+                src.append('          const R %s = ps[%d * %d + u];' % (nm, k, self.G))
             for m in range(L + 1):
                 src.append('        const R f%d = ps[%d * %d + u];' % (m, len(fields) + m, self.G))
         if bra:
@@ -675,11 +697,13 @@ class GroupEmitter:
             src.append('        const R b%d = c1_%d;' % (m, m))
         src += chain
         if self.G == 1:
-            src.append('    }')
-        else:
             src.append('      }')
-            src.append('      %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
-            src.append('    }')
+        else:
+            src.append('        }')
+            src.append('        %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+            src.append('      }')
+        src.append('      ib_sg_sync(SG, sg, sgmask);  // every slice is done with the lists before the next tile')
+        src.append('    }')
         # FP32: sum the error bound over the group, reject the quartet if too large
         src.append('    if (sizeof(R) == 4) {')
         if self.packed:  # not a power of two: through the group's table area, still unused
