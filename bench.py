@@ -58,6 +58,8 @@ def parse():
     ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx'],
                     help='eri: the headline; *_2idx: the example script\'s two-index classes')
     ap.add_argument('--npairs', type=int, default=4_000_000)
+    ap.add_argument('--only', default=None, choices=['fp64', 'screened'],
+                    help='profiling: run only this ERI step (W warm-up + K timed) and print its time')
     return ap.parse_args()
 
 
@@ -388,6 +390,30 @@ def run_twoidx(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_only(args, eng, out):
+    """One step kind alone (for profilers): the FP64 step over every quartet,
+    or the screened FP64 step (bounds computed first, outside the timing)."""
+    import torch
+    from intception_b200 import eri
+    bounds, skip = None, 0.0
+    if args.only == 'screened':
+        bounds, skip = eng.quartet_bounds(), SKIP_BELOW
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        eng.compute(out=out, bounds=bounds, skip_below=skip)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        eng.compute(out=out, bounds=bounds, skip_below=skip)
+    ev1.record()
+    torch.cuda.synchronize()
+    assert eng.device_status() == 0
+    print(json.dumps({'only': args.only, 'nq': args.nq, 'steps': args.steps, 'warmup': args.warmup,
+                      'ms_per_step': ev0.elapsed_time(ev1) / args.steps,
+                      'kernels_per_step': eri.EriEngine.last_launch_count()}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_init(args.gpus)
@@ -406,6 +432,9 @@ def main():
     eng = eri.EriEngine(batch)
     stream = torch.cuda.current_stream()
     out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+    if args.only:
+        run_only(args, eng, out)
+        return
 
     def step(precision=eri.PREC_FP64, bounds=None, skip=0.0):
         eng.compute(out=out, precision=precision, bounds=bounds, skip_below=skip, fp32_below=FP32_BELOW,

@@ -410,6 +410,18 @@ long long generic_slice(int lmax) {
   return (best + 31) / 32 * 32;
 }
 
+// Largest l of canonical class cid (pair index pb = la(la+1)/2 + lb, pb >= pk).
+int class_lmax(int cid) {
+  int pb = 0;
+  while ((pb + 1) * (pb + 2) / 2 <= cid) ++pb;
+  int la = 0;
+  while ((la + 1) * (la + 2) / 2 <= pb) ++la;
+  const int pk = cid - pb * (pb + 1) / 2;
+  int lc = 0;
+  while ((lc + 1) * (lc + 2) / 2 <= pk) ++lc;
+  return std::max(la, lc);
+}
+
 // Launch the emitted kernels for the given variants and the generic kernel;
 // items/ranges already on the device.  Returns the number of kernels launched.
 int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
@@ -429,7 +441,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     const int variant = prec * 2 + (sph ? 1 : 0);
     // heaviest classes first so they start early on their streams
     for (int cid = IB_NCLASS - 1; cid >= 0; --cid) {
-      if (!c->table[cid].launch) continue;
+      if (!c->table[cid].launch || class_lmax(cid) > lmax) continue;  // no quartet of the batch has this class
       if (prec == 1 && c->table[cid].kind != 2) continue;
       const int vt = variant + 4 * c->minb_idx[cid][variant];
       const int grid = c->nsm * c->occ[cid][vt];
