@@ -224,26 +224,34 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
 }
 
 // Screened-out quartets (bound below the skip threshold, so |(ab|cd)| <= bound):
-// their blocks are written as zeros, one warp per quartet.
+// their blocks are written as zeros, 32 quartets per warp.
 __global__ void ib_zero_blocks(const IbItem* __restrict__ items, const int* __restrict__ ranges,
                                const int* __restrict__ shell_l, int spherical, double* __restrict__ out) {
+  // A quartet's block is the contiguous range [off, off + na nb nc nd) whatever
+  // the canonical permutation (it only reorders the four indices).  Each lane
+  // fetches one quartet's offset and size; the warp then writes the 32 blocks
+  // with coalesced stores.
   const int beg = ranges[kSlotSkip], end = ranges[kSlotSkip + 1];
   const int lane = threadIdx.x & 31;
   const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (int p = beg + wg; p < end; p += nw) {
-    const IbItem it = items[p];
-    int n[4];
-    for (int i = 0; i < 4; ++i) {
-      const int l = min(max(shell_l[it.s[i]], 0), IB_LMAX);
-      n[i] = spherical ? 2 * l + 1 : ib_ncart_d(l);
+  for (int base = beg + wg * 32; base < end; base += nw * 32) {  // warp-uniform
+    const int p = base + lane;
+    long long off = 0;
+    int tot = 0;
+    if (p < end) {
+      const IbItem it = items[p];
+      tot = 1;
+      for (int i = 0; i < 4; ++i) {
+        const int l = min(max(shell_l[it.s[i]], 0), IB_LMAX);
+        tot *= spherical ? 2 * l + 1 : ib_ncart_d(l);
+      }
+      off = it.off;
     }
-    double* o = out + it.off;
-    const int tot = n[0] * n[1] * n[2] * n[3];
-    for (int e = lane; e < tot; e += 32) {
-      const int i3 = e % n[3], r3 = e / n[3];
-      const int i2 = r3 % n[2], r2 = r3 / n[2];
-      const int i1 = r2 % n[1], i0 = r2 / n[1];
-      o[(long long)i0 * it.st[0] + (long long)i1 * it.st[1] + (long long)i2 * it.st[2] + (long long)i3 * it.st[3]] = 0.0;
+    for (int k = 0; k < 32; ++k) {
+      const long long o = __shfl_sync(0xffffffffu, off, k);
+      const int n = __shfl_sync(0xffffffffu, tot, k);
+      double* __restrict__ d = out + o;
+      for (int e = lane; e < n; e += 32) d[e] = 0.0;
     }
   }
 }
