@@ -308,6 +308,108 @@ class EriEngine:
         return load().intception_b200_batch_status()
 
 
+class HostPipeline:
+    """Batches held in pinned host memory, streamed through the current GPU with
+    the copies overlapped: while batch i is evaluated, the inputs of batch i+1
+    go up and the blocks of batch i-1 come down (``depth`` device buffer sets,
+    one stream per direction, events between them; the evaluations themselves
+    run one after another on one stream, as they share the library's work
+    buffers).  ``submit`` returns once the batch is queued; the host output of a
+    batch is valid after ``synchronize`` (or ``wait``) covers it.
+
+    A batch is a dict of pinned host tensors: shell_l, shell_k, shell_ptr
+    (int32), shell_xyz, prim_exp, prim_coef (float64), quartets (int32, 4 per
+    quartet), out_off (int64), and with screening bounds (float64), laid out as
+    ``basis.ShellBatch``.
+    """
+
+    INPUTS = ('shell_l', 'shell_k', 'shell_ptr', 'shell_xyz', 'prim_exp', 'prim_coef', 'quartets', 'out_off',
+              'bounds')
+
+    def __init__(self, spherical, depth=2, device='cuda'):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.spherical = bool(spherical)
+        self.depth = int(depth)
+        self.s_in = torch.cuda.Stream(self.device)
+        self.s_run = torch.cuda.Stream(self.device)
+        self.s_out = torch.cuda.Stream(self.device)
+        self.slots = [{'buf': {}, 'ev': {}, 'used': set()} for _ in range(self.depth)]
+        self.k = 0
+        load()
+
+    def _buffer(self, slot, name, like, n):
+        b = slot['buf'].get(name)
+        if b is None or b.numel() < n:
+            b = self.torch.empty(max(n, 1), dtype=like.dtype, device=self.device)
+            slot['buf'][name] = b
+        return b
+
+    def _event(self, slot, name):
+        ev = slot['ev'].get(name)
+        if ev is None:
+            ev = slot['ev'][name] = self.torch.cuda.Event()
+        return ev
+
+    def _wait(self, stream, slot, name):
+        if name in slot['used']:
+            stream.wait_event(slot['ev'][name])
+
+    def submit(self, h, out_host, precision=PREC_FP64, skip_below=0.0, fp32_below=0.0, mixed_tol=5e-11, lmax=None):
+        """Queue one batch; out_host (pinned float64, the batch's output size)
+        receives its blocks."""
+        torch = self.torch
+        slot = self.slots[self.k % self.depth]
+        self.k += 1
+        nq = h['quartets'].numel() // 4
+        nout = out_host.numel()
+        if lmax is None:
+            lmax = int(h['shell_l'].max()) if h['shell_l'].numel() else 0
+        names = [n for n in self.INPUTS if h.get(n) is not None]
+        # inputs up, once the slot's previous evaluation has read its inputs
+        self._wait(self.s_in, slot, 'run')
+        d = {}
+        with torch.cuda.stream(self.s_in):
+            for n in names:
+                src = h[n].reshape(-1)
+                d[n] = self._buffer(slot, n, src, src.numel())
+                d[n][:src.numel()].copy_(src, non_blocking=True)
+        self._event(slot, 'in').record(self.s_in)
+        slot['used'].add('in')
+        out = self._buffer(slot, 'out', out_host, nout)
+        # evaluation, once the inputs are up and the slot's previous blocks are down
+        self.s_run.wait_event(slot['ev']['in'])
+        self._wait(self.s_run, slot, 'down')
+        bas = _Basis(d['shell_l'].data_ptr(), d['shell_k'].data_ptr(), d['shell_ptr'].data_ptr(),
+                     d['shell_xyz'].data_ptr(), d['prim_exp'].data_ptr(), d['prim_coef'].data_ptr(),
+                     h['shell_l'].numel(), h['prim_exp'].numel(), lmax)
+        st = load().intception_b200_eri_batch(
+            C.byref(bas), d['quartets'].data_ptr(), d['out_off'].data_ptr(), nq, 1 if self.spherical else 0,
+            precision, d['bounds'].data_ptr() if 'bounds' in d else None, float(skip_below), float(fp32_below),
+            float(mixed_tol), out.data_ptr(), C.c_void_p(self.s_run.cuda_stream))
+        _check(st)
+        self._event(slot, 'run').record(self.s_run)
+        slot['used'].add('run')
+        # blocks down
+        self.s_out.wait_event(slot['ev']['run'])
+        with torch.cuda.stream(self.s_out):
+            out_host.reshape(-1)[:nout].copy_(out[:nout], non_blocking=True)
+        self._event(slot, 'down').record(self.s_out)
+        slot['used'].add('down')
+
+    def wait_event(self):
+        """A CUDA event recorded after every queued copy-out (for timing)."""
+        ev = self.torch.cuda.Event(enable_timing=True)
+        ev.record(self.s_out)
+        return ev
+
+    def synchronize(self):
+        self.s_out.synchronize()
+        self.s_run.synchronize()
+        self.s_in.synchronize()
+
+
 class EriGraph:
     """A captured batch (intception_b200_eri_graph_*)."""
 
@@ -338,4 +440,4 @@ def batch_reference_layout(batch):
 
 
 __all__ = ['IntceptionError', 'load', 'lmax', 'sph_matrix', 'work_array_size', 'cont_cart_main', 'cont_sph_main',
-           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap', 'set_class_minb']
+           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap', 'set_class_minb', 'HostPipeline']
