@@ -11,11 +11,17 @@ quartet in the FP32 tier and every result accepted, so that the FP32 kernel
 itself is what is measured.
 
 Output: ``intception_b200/tuning.json`` -- per class the chosen budget index
-per variant (``minb``, indexes into (1, 3, 4, 5)) and the measured times.
-``python -m intception_b200.build`` bakes it into the library as the default;
-``eri.set_class_minb`` overrides it at run time.
+per variant (``minb``, indexes into (1, 3, 4, 5)), the chain emission order
+(``order``) and the measured times.  ``python -m intception_b200.build`` bakes
+it into the library (budgets as defaults, ``eri.set_class_minb`` overrides
+them at run time; the order selects the emitted code).
+
+The chain order changes the emitted code, so it is tuned across builds: build
+and tune once per order (``INTCEPTION_B200_CHAIN_ORDER=dfs`` and ``=level``
+set for both the build and the tuning run), then ``--merge`` the two files.
 
     python -m intception_b200.autotune [--nq 40000] [--reps 5] [--out PATH]
+    python -m intception_b200.autotune --merge dfs.json level.json --out PATH
 """
 import argparse
 import json
@@ -92,18 +98,54 @@ def tune(nq=40000, reps=5, classes=None, log=print):
     return result
 
 
+def merge(paths, out):
+    """Combine tuning runs made with different chain orders (one build per
+    order, INTCEPTION_B200_CHAIN_ORDER=dfs|level): per class the order whose
+    kernels were fastest over the four variants (each at its best budget), and
+    that run's budgets."""
+    runs = []
+    for p in paths:
+        with open(p) as fh:
+            runs.append(json.load(fh))
+    classes = {}
+    for tag in runs[0]['classes']:
+        best = None
+        for r in runs:
+            ent = r['classes'][tag]
+            cost = sum(min(v) for v in ent['ms'].values())
+            if best is None or cost < best[0]:
+                best = (cost, r, ent)
+        ent = dict(best[2])
+        ent['order'] = best[1]['meta']['chain_order']
+        ent['ms_by_order'] = {r['meta']['chain_order']: round(sum(min(v) for v in r['classes'][tag]['ms'].values()), 4)
+                              for r in runs}
+        classes[tag] = ent
+    meta = dict(runs[0]['meta'])
+    meta['chain_order'] = 'per class (merged: %s)' % ', '.join(r['meta']['chain_order'] for r in runs)
+    with open(out, 'w') as fh:
+        json.dump({'meta': meta, 'classes': classes}, fh, indent=1)
+    return classes
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--nq', type=int, default=40000)
     ap.add_argument('--reps', type=int, default=5)
     ap.add_argument('--out', default=os.path.join(PKG, 'tuning.json'))
+    ap.add_argument('--merge', nargs='+', default=None,
+                    help='combine tuning files of builds with different chain orders into --out (no GPU)')
     a = ap.parse_args()
+    if a.merge:
+        merge(a.merge, a.out)
+        print('wrote', a.out)
+        return
     import torch
     t0 = time.time()
     res = tune(a.nq, a.reps)
     meta = {'device': torch.cuda.get_device_name(0), 'nq_per_class': a.nq, 'reps': a.reps,
             'minb_values': list(MINB_VALUES), 'variants': list(VARIANTS),
             'workload': 'per class: K uniform 1..6, alpha log-uniform [0.05,1e4], 30-bohr cube, seed 1000+cid',
+            'chain_order': os.environ.get('INTCEPTION_B200_CHAIN_ORDER', 'as built'),
             'seconds': round(time.time() - t0, 1)}
     with open(a.out, 'w') as fh:
         json.dump({'meta': meta, 'classes': res}, fh, indent=1)

@@ -59,9 +59,33 @@ def orientation(la, lb, lc, ld):
     return 'bra' if ne <= nf else 'ket'
 
 
-# emit the chain level by level with each level's shuffles batched (True), or
-# in dependency order with shuffles inline (False: fewer live registers)
-LEVEL_ORDER = False
+# Chain emission order, per class: 'level' (level by level, each level's
+# shuffles batched: more independent work between dependent instructions, more
+# live registers) or 'dfs' (dependency order with shuffles inline).  Chosen by
+# the autotuner (intception_b200/tuning.json "order"); INTCEPTION_B200_CHAIN_ORDER
+# forces one order for every class (the autotuner's tuning builds).
+def _chain_orders():
+    import json
+    import os
+    out = {}
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'tuning.json')
+    if os.path.exists(path):
+        with open(path) as fh:
+            for tag, ent in json.load(fh).get('classes', {}).items():
+                if ent.get('order') in ('level', 'dfs'):
+                    out[tag] = ent['order']
+    return out
+
+
+CHAIN_ORDER = _chain_orders()
+
+
+def chain_order(tag):
+    import os
+    forced = os.environ.get('INTCEPTION_B200_CHAIN_ORDER')
+    if forced in ('level', 'dfs'):
+        return forced
+    return CHAIN_ORDER.get(tag, 'dfs')
 
 
 def group_size(n):
@@ -285,7 +309,7 @@ class GroupEmitter:
         nodes, then the accumulation of the level's targets."""
         if self.wide:
             return self.emit_chain_wide()
-        if not LEVEL_ORDER:
+        if chain_order(self.tag) == 'dfs':
             return self.emit_chain_dfs()
         targets = comps_range(self.C_lo, self.C_hi)
         for c in targets:
