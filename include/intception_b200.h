@@ -209,6 +209,13 @@ int intception_b200_set_slice_cap(int cid, int cap);
  * reference has no counterpart. */
 int intception_b200_set_class_minb(int cid, int v4, int minb);
 
+/* Tuning: whether the FP32 tier (IB_PREC_MIXED) runs the FP32-VRR kernel of
+ * canonical class cid (cid < 0: every class): 1 where the class has one, 0
+ * never (that class's FP32-tier quartets are evaluated in FP64), -1 the
+ * default built into the library (the classes whose FP32 kernel the autotuner
+ * measured faster).  Waits for the device.  New: no reference counterpart. */
+int intception_b200_set_class_fp32(int cid, int on);
+
 /* Waits for the device and returns the device status word of the last batch
  * (IB_OK, IB_ERR_ARG for an out-of-range l, IB_ERR_SCRATCH). */
 int intception_b200_batch_status(void);

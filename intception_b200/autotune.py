@@ -33,6 +33,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 MINB_VALUES = (1, 3, 4, 5)
 VARIANTS = ('fp64_cart', 'fp64_sph', 'fp32_cart', 'fp32_sph')
+FP32_GAIN = 0.97  # the FP32 kernel must be at least 3 % faster (rejected quartets are redone in FP64)
 
 
 def class_batch(cls, nq, seed, spherical):
@@ -93,8 +94,12 @@ def tune(nq=40000, reps=5, classes=None, log=print):
                 ent['minb'][v4] = best
                 ent['ms'][VARIANTS[v4]] = [round(t, 4) for t in times]
             del eng, out
+        # the FP32 tier uses this class's FP32 kernel only where it beats FP64
+        ent['fp32'] = bool(min(ent['ms']['fp32_sph']) < FP32_GAIN * min(ent['ms']['fp64_sph']) and
+                           min(ent['ms']['fp32_cart']) < FP32_GAIN * min(ent['ms']['fp64_cart']))
         result[tag] = ent
-        log('%s %s' % (tag, ' '.join('%s:%s' % (VARIANTS[v], MINB_VALUES[ent['minb'][v]]) for v in range(4))))
+        log('%s %s fp32:%s' % (tag, ' '.join('%s:%s' % (VARIANTS[v], MINB_VALUES[ent['minb'][v]]) for v in range(4)),
+                               ent['fp32']))
     return result
 
 
@@ -117,6 +122,9 @@ def merge(paths, out):
                 best = (cost, r, ent)
         ent = dict(best[2])
         ent['order'] = best[1]['meta']['chain_order']
+        ms = ent['ms']
+        ent['fp32'] = bool(min(ms['fp32_sph']) < FP32_GAIN * min(ms['fp64_sph']) and
+                           min(ms['fp32_cart']) < FP32_GAIN * min(ms['fp64_cart']))
         ent['ms_by_order'] = {r['meta']['chain_order']: round(sum(min(v) for v in r['classes'][tag]['ms'].values()), 4)
                               for r in runs}
         classes[tag] = ent

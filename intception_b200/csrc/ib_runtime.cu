@@ -37,6 +37,7 @@ extern const int ib_n_emitted_classes;
 extern const int ib_lmax_emitted;
 extern const int ib_tuned_minb[IB_NCLASS][4];
 extern const int ib_tuned_slice_cap[IB_NCLASS];
+extern const int ib_tuned_fp32[IB_NCLASS];
 __global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double* scratch, long long slice);
 
 namespace {
@@ -113,6 +114,7 @@ struct Context {
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;                                             // FP32 rejections of the last mixed batch
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
+  int kind_h[IB_NCLASS] = {};  // host copy of kind: 2 where the class has FP32 kernels and the FP32 tier uses them
   DevBuf d_stage, d_cart, d_res;
   HostBuf h_stage, h_res;
   IbClassEntry table[IB_NCLASS] = {};
@@ -380,7 +382,8 @@ int get_context(Context** out) {
     std::vector<int> kind(IB_NCLASS, 0);
     for (int cid = 0; cid < IB_NCLASS; ++cid) {
       if (!c->table[cid].launch) continue;
-      kind[cid] = c->table[cid].kind;
+      kind[cid] = (c->table[cid].kind == 2 && ib_tuned_fp32[cid]) ? 2 : 1;
+      c->kind_h[cid] = kind[cid];
       for (int v = 0; v < 4 * IB_NMINB; ++v) c->occ[cid][v] = std::max(1, c->table[cid].occupancy(v));
       for (int v = 0; v < 4; ++v) c->minb_idx[cid][v] = std::min(std::max(ib_tuned_minb[cid][v], 0), IB_NMINB - 1);
       c->slice_cap[cid] = ib_tuned_slice_cap[cid];
@@ -450,7 +453,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
     // heaviest classes first so they start early on their streams
     for (int cid = IB_NCLASS - 1; cid >= 0; --cid) {
       if (!c->table[cid].launch || class_lmax(cid) > lmax) continue;  // no quartet of the batch has this class
-      if (prec == 1 && c->table[cid].kind != 2) continue;
+      if (prec == 1 && c->kind_h[cid] != 2) continue;
       const int vt = variant + 4 * c->minb_idx[cid][variant];
       const int grid = c->nsm * c->occ[cid][vt];
       cudaStream_t ss = c->side[k % c->nside];
@@ -1133,6 +1136,25 @@ int intception_b200_set_class_minb(int cid, int v4, int minb) {
   if (cid < 0 || cid >= IB_NCLASS || v4 < 0 || v4 > 3 || mi < 0 || !c->table[cid].launch)
     return set_status(IB_ERR_ARG, "set_class_minb: class, variant or budget not available");
   c->minb_idx[cid][v4] = mi;
+  return set_status(IB_OK, "");
+}
+
+// Whether the FP32 tier runs the FP32 kernel of canonical class cid (cid < 0:
+// every class): on = 1 where the class has one, 0 never (its FP32-tier
+// quartets run in FP64), -1 the built-in (autotuned) default.  Waits for the
+// device first: the classify kernel of a batch in flight reads the table.
+int intception_b200_set_class_fp32(int cid, int on) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  if (cid >= IB_NCLASS || on < -1 || on > 1) return set_status(IB_ERR_ARG, "set_class_fp32: class id or value");
+  for (int k = 0; k < IB_NCLASS; ++k) {
+    if ((cid >= 0 && k != cid) || !c->table[k].launch) continue;
+    const int want = on < 0 ? ib_tuned_fp32[k] : on;
+    c->kind_h[k] = (c->table[k].kind == 2 && want) ? 2 : 1;
+  }
+  IB_CUDA(cudaDeviceSynchronize());
+  IB_CUDA(cudaMemcpy(c->kind.p, c->kind_h, IB_NCLASS * sizeof(int), cudaMemcpyHostToDevice));
   return set_status(IB_OK, "");
 }
 

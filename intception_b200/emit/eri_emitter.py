@@ -470,9 +470,11 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
     disp.append('}')
     # autotuned defaults (intception_b200/tuning.json, written by
     # python -m intception_b200.autotune on a GPU): per class and variant the
-    # register-budget index, per class the slice cap
+    # register-budget index, per class the slice cap and whether the FP32 tier
+    # uses the class's FP32 kernel (where it measured faster than FP64)
     minb = [[0] * 4 for _ in range(NCLASS_TOTAL)]
     scap = [0] * NCLASS_TOTAL
+    fp32on = [1] * NCLASS_TOTAL
     tpath = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'tuning.json')
     if os.path.exists(tpath):
         import json
@@ -482,9 +484,11 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
             cid = class_id(*(int(ch) for ch in tag))
             minb[cid] = [int(x) for x in ent.get('minb', [0, 0, 0, 0])]
             scap[cid] = int(ent.get('slice_cap', 0))
+            fp32on[cid] = 1 if ent.get('fp32', True) else 0
     disp.append('extern const int ib_tuned_minb[%d][4] = {%s};'
                 % (NCLASS_TOTAL, ', '.join('{%s}' % ', '.join(map(str, r)) for r in minb)))
     disp.append('extern const int ib_tuned_slice_cap[%d] = {%s};' % (NCLASS_TOTAL, ', '.join(map(str, scap))))
+    disp.append('extern const int ib_tuned_fp32[%d] = {%s};' % (NCLASS_TOTAL, ', '.join(map(str, fp32on))))
     disp.append('extern const int ib_n_emitted_classes = %d;' % len(classes))
     disp.append('extern const int ib_lmax_emitted = %d;' % lmax)
     _write_if_changed(os.path.join(outdir, 'eri_dispatch.cu'), '\n'.join(disp) + '\n')

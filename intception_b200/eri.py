@@ -109,6 +109,8 @@ def load():
     lib.intception_b200_set_slice_cap.restype = C.c_int
     lib.intception_b200_set_class_minb.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.intception_b200_set_class_minb.restype = C.c_int
+    lib.intception_b200_set_class_fp32.argtypes = [C.c_int, C.c_int]
+    lib.intception_b200_set_class_fp32.restype = C.c_int
     _lib = lib
     return lib
 
@@ -156,6 +158,13 @@ def set_class_minb(cls, variant, minb):
     0..3 (FP64 cart, FP64 sph, FP32 cart, FP32 sph): the kernel compiled for
     minb in (1, 3, 4, 5) resident blocks per SM; 0 restores the default."""
     _check(load().intception_b200_set_class_minb(class_id(*cls), int(variant), int(minb)))
+
+
+def set_class_fp32(on, cls=None):
+    """Whether the FP32 tier runs the FP32 kernel of class cls (every class
+    when None): True, False, or None for the built-in default."""
+    cid = -1 if cls is None else class_id(*cls)
+    _check(load().intception_b200_set_class_fp32(cid, -1 if on is None else int(bool(on))))
 
 
 def sph_matrix(l):
@@ -440,4 +449,4 @@ def batch_reference_layout(batch):
 
 
 __all__ = ['IntceptionError', 'load', 'lmax', 'sph_matrix', 'work_array_size', 'cont_cart_main', 'cont_sph_main',
-           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap', 'set_class_minb', 'HostPipeline']
+           'boys', 'EriEngine', 'header_functions', '_basis', 'class_id', 'set_slice_cap', 'set_class_minb', 'set_class_fp32', 'HostPipeline']

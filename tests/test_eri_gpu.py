@@ -81,6 +81,7 @@ def test_every_register_budget_vs_oracle(minb):
     from intception_b200.emit.eri_emitter import canonical_classes
     classes = canonical_classes(2)
     try:
+        eri.set_class_fp32(True)  # every class's FP32 kernel, also where the tuned default skips it
         for cls in classes:
             for v4 in range(4):
                 eri.set_class_minb(cls, v4, minb)
@@ -96,6 +97,7 @@ def test_every_register_budget_vs_oracle(minb):
             assert np.abs(out.cpu().numpy() - ref).max() <= tolerance(ref)
             assert np.abs(mix.cpu().numpy() - ref).max() <= 1e-10
     finally:
+        eri.set_class_fp32(None)
         for cls in classes:
             for v4 in range(4):
                 eri.set_class_minb(cls, v4, 0)
@@ -109,6 +111,7 @@ def test_slices_mixed_tier_meets_error_bar(cap):
     b = _all_l2_orderings(81, True, kmax=6, copies=4, box=2.0)
     eng = eri.EriEngine(b)
     eri.set_slice_cap(cap)
+    eri.set_class_fp32(True)
     try:
         ref = eng.compute().clone()
         bounds = eng.quartet_bounds()
@@ -117,8 +120,40 @@ def test_slices_mixed_tier_meets_error_bar(cap):
         torch.cuda.synchronize()
     finally:
         eri.set_slice_cap(0)
+        eri.set_class_fp32(None)
     assert eng.device_status() == 0
     assert np.abs(mix.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-10
+
+
+def test_fp32_switch_per_class():
+    """With every class's FP32 kernel switched off the FP32 tier reproduces the
+    FP64 path bit for bit; switched on for one class only, only that class's
+    blocks move (within the error bar)."""
+    import torch
+    b = _all_l2_orderings(83, True, kmax=4, copies=2, box=2.0)
+    eng = eri.EriEngine(b)
+    bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+    ref = eng.compute().cpu().numpy()
+    try:
+        eri.set_class_fp32(False)
+        off = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, fp32_below=2.0, mixed_tol=1e300).cpu().numpy()
+        assert np.array_equal(off, ref)
+        eri.set_class_fp32(True, (2, 2, 2, 1))
+        # every FP32 result accepted (no error-bound rejection), so they show
+        one = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, fp32_below=2.0, mixed_tol=1e300).cpu().numpy()
+        torch.cuda.synchronize()
+    finally:
+        eri.set_class_fp32(None)
+    assert eng.device_status() == 0
+    assert np.abs(one - ref).max() <= 1e-5 * np.abs(ref).max()  # FP32-VRR rounding, nothing else
+    moved = np.nonzero(one != ref)[0]
+    assert len(moved) > 0
+    ls = b.shell_l[b.quartets]
+    sizes = basis.block_sizes(b.shell_l, b.quartets, True)
+    q_of = np.searchsorted(b.out_off, moved, side='right') - 1
+    for q in np.unique(q_of):
+        assert sorted(ls[q]) == [1, 2, 2, 2], ls[q]
+    assert np.all(moved < b.out_off[q_of] + sizes[q_of])
 
 
 @pytest.mark.parametrize('sph', [False, True])
