@@ -118,6 +118,7 @@ int intception_integral_nuclear_2idx_ab_m_cC_prim_cart_work_array_size(const int
 #define IB_ERR_CUDA 2      /* CUDA runtime error */
 #define IB_ERR_SCRATCH 3   /* a class needed more scratch than reserved */
 #define IB_ERR_NODEVICE 4  /* no CUDA device */
+#define IB_ERR_TIMEOUT 5   /* a kernel's bounded wait for its own data copies gave up */
 
 /* Status of the last call made on this thread (drop-ins included). */
 int intception_b200_last_status(void);

@@ -58,6 +58,7 @@ struct Ib2Args {
   const double* boys;
   int* status;
   int lthr;  // lane-group kernels: pairs with max(la, lb) <= lthr belong to the thread-per-pair kernels
+  int bulk_ok;  // thread-per-pair kernel: every input array 16-byte aligned (complete chunks by bulk copy)
 };
 
 __host__ __device__ __forceinline__ int ib2_ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -454,24 +455,86 @@ __device__ __forceinline__ void ib2_overlap_pair(double xa, const double* __rest
 // there, and its warps run the sorted list, so the 32 lanes of a warp execute
 // the same unrolled class code.  Pairs of the lane-group kernel and refused
 // pairs are left out of the list.
+//
+// The inputs of a complete chunk are contiguous byte ranges of the caller's
+// arrays; they are fetched by bulk copies (TMA, cp.async.bulk) into one of two
+// chunk buffers while the block evaluates the other, with completion counted
+// on an mbarrier per buffer.  The last (partial) chunk, and callers whose
+// arrays are not 16-byte aligned, take plain loads.
 #define IB2_CHUNK 512
-#define IB2_TPB 128
+#define IB2_TPB 256
+
+// One chunk's inputs; every member is a whole number of 16-byte units.
+template <int KIND>
+struct Ib2Buf {
+  double xa[IB2_CHUNK], xb[IB2_CHUNK];
+  double ca[3 * IB2_CHUNK], cb[3 * IB2_CHUNK];
+  double cc[KIND == 1 ? 3 * IB2_CHUNK : 2];
+  long long off[IB2_CHUNK];
+  int la[IB2_CHUNK], lb[IB2_CHUNK];
+};
 
 template <int KIND>
 struct Ib2Stage {
-  double xa[IB2_CHUNK], xb[IB2_CHUNK];
-  double ca[3 * IB2_CHUNK], cb[3 * IB2_CHUNK];
-  double cc[KIND == 1 ? 3 * IB2_CHUNK : 1];
-  long long off[IB2_CHUNK];
+  Ib2Buf<KIND> buf[2];
+  unsigned long long full[2];  // mbarrier of each buffer: complete when its bulk copies have landed
   short order[IB2_CHUNK];     // chunk-local pair index, sorted by class
   unsigned char cls[IB2_CHUNK];
   unsigned char swp[IB2_CHUNK];
   int count[16], start[16];
 };
 
+__device__ __forceinline__ unsigned ib2_smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Thread 0: fetch complete chunk ch into bf; the buffer's mbarrier completes
+// when every byte has arrived.  The block has finished reading bf (a block
+// barrier precedes the call); the proxy fence orders those reads before the
+// copies' writes.
 template <int KIND>
-__device__ __forceinline__ void ib2_thread_pair(const Ib2Stage<KIND>& st, int c, int j, const double* boys,
-                                                double* out) {
+__device__ __forceinline__ void ib2_issue(const Ib2Args& a, Ib2Buf<KIND>& bf, long long ch, unsigned mb) {
+  const long long p0 = ch * IB2_CHUNK;
+  const unsigned n8 = IB2_CHUNK * 8, n24 = 3 * IB2_CHUNK * 8, n4 = IB2_CHUNK * 4;
+  const unsigned bytes = 3 * n8 + 2 * n4 + 2 * n24 + (KIND == 1 ? n24 : 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+#define IB2_BULK(dst, src, nb)                                                                                  \
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"( \
+                   ib2_smem_addr(dst)),                                                                         \
+               "l"(src), "r"(nb), "r"(mb)                                                                       \
+               : "memory")
+  IB2_BULK(bf.xa, a.xa + p0, n8);
+  IB2_BULK(bf.xb, a.xb + p0, n8);
+  IB2_BULK(bf.off, a.off + p0, n8);
+  IB2_BULK(bf.la, a.la + p0, n4);
+  IB2_BULK(bf.lb, a.lb + p0, n4);
+  IB2_BULK(bf.ca, a.ca + 3 * p0, n24);
+  IB2_BULK(bf.cb, a.cb + 3 * p0, n24);
+  if (KIND == 1) IB2_BULK(bf.cc, a.cc + 3 * p0, n24);
+#undef IB2_BULK
+}
+
+// Bounded wait for phase `parity` of the mbarrier at mb: false after about
+// 0.4 s without completion (a copy that never lands), so that the block can
+// report the error and return instead of spinning on.
+__device__ __forceinline__ bool ib2_wait(unsigned mb, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(mb), "r"(parity)
+        : "memory");
+    if (done) return true;
+    __nanosleep(100);
+  }
+  return false;
+}
+
+template <int KIND>
+__device__ __forceinline__ void ib2_thread_pair(const Ib2Buf<KIND>& st, const unsigned char* swp, int c, int j,
+                                                const double* boys, double* out) {
   if (KIND == 0) {
     const double* pa = st.ca + 3 * j;
     const double* pb = st.cb + 3 * j;
@@ -489,7 +552,7 @@ __device__ __forceinline__ void ib2_thread_pair(const Ib2Stage<KIND>& st, int c,
       default: ib2_overlap_pair<2, 2>(xa, pa, xb, pb, o); break;
     }
   } else {
-    const bool swap = st.swp[j];
+    const bool swap = swp[j];
     const double* pa = swap ? st.cb + 3 * j : st.ca + 3 * j;
     const double* pb = swap ? st.ca + 3 * j : st.cb + 3 * j;
     const double xa = swap ? st.xb[j] : st.xa[j], xb = swap ? st.xa[j] : st.xb[j];
@@ -511,31 +574,62 @@ __device__ __forceinline__ void ib2_thread_pair(const Ib2Stage<KIND>& st, int c,
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(IB2_TPB, 4) ib2_thread_kernel(const Ib2Args a) {
+__global__ void __launch_bounds__(IB2_TPB, 2) ib2_thread_kernel(const Ib2Args a) {
   constexpr int kClasses = KIND == 0 ? (IB2_LT + 1) * (IB2_LT + 1) : (IB2_LT + 1) * (IB2_LT + 2) / 2;
   extern __shared__ __align__(16) unsigned char ib2_raw[];
   Ib2Stage<KIND>& st = *reinterpret_cast<Ib2Stage<KIND>*>(ib2_raw);
   const long long nchunk = ((long long)a.n + IB2_CHUNK - 1) / IB2_CHUNK;
-  for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+  const long long nfull = a.bulk_ok ? (long long)a.n / IB2_CHUNK : 0;  // chunks fetched by bulk copies
+  const unsigned mb0 = ib2_smem_addr(&st.full[0]), mb1 = ib2_smem_addr(&st.full[1]);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if ((long long)blockIdx.x < nfull) ib2_issue<KIND>(a, st.buf[0], blockIdx.x, mb0);
+  }
+  __syncthreads();
+  int k = 0;
+  for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x, ++k) {
+    const int b = k & 1;
+    Ib2Buf<KIND>& bf = st.buf[b];
+    const unsigned mb_this = b ? mb1 : mb0, mb_next = b ? mb0 : mb1;
+    const long long nxt = ch + gridDim.x;
+    // prefetch the next chunk into the other buffer (read by the previous
+    // iteration, which ended with a block barrier)
+    if (threadIdx.x == 0 && nxt < nfull) ib2_issue<KIND>(a, st.buf[b ^ 1], nxt, mb_next);
     const int p0 = (int)(ch * IB2_CHUNK);
     const int np = min(IB2_CHUNK, a.n - p0);
+    if (ch < nfull) {
+      const bool ok = ib2_wait(mb_this, (k >> 1) & 1);
+      if (__syncthreads_or(!ok)) {  // uniform: report, drain the copies still in flight, stop
+        if (threadIdx.x == 0) {
+          if (a.status) atomicExch(a.status, IB_ERR_TIMEOUT);
+          ib2_wait(mb_this, (k >> 1) & 1);
+          if (nxt < nfull) ib2_wait(mb_next, ((k + 1) >> 1) & 1);
+        }
+        return;
+      }
+    } else {
+      for (int t = threadIdx.x; t < np; t += IB2_TPB) {
+        bf.xa[t] = __ldg(a.xa + p0 + t);
+        bf.xb[t] = __ldg(a.xb + p0 + t);
+        bf.off[t] = __ldg(a.off + p0 + t);
+        bf.la[t] = __ldg(a.la + p0 + t);
+        bf.lb[t] = __ldg(a.lb + p0 + t);
+      }
+      for (int t = threadIdx.x; t < 3 * np; t += IB2_TPB) {
+        bf.ca[t] = __ldg(a.ca + 3LL * p0 + t);
+        bf.cb[t] = __ldg(a.cb + 3LL * p0 + t);
+        if (KIND == 1) bf.cc[t] = __ldg(a.cc + 3LL * p0 + t);
+      }
+    }
     if (threadIdx.x < 16) st.count[threadIdx.x] = 0;
-    for (int t = threadIdx.x; t < np; t += IB2_TPB) {
-      st.xa[t] = __ldg(a.xa + p0 + t);
-      st.xb[t] = __ldg(a.xb + p0 + t);
-      st.off[t] = __ldg(a.off + p0 + t);
-    }
-    for (int t = threadIdx.x; t < 3 * np; t += IB2_TPB) {
-      st.ca[t] = __ldg(a.ca + 3LL * p0 + t);
-      st.cb[t] = __ldg(a.cb + 3LL * p0 + t);
-      if (KIND == 1) st.cc[t] = __ldg(a.cc + 3LL * p0 + t);
-    }
     __syncthreads();
     // class of every staged pair; per-class counts
     for (int t = threadIdx.x; t < np; t += IB2_TPB) {
-      const int la = __ldg(a.la + p0 + t), lb = __ldg(a.lb + p0 + t);
+      const int la = bf.la[t], lb = bf.lb[t];
       int c = 255;
-      if (ib2_bad(la, lb, a.lmax, st.xa[t], st.xb[t])) {
+      if (ib2_bad(la, lb, a.lmax, bf.xa[t], bf.xb[t])) {
         if (a.status) atomicExch(a.status, IB_ERR_ARG);
       } else if (KIND == 0) {
         if (la <= IB2_LT && lb <= IB2_LT) c = la * (IB2_LT + 1) + lb;
@@ -566,9 +660,9 @@ __global__ void __launch_bounds__(IB2_TPB, 4) ib2_thread_kernel(const Ib2Args a)
     const int total = st.start[kClasses];
     for (int i = threadIdx.x; i < total; i += IB2_TPB) {
       const int j = st.order[i];
-      ib2_thread_pair<KIND>(st, st.cls[j], j, a.boys, a.out);
+      ib2_thread_pair<KIND>(bf, st.swp, st.cls[j], j, a.boys, a.out);
     }
-    __syncthreads();  // the stage is reused by the next chunk
+    __syncthreads();  // this buffer and the sort arrays are reused
   }
 }
 
@@ -681,16 +775,21 @@ int grid_for(K kernel, size_t smem, int n, int groups, int nsm) {
   return (int)std::max(1LL, std::min<long long>(need, (long long)per_sm * nsm));
 }
 
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 int launch(int kind, const Ib2Args& a0, int nsm, cudaStream_t s) {
   // every pair passes the thread-per-pair kernel (which also flags invalid
   // pairs); pairs with max(la, lb) > IB2_LT then take the lane-group kernel
   {
+    Ib2Args at = a0;
+    at.bulk_ok = aligned16(a0.xa) && aligned16(a0.xb) && aligned16(a0.ca) && aligned16(a0.cb) &&
+                 aligned16(a0.off) && aligned16(a0.la) && aligned16(a0.lb) && (kind == 0 || aligned16(a0.cc));
     const long long chunks = ((long long)a0.n + IB2_CHUNK - 1) / IB2_CHUNK;
-    const int grid = (int)std::max(1LL, std::min<long long>(chunks, 4LL * nsm));
+    const int grid = (int)std::max(1LL, std::min<long long>(chunks, 2LL * nsm));
     if (kind == 0)
-      ib2_thread_kernel<0><<<grid, IB2_TPB, sizeof(Ib2Stage<0>), s>>>(a0);
+      ib2_thread_kernel<0><<<grid, IB2_TPB, sizeof(Ib2Stage<0>), s>>>(at);
     else
-      ib2_thread_kernel<1><<<grid, IB2_TPB, sizeof(Ib2Stage<1>), s>>>(a0);
+      ib2_thread_kernel<1><<<grid, IB2_TPB, sizeof(Ib2Stage<1>), s>>>(at);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return IB_ERR_CUDA;
   }

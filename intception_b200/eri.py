@@ -27,7 +27,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, 'libintception_b200.so')
 HEADER = os.path.join(os.path.dirname(PKG), 'include', 'intception_b200.h')
 
-IB_OK, IB_ERR_ARG, IB_ERR_CUDA, IB_ERR_SCRATCH, IB_ERR_NODEVICE = 0, 1, 2, 3, 4
+IB_OK, IB_ERR_ARG, IB_ERR_CUDA, IB_ERR_SCRATCH, IB_ERR_NODEVICE, IB_ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
 PREC_FP64, PREC_MIXED = 0, 1
 
 _dp = C.POINTER(C.c_double)

@@ -230,3 +230,29 @@ def test_large_batch_symmetry_and_translation(kind):
         assert np.abs(bp - bq.T).max() <= 1e-12 * scale
     scale = np.maximum(1.0, np.abs(g[0]))
     assert np.max(np.abs(g[2] - g[0]) / scale) <= 1e-9  # shifted centres round differently
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('kind', [0, 1])
+def test_batch_bulk_copied_chunks_vs_oracle(kind):
+    """Five complete 512-pair chunks (their inputs fetched by bulk copies into
+    alternating shared-memory buffers) and a partial one (plain loads), against
+    the C restatement; then the same pairs with one input array 8 bytes off a
+    16-byte boundary, which sends every chunk through plain loads."""
+    import torch
+    from intception_b200 import twoidx
+    from oracle import loader
+    pairs = twoidx.make_pairs(5 * 512 + 77, lmax=2, seed=12)
+    pairs['off'], pairs['size'] = twoidx.block_offsets(pairs['la'], pairs['lb'])
+    ref = loader.twoidx_batch(kind, pairs)
+    batch = twoidx.TwoIndexBatch(pairs)
+    got = batch.compute(kind).cpu().numpy()
+    assert batch.device_status() == 0
+    _assert_blocks(got, ref, pairs, 1e-12)
+    shifted = torch.empty(batch.n + 1, dtype=torch.float64, device=batch.xa.device)
+    shifted[1:] = batch.xa
+    batch.xa = shifted[1:]
+    assert batch.xa.data_ptr() % 16 == 8
+    got2 = batch.compute(kind).cpu().numpy()
+    assert batch.device_status() == 0
+    assert np.array_equal(got, got2)
