@@ -47,6 +47,7 @@ struct IbLaunch {
   int recheck;             // FP64 kernels: evaluate only flagged items
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
   int max_slices;          // class kernels: cap on lane groups sharing one quartet (0: lane groups per block)
+  int slice_boost;         // class kernels: choose slices as if the grid had this many times its lane groups (>= 1)
 };
 
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
@@ -71,12 +72,13 @@ __device__ __forceinline__ unsigned ib_pin(unsigned x) {
 __device__ __forceinline__ void ib_group_bar(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
 
 // Slices per quartet of a class kernel: the largest power of two W <= gpb
-// (and <= cap when cap > 0) with n * W <= the grid's lane groups, so that a
-// class with fewer quartets than lane groups spreads each quartet's primitive
-// quartets over W groups.  Uniform over the grid (n, gridDim, cap are).
-__device__ __forceinline__ int ib_slices(int n, int gpb, int cap) {
+// (and <= cap when cap > 0) with n * W <= boost x the grid's lane groups, so
+// that a class with fewer quartets than lane groups spreads each quartet's
+// primitive quartets over W groups.  Uniform over the grid (n, gridDim, cap,
+// boost are).
+__device__ __forceinline__ int ib_slices(int n, int gpb, int cap, int boost = 1) {
   const int wmax = cap > 0 ? min(cap, gpb) : gpb;
-  const long long groups = (long long)gridDim.x * gpb;
+  const long long groups = (long long)gridDim.x * gpb * max(boost, 1);
   int w = 1;
   while (2 * w <= wmax && (long long)n * (2 * w) <= groups) w *= 2;
   return w;
@@ -85,8 +87,8 @@ __device__ __forceinline__ int ib_slices(int n, int gpb, int cap) {
 // Slices for kernels with three lane groups per warp: 3 (one warp per
 // quartet) when the class's quartets fill at most a third of the grid's groups
 // and the cap allows it, else 1.
-__device__ __forceinline__ int ib_slices_in_threes(int n, int gpb, int cap) {
-  const long long groups = (long long)gridDim.x * gpb;
+__device__ __forceinline__ int ib_slices_in_threes(int n, int gpb, int cap, int boost = 1) {
+  const long long groups = (long long)gridDim.x * gpb * max(boost, 1);
   return ((cap == 0 || cap >= 3) && (long long)n * 3 <= groups) ? 3 : 1;
 }
 

@@ -108,6 +108,12 @@ struct Context {
   cudaStream_t stream = nullptr;
   int nside = 40;  // INTCEPTION_B200_STREAMS, 1..64: enough for every class kernel to run concurrently
   int slice_cap[IB_NCLASS] = {};  // per class: cap on lane groups per quartet (0: no cap; INTCEPTION_B200_MAX_SLICES)
+  // INTCEPTION_B200_SLICE_BOOST: slices chosen as if the grid had this many
+  // times its lane groups.  The class kernels of a batch run concurrently and
+  // their quartets differ widely in length; measured on the l <= 2 workload,
+  // 4 shortens the last, thinly occupied waves (screened step -17 %, full
+  // FP64 step -5 %) and 8 is slower again.
+  int slice_boost = 4;
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
@@ -388,6 +394,7 @@ int get_context(Context** out) {
       for (int v = 0; v < 4; ++v) c->minb_idx[cid][v] = std::min(std::max(ib_tuned_minb[cid][v], 0), IB_NMINB - 1);
       c->slice_cap[cid] = ib_tuned_slice_cap[cid];
     }
+    if (const char* env = std::getenv("INTCEPTION_B200_SLICE_BOOST")) c->slice_boost = std::max(1, std::atoi(env));
     if (const char* env = std::getenv("INTCEPTION_B200_MAX_SLICES"))
       for (int cid = 0; cid < IB_NCLASS; ++cid) c->slice_cap[cid] = std::max(0, std::atoi(env));
     IB_CUDA(c->kind.ensure(IB_NCLASS * sizeof(int)));
@@ -405,6 +412,7 @@ IbLaunch base_launch(Context* c) {
   a.boys_tab = c->boys_tab.as<double>();
   a.sph = c->sph.as<double>();
   a.status = c->status.as<int>();
+  a.slice_boost = c->slice_boost;
   return a;
 }
 

@@ -530,9 +530,9 @@ class GroupEmitter:
         src.append('  constexpr int GPB = %s;  // lane groups per block' % gpb)
         src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (self.cid, self.cid))
         if self.packed:
-            src.append('  const int W = ib_slices_in_threes(end - beg, GPB, a.max_slices);')
+            src.append('  const int W = ib_slices_in_threes(end - beg, GPB, a.max_slices, a.slice_boost);')
         else:
-            src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices);')
+            src.append('  const int W = ib_slices(end - beg, GPB, a.max_slices, a.slice_boost);')
         src.append('  const int SPB = GPB / W;  // quartets in flight per block')
         src.append('  if (beg + (int)blockIdx.x * SPB >= end) return;  // block-uniform')
         if self.wide:
