@@ -48,6 +48,7 @@ struct IbLaunch {
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
   int max_slices;          // class kernels: cap on lane groups sharing one quartet (0: lane groups per block)
   int slice_boost;         // class kernels: choose slices as if the grid had this many times its lane groups (>= 1)
+  int* counter;            // class kernels: next quartet of the range (zero before the launch; one per launch)
 };
 
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
@@ -110,6 +111,24 @@ __device__ __forceinline__ void ib_sg_sync(int SG, int sg, unsigned mask) {
 // SM; 1 = no register cap).  The autotuner picks mi per class and variant.
 #define IB_NMINB 4
 __host__ __device__ inline constexpr int ib_minb_value(int mi) { return mi == 0 ? 1 : mi + 2; }  // 1, 3, 4, 5
+
+// The next quartet for the sg-th quartet slot of the block (SG lanes, r = this
+// lane's rank, lane0 = the warp lane of rank 0 when SG <= 32): one atomic per
+// quartet, broadcast to the slot, so that slots that finish early take the
+// remaining quartets (the range is sorted longest first).  slot: an int of
+// shared memory owned by the quartet slot (used when it spans warps).
+__device__ __forceinline__ int ib_grab(int* ctr, int beg, int r, int SG, int sg, unsigned sgmask, int lane0,
+                                       int* slot) {
+  if (SG <= 32) {
+    int v = 0;
+    if (r == 0) v = atomicAdd(ctr, 1);
+    return beg + __shfl_sync(sgmask, v, lane0);
+  }
+  ib_sg_sync(SG, sg, sgmask);  // every lane has read the previous value
+  if (r == 0) *slot = atomicAdd(ctr, 1);
+  ib_sg_sync(SG, sg, sgmask);
+  return beg + *slot;
+}
 
 typedef void (*IbLaunchFn)(int variant, int grid, cudaStream_t s, const IbLaunch& a);
 typedef int (*IbOccFn)(int variant);

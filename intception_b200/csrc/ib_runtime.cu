@@ -47,6 +47,7 @@ constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 cop
 constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
 constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
 constexpr int kNRanges = 4 * IB_NCLASS + 4;
+constexpr int kNCounters = 3 * IB_NCLASS;      // quartet counters: FP64 pass, FP32 pass, FP64 recheck pass
 constexpr int kKeyBits = 24;                    // skip(1) generic(1) fp32(1) class(9) Kab(6) Kcd(6)
 constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
 
@@ -117,6 +118,7 @@ struct Context {
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
+  DevBuf counters;  // per class kernel launch of a batch: the next quartet (FP64, FP32, FP64 recheck passes)
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;                                             // FP32 rejections of the last mixed batch
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
@@ -382,6 +384,7 @@ int get_context(Context** out) {
     IB_CUDA(c->sph.ensure(sph.size() * sizeof(double)));
     IB_CUDA(cudaMemcpy(c->sph.p, sph.data(), sph.size() * sizeof(double), cudaMemcpyHostToDevice));
     IB_CUDA(c->ranges.ensure(kNRanges * sizeof(int)));
+    IB_CUDA(c->counters.ensure((kNCounters + 1) * sizeof(int)));  // + the drop-in's own
     IB_CUDA(c->status.ensure(sizeof(int)));
     IB_CUDA(cudaMemset(c->status.p, 0, sizeof(int)));
     ib_register_emitted_classes(c->table);
@@ -466,6 +469,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       const int grid = c->nsm * c->occ[cid][vt];
       cudaStream_t ss = c->side[k % c->nside];
       ap.max_slices = c->slice_cap[cid];
+      ap.counter = c->counters.as<int>() + prec * IB_NCLASS + cid;
       c->table[cid].launch(vt, grid, ss, ap);
       ++k;
       if (prec == 1) {
@@ -473,6 +477,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
         // kernel rejected (same stream, so it sees their flags)
         IbLaunch ar = ap;
         ar.recheck = 1;
+        ar.counter = c->counters.as<int>() + 2 * IB_NCLASS + cid;
         const int v64 = sph ? 1 : 0;
         const int vt64 = v64 + 4 * c->minb_idx[cid][v64];
         c->table[cid].launch(vt64, c->nsm * c->occ[cid][vt64], ss, ar);
@@ -645,6 +650,8 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
   if (emitted) {
     const int vt = 4 * c->minb_idx[cid][0];
     const int grid = std::max(1, std::min(c->nsm * c->occ[cid][vt], (nblk + IB_BLOCK - 1) / IB_BLOCK));
+    a.counter = c->counters.as<int>() + kNCounters;  // never used by a batch that may still run
+    IB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
     c->table[cid].launch(vt, grid, s, a);
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
@@ -818,6 +825,7 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
                                           c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
   IB_CUDA(c->cub_tmp.ensure(tmp_bytes));
   IB_CUDA(cudaMemsetAsync(c->ranges.p, 0, kNRanges * sizeof(int), s));
+  IB_CUDA(cudaMemsetAsync(c->counters.p, 0, kNCounters * sizeof(int), s));
   IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
   const int grid = std::min((nq + 255) / 256, c->nsm * 16);
   const bool use_bounds = bounds != nullptr && (precision == IB_PREC_MIXED || skip_below > 0.0);

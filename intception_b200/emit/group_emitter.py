@@ -558,7 +558,7 @@ class GroupEmitter:
         nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
         per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
         self.list_off = per_group
-        per_group += 17  # live-pair lists of the quartet's current tile (2 x 64 bytes) and their counts
+        per_group += 18  # live-pair lists of the quartet's current tile (2 x 64 bytes), their counts, the grab slot
         per_group += 1  # this slice's FP32 error bound, summed over the slices
         src.append('  double* __restrict__ sb = ib_smem + gid * %d;' % per_group)
         src.append('  double* __restrict__ sb0 = ib_smem + sg * W * %d;  // slice 0'
@@ -588,7 +588,10 @@ class GroupEmitter:
         src.append('  const double lcx = (double)(lmisc & 15), lcy = (double)((lmisc >> 4) & 15), '
                    'lcz = (double)((lmisc >> 8) & 15);')
         src.append('  (void)src0; (void)src1; (void)src2; (void)lsteps; (void)lcx; (void)lcy; (void)lcz;')
-        src.append('  for (int p = beg + (int)blockIdx.x * SPB + sg; p < end; p += (int)gridDim.x * SPB) {')
+        # quartets handed out one at a time (ib_grab) instead of a fixed stride
+        lane0 = '0' if self.wide else 'lane - r'
+        grab = 'ib_grab(a.counter, beg, r, SG, sg, sgmask, %s, lcnt + 2)' % lane0
+        src.append('  for (int p = %s; p < end; p = %s) {' % (grab, grab))
         src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // uniform over the quartet\'s lanes')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
