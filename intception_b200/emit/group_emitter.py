@@ -614,6 +614,11 @@ class GroupEmitter:
         src.append('    const int kab = g.k[0] * kb_, kcd = g.k[2] * kd_;')
         src.append('    // exact small-integer quotients: (x + 0.5) / k is >= 1/128 away from an integer')
         src.append('    const float rkb = 1.0f / (float)kb_, rkd = 1.0f / (float)kd_;')
+        # FP32 tier: growth of an accumulator's error through the HRRs and
+        # transforms; a quartet whose error bound already exceeds the
+        # tolerance stops its FP32 primitive loop (the final check rejects it)
+        src.append('    const double famp = sizeof(R) == 4 ? %s : 0.0;' % self.amp_expr())
+        src.append('    (void)famp;')
         src.append('    for (int ab0 = 0; ab0 < kab; ab0 += 64)')
         src.append('    for (int cd0 = 0; cd0 < kcd; cd0 += 64) {')
         src.append('      if (r < 32) {')
@@ -648,7 +653,10 @@ class GroupEmitter:
             src.append('        IbPrimQuartet<R> pq;')
             src.append('        double F[%d];' % (L + 1))
             src.append('        if (!ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq)) continue;' % L)
-            src.append('        if (sizeof(R) == 4) est += %s;' % self.err_expr())
+            src.append('        if (sizeof(R) == 4) {')
+            src.append('          est += %s;' % self.err_expr())
+            src.append('          if (est * famp > a.mixed_tol) break;  // this slice alone already exceeds it')
+            src.append('        }')
             for f, nm in zip(fields, names):
                 src.append('        const R %s = pq.%s;' % (nm, f))
             for m in range(L + 1):
@@ -681,6 +689,27 @@ class GroupEmitter:
             src.append('          }')
             src.append('        }')
             src.append('        %s;' % sync)
+            # the group's bound so far (its lanes' partial sums): past the
+            # tolerance, the rest of this quartet's FP32 work is skipped
+            src.append('        if (sizeof(R) == 4) {')
+            src.append('          double eg = est;')
+            if self.packed:
+                src.append('          sb[j] = est;')
+                src.append('          __syncwarp(gmask);')
+                src.append('          eg = 0.0;')
+                src.append('          for (int v = 0; v < %d; ++v) eg += sb[v];' % self.G)
+                src.append('          __syncwarp(gmask);')
+            elif self.wide:
+                src.append('          for (int o = 16; o > 0; o >>= 1) eg += __shfl_xor_sync(0xffffffffu, eg, o);')
+                src.append('          if ((j & 31) == 0) sb[j >> 5] = eg;')
+                src.append('          ib_group_bar(gid);')
+                src.append('          eg = sb[0] + sb[1];')
+                src.append('          ib_group_bar(gid);')
+            else:
+                src.append('          for (int o = %d; o > 0; o >>= 1) eg += __shfl_xor_sync(gmask, eg, o, %d);'
+                           % (self.G // 2, self.G))
+            src.append('          if (eg * famp > a.mixed_tol) break;  // uniform over the group')
+            src.append('        }')
             src.append('        const int nu = min(%d, npl - q0);' % self.G)
             src.append('        for (int u = 0; u < nu; ++u) {')
             src.append('          if (!pz[u]) continue;  // group-uniform: exact-zero primitive quartet')
@@ -757,7 +786,7 @@ class GroupEmitter:
         src.append('        est = 0.0;')
         src.append('        for (int v = 0; v < W; ++v) est += sb0[v * %d + %d];' % (pg, pg - 1))
         src.append('      }')
-        src.append('      if (est * %s > a.mixed_tol) {' % self.amp_expr())
+        src.append('      if (est * famp > a.mixed_tol) {')
         src.append('        if (r == 0) a.flags[p] = 1;')
         src.append('        continue;  // uniform over the quartet: the FP64 pass recomputes and stores it')
         src.append('      }')
