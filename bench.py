@@ -416,15 +416,21 @@ def run_only(args, eng, out):
 
 def main():
     args = parse()
+    if args.impl == 'reference':
+        # host cores only: no process group; rank 0 runs the reference, the
+        # other ranks of a multi-GPU launch exit at once
+        rank, world = int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1'))
+        if args.workload != 'eri':
+            run_twoidx(args, rank, world, 0)
+        else:
+            run_reference_arm(args, rank, world)
+        return
     rank, world, local = dist_init(args.gpus)
     if args.workload != 'eri':
         run_twoidx(args, rank, world, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
-        return
-    if args.impl == 'reference':
-        run_reference_arm(args, rank, world)
         return
     import torch
     from intception_b200 import basis, eri
