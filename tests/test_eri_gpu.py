@@ -72,6 +72,36 @@ def test_slices_every_l2_class_vs_oracle(cap, sph):
     assert np.abs(out - ref).max() <= tolerance(ref)
 
 
+@pytest.mark.parametrize('sph', [False, True])
+def test_long_contractions_span_pair_tiles(sph):
+    """K up to 20 per shell (up to 400 primitive pairs a side): the live-pair
+    lists run over several 64 x 64 tiles of a quartet; every l <= 2 ordering,
+    FP64, against the oracle; slices forced both ways."""
+    rng = np.random.default_rng(97 + sph)
+    quartets, ls = [], []
+    for la in range(3):
+        for lb in range(3):
+            for lc in range(3):
+                for ld in range(3):
+                    base = len(ls)
+                    ls += [la, lb, lc, ld]
+                    quartets.append([base, base + 1, base + 2, base + 3])
+    ks = rng.choice(np.array([1, 7, 9, 13, 20], np.int32), len(ls))
+    l_, k_, p_, xyz, e, c = basis.make_shells(rng, np.array(ls, np.int32), ks, 0.1, 30.0, 2.5)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    b = basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
+    assert (k_[q[:, 0]] * k_[q[:, 1]] > 64).any() and (k_[q[:, 2]] * k_[q[:, 3]] > 64).any()
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    for cap in (1, 0):
+        eri.set_slice_cap(cap)
+        try:
+            out = run_batch(b)
+        finally:
+            eri.set_slice_cap(0)
+        assert np.abs(out - ref).max() <= tolerance(ref)
+
+
 @pytest.mark.parametrize('minb', [1, 3, 4, 5])
 def test_every_register_budget_vs_oracle(minb):
     """Each register budget the class kernels are compiled with (minimum
