@@ -366,8 +366,12 @@ class HostPipeline:
             stream.wait_event(slot['ev'][name])
 
     def submit(self, h, out_host, precision=PREC_FP64, skip_below=0.0, fp32_below=0.0, mixed_tol=5e-11, lmax=None):
-        """Queue one batch; out_host (pinned float64, the batch's output size)
-        receives its blocks."""
+        """Queue one batch; out_host (pinned float64) receives its blocks.  As
+        for the out argument of intception_b200_eri_batch, out_host must hold
+        every block of the batch: out_off[q] + na nb nc nd <= out_host.numel()
+        for every quartet q (the device buffer is sized from it and the
+        kernels write each block at its offset).  lmax: the largest shell l
+        (computed from shell_l when None)."""
         torch = self.torch
         slot = self.slots[self.k % self.depth]
         self.k += 1
