@@ -406,14 +406,17 @@ class Emitter:
 
 
 def emitted_classes():
-    """Canonical classes with an unrolled kernel: every class with l <= 2, and
-    the classes with one f shell and the rest <= d (FP64 only), which the
-    nuclear-gradient batches of an l <= 2 basis reach."""
+    """Canonical classes with an unrolled kernel: every class with l <= 2
+    (FP64 and FP32-VRR variants), and every class with an f shell and the rest
+    <= f whose smaller side fits a 64-lane group (FP64 only) -- all l <= 3
+    classes but (ff|ff), which the generic kernel serves (the nuclear-gradient
+    batches of an l <= 2 basis reach the one-f classes; an f basis reaches
+    them all)."""
+    from .group_emitter import orientation
     out = [(c, True) for c in canonical_classes(LMAX_EMIT)]
-    pairs = [(a, b) for a in range(3) for b in range(a + 1)]
-    for lb in range(3):
-        for (lc, ld) in pairs:
-            out.append(((3, lb, lc, ld), False))
+    for c in canonical_classes(3):
+        if max(c) == 3 and orientation(*c) is not None:
+            out.append((c, False))
     out.sort(key=lambda x: class_id(*x[0]))
     return out
 
