@@ -54,8 +54,8 @@ struct IbLaunch {
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
 // path, 5 bits per step (direction 0..2, or 3 for an identity step that pads
 // shorter paths at the front; then the exponent before the step); misc: the
-// lane's Cartesian component (4 bits per axis) and the lanes owning
-// component - 1x, - 1y, - 1z inside the group (6 bits each).
+// lane's Cartesian component (3 bits per axis) and the lanes owning
+// component - 1x, - 1y, - 1z inside the group (7 bits each).
 struct IbLaneCode {
   unsigned steps;
   unsigned misc;
@@ -69,8 +69,11 @@ __device__ __forceinline__ unsigned ib_pin(unsigned x) {
   return y;
 }
 
-// Barrier over the 64 threads of two-warp group g of the block (named barrier g+1).
-__device__ __forceinline__ void ib_group_bar(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
+// Barrier over the n threads (64 or 128) of multi-warp lane group g of the
+// block (named barrier g+1).
+__device__ __forceinline__ void ib_group_bar(int g, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(n) : "memory");
+}
 
 // Slices per quartet of a class kernel: the largest power of two W <= gpb
 // (and <= cap when cap > 0) with n * W <= boost x the grid's lane groups, so

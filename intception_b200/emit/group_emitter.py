@@ -52,9 +52,9 @@ def cidx(c):
 
 def orientation(la, lb, lc, ld):
     """'bra' if the lanes own bra components, 'ket' otherwise; None when
-    neither side fits a 64-lane (two-warp) group."""
+    neither side fits a 128-lane (four-warp, whole-block) group."""
     ne, nf = ncum(la + lb), ncum(lc + ld)
-    if min(ne, nf) > 64:
+    if min(ne, nf) > 128:
         return None
     return 'bra' if ne <= nf else 'ket'
 
@@ -125,8 +125,8 @@ class GroupEmitter:
         self.packed = PACK_TEN and self.NL == 10
         if self.packed:
             self.G = 10
-        # G = 64: two warps per quartet; transfer operands go through shared
-        # memory, one named barrier per recurrence level
+        # G = 64 or 128: two or four warps per quartet; transfer operands go
+        # through shared memory, one named barrier per recurrence level
         self.wide = self.G > 32
         self.QPW = max(1, 32 // self.G)
         self.tag = '%d%d%d%d' % (la, lb, lc, ld)
@@ -197,7 +197,7 @@ class GroupEmitter:
             if self.wide:
                 lvl = sum(cm)
                 slot = self.slot_index(cm, m + 1)
-                expr += ' + tf%s * xb%d[%d * 64 + src%s]' % (d, lvl % 2, slot, 'xyz'.index(d))
+                expr += ' + tf%s * xb%d[%d * %d + src%s]' % (d, lvl % 2, slot, self.G, 'xyz'.index(d))
             else:
                 expr += ' + tf%s * %s' % (d, self._shfl(a1, i, sum(cm)))
             fl += 2
@@ -250,7 +250,7 @@ class GroupEmitter:
         # level 0: base values
         for mm in range(1, self.C_hi + 1):
             if ((0, 0, 0), mm) in self.nodes:
-                out.append('        xb0[%d * 64 + j] = b%d;' % (self.slot_index(ZERO, mm), mm))
+                out.append('        xb0[%d * %d + j] = b%d;' % (self.slot_index(ZERO, mm), self.G, mm))
         out.append('        ib_group_bar(gid);')
         t_index = {c: t for t, c in enumerate(targets)}
         for k in range(1, self.C_hi + 1):
@@ -263,7 +263,7 @@ class GroupEmitter:
                 for c in comps(k):
                     for mm in range(1, self.C_hi - k + 1):
                         if (c, mm) in self.nodes:
-                            out.append('        xb%d[%d * 64 + j] = %s;' % (k % 2, self.slot_index(c, mm),
+                            out.append('        xb%d[%d * %d + j] = %s;' % (k % 2, self.slot_index(c, mm), self.G,
                                                                          self.nodes[(c, mm)]))
                 out.append('        ib_group_bar(gid);')
         defs = ['        const R %s = (R)%d * %s;' % (name, k, base) for (base, k), name in sorted(self.mult.items())]
@@ -504,7 +504,7 @@ class GroupEmitter:
         # steps to S_hi (5 bits each: direction 0..2 or 3 = identity, then the
         # exponent before the step), and the component with the lanes owning
         # s - 1x, s - 1y, s - 1z (4 + 4 + 4 + 6 + 6 + 6 bits)
-        assert self.S_hi <= 6 and self.G <= 64
+        assert self.S_hi <= 6 and self.G <= 128
         src.append('__constant__ IbLaneCode ib_lane_%s[%d] = {' % (t, self.G))
         for (c, dirs, nbs, sr) in rows:
             pad = self.S_hi - len(dirs)
@@ -513,8 +513,8 @@ class GroupEmitter:
             for k, (d, nb) in enumerate(steps):
                 assert nb < 8
                 code |= (d | (nb << 2)) << (5 * k)
-            assert max(c) < 16
-            misc = c[0] | (c[1] << 4) | (c[2] << 8) | (sr[0] << 12) | (sr[1] << 18) | (sr[2] << 24)
+            assert max(c) < 8 and max(sr) < 128
+            misc = c[0] | (c[1] << 3) | (c[2] << 6) | (sr[0] << 9) | (sr[1] << 16) | (sr[2] << 23)
             src.append('  {0x%08xu, 0x%08xu},' % (code, misc))
         src.append('};')
         src.append('template <typename R, bool SPH, int MINB>')
@@ -526,7 +526,7 @@ class GroupEmitter:
         # before the HRR.  W grows while the class's quartets cannot fill the
         # grid's groups, so a class with few (or very long) quartets still uses
         # the whole device.  W = 1 is the plain one-group-per-quartet kernel.
-        gpb = 'IB_BLOCK / 64' if self.wide else '(IB_BLOCK / 32) * %d' % self.QPW
+        gpb = 'IB_BLOCK / %d' % self.G if self.wide else '(IB_BLOCK / 32) * %d' % self.QPW
         src.append('  constexpr int GPB = %s;  // lane groups per block' % gpb)
         src.append('  const int beg = a.ranges[2 * %d], end = a.ranges[2 * %d + 1];' % (self.cid, self.cid))
         if self.packed:
@@ -536,7 +536,7 @@ class GroupEmitter:
         src.append('  const int SPB = GPB / W;  // quartets in flight per block')
         src.append('  if (beg + (int)blockIdx.x * SPB >= end) return;  // block-uniform')
         if self.wide:
-            src.append('  const int gid = threadIdx.x / 64, j = threadIdx.x % 64;')
+            src.append('  const int gid = threadIdx.x / %d, j = threadIdx.x %% %d;' % (self.G, self.G))
             src.append('  const unsigned gmask = 0xffffffffu;')
             src.append('  const unsigned sgmask = 0xffffffffu;')
         else:
@@ -556,22 +556,28 @@ class GroupEmitter:
         src.append('  const int SG = W * %d, r = w * %d + j;  // lanes per quartet, this lane among them'
                    % (self.G, self.G))
         nfield = 17 + self.L + 1 + 1  # setup fields, scaled F_0..F_L, and the live flags
-        per_group = smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (nfield * self.G if self.G > 1 else 0)
+        # the transfer buffers (xb) and the primitive setup table (ps, pz) are
+        # live only inside the primitive loop, the contracted table only after
+        # it (behind the super-group sync that closes the last tile): they
+        # share the area at the start of the group's block
+        xb_len = 2 * self.n_slots() * self.G if self.wide else 0
+        loop_len = xb_len + (nfield * self.G if self.G > 1 else 0)
+        per_group = max(smem_group, loop_len)
         self.list_off = per_group
         per_group += 18  # live-pair lists of the quartet's current tile (2 x 64 bytes), their counts, the grab slot
+        self.red_off = per_group  # partial sums of a multi-warp or packed group's FP32 bound
+        per_group += self.G if self.packed else (self.G // 32 if self.wide else 0)
         per_group += 1  # this slice's FP32 error bound, summed over the slices
         src.append('  double* __restrict__ sb = ib_smem + gid * %d;' % per_group)
         src.append('  double* __restrict__ sb0 = ib_smem + sg * W * %d;  // slice 0'
                    % per_group)
         if self.wide:
-            src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb + %d);' % smem_group)
-            src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * 64))
+            src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb);')
+            src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * self.G))
             src.append('  (void)xb1;')
         if self.G > 1:
-            src.append('  R* __restrict__ ps = reinterpret_cast<R*>(sb + %d);'
-                       % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0)))
-            src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);'
-                       % (smem_group + (2 * self.n_slots() * 64 if self.wide else 0) + (17 + self.L + 1) * self.G))
+            src.append('  R* __restrict__ ps = reinterpret_cast<R*>(sb + %d);' % xb_len)
+            src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);' % (xb_len + (17 + self.L + 1) * self.G))
         self.per_group = per_group
         src.append('  unsigned char* __restrict__ lst = reinterpret_cast<unsigned char*>(sb0 + %d);' % self.list_off)
         src.append('  int* __restrict__ lcnt = reinterpret_cast<int*>(sb0 + %d);' % (self.list_off + 16))
@@ -581,12 +587,12 @@ class GroupEmitter:
         src.append('  const unsigned lsteps = ib_pin(ib_lane_%s[j].steps), lmisc = ib_pin(ib_lane_%s[j].misc);'
                    % (t, t))
         if self.packed:
-            src.append('  const int src0 = gq * %d + ((lmisc >> 12) & 63), src1 = gq * %d + ((lmisc >> 18) & 63), '
-                       'src2 = gq * %d + ((lmisc >> 24) & 63);' % (self.G, self.G, self.G))
+            src.append('  const int src0 = gq * %d + ((lmisc >> 9) & 127), src1 = gq * %d + ((lmisc >> 16) & 127), '
+                       'src2 = gq * %d + ((lmisc >> 23) & 127);' % (self.G, self.G, self.G))
         else:
-            src.append('  const int src0 = (lmisc >> 12) & 63, src1 = (lmisc >> 18) & 63, src2 = (lmisc >> 24) & 63;')
-        src.append('  const double lcx = (double)(lmisc & 15), lcy = (double)((lmisc >> 4) & 15), '
-                   'lcz = (double)((lmisc >> 8) & 15);')
+            src.append('  const int src0 = (lmisc >> 9) & 127, src1 = (lmisc >> 16) & 127, src2 = (lmisc >> 23) & 127;')
+        src.append('  const double lcx = (double)(lmisc & 7), lcy = (double)((lmisc >> 3) & 7), '
+                   'lcz = (double)((lmisc >> 6) & 7);')
         src.append('  (void)src0; (void)src1; (void)src2; (void)lsteps; (void)lcx; (void)lcy; (void)lcz;')
         # quartets handed out one at a time (ib_grab) instead of a fixed stride
         lane0 = '0' if self.wide else 'lane - r'
@@ -694,16 +700,16 @@ class GroupEmitter:
             src.append('        if (sizeof(R) == 4) {')
             src.append('          double eg = est;')
             if self.packed:
-                src.append('          sb[j] = est;')
+                src.append('          sb[%d + j] = est;' % self.red_off)
                 src.append('          __syncwarp(gmask);')
                 src.append('          eg = 0.0;')
-                src.append('          for (int v = 0; v < %d; ++v) eg += sb[v];' % self.G)
+                src.append('          for (int v = 0; v < %d; ++v) eg += sb[%d + v];' % (self.G, self.red_off))
                 src.append('          __syncwarp(gmask);')
             elif self.wide:
                 src.append('          for (int o = 16; o > 0; o >>= 1) eg += __shfl_xor_sync(0xffffffffu, eg, o);')
-                src.append('          if ((j & 31) == 0) sb[j >> 5] = eg;')
+                src.append('          if ((j & 31) == 0) sb[%d + (j >> 5)] = eg;' % self.red_off)
                 src.append('          ib_group_bar(gid);')
-                src.append('          eg = sb[0] + sb[1];')
+                src.append('          eg = %s;' % ' + '.join('sb[%d]' % (self.red_off + w) for w in range(self.G // 32)))
                 src.append('          ib_group_bar(gid);')
             else:
                 src.append('          for (int o = %d; o > 0; o >>= 1) eg += __shfl_xor_sync(gmask, eg, o, %d);'
@@ -762,11 +768,11 @@ class GroupEmitter:
         src.append('    }')
         # FP32: sum the error bound over the group, reject the quartet if too large
         src.append('    if (sizeof(R) == 4) {')
-        if self.packed:  # not a power of two: through the group's table area, still unused
-            src.append('      sb[j] = est;')
+        if self.packed:  # not a power of two: through shared memory
+            src.append('      sb[%d + j] = est;' % self.red_off)
             src.append('      __syncwarp(gmask);')
             src.append('      est = 0.0;')
-            src.append('      for (int v = 0; v < %d; ++v) est += sb[v];' % self.G)
+            src.append('      for (int v = 0; v < %d; ++v) est += sb[%d + v];' % (self.G, self.red_off))
             src.append('      __syncwarp(gmask);')
         elif self.G > 1 and not self.wide:
             src.append('      for (int o = %d; o > 0; o >>= 1) est += __shfl_xor_sync(gmask, est, o, %d);'
@@ -774,9 +780,9 @@ class GroupEmitter:
         elif self.wide:
             src.append('      for (int o = 16; o > 0; o >>= 1) est += __shfl_xor_sync(0xffffffffu, est, o);')
             src.append('      ib_group_bar(gid);')
-            src.append('      if ((j & 31) == 0) sb[j >> 5] = est;')
+            src.append('      if ((j & 31) == 0) sb[%d + (j >> 5)] = est;' % self.red_off)
             src.append('      ib_group_bar(gid);')
-            src.append('      est = sb[0] + sb[1];')
+            src.append('      est = %s;' % ' + '.join('sb[%d]' % (self.red_off + w) for w in range(self.G // 32)))
             src.append('      ib_group_bar(gid);')
         pg = self.per_group
         src.append('      if (W > 1) {  // sum over the slices')
@@ -825,7 +831,7 @@ class GroupEmitter:
         src.append('}')
         src.append('')
         if self.wide:
-            smem_bytes = '(sizeof(double) * (IB_BLOCK / 64) * %d)' % per_group
+            smem_bytes = '(sizeof(double) * (IB_BLOCK / %d) * %d)' % (self.G, per_group)
         else:
             smem_bytes = '(sizeof(double) * (IB_BLOCK / 32) * %d * %d)' % (self.QPW, per_group)
         src.append('static size_t ib_smem_%s() { return %s; }' % (t, smem_bytes))
@@ -860,6 +866,8 @@ class GroupEmitter:
         src.append('  return n;')
         src.append('}')
         src.append('')
+        # the group barrier counts the group's G threads (named barrier gid + 1)
+        src = [ln.replace('ib_group_bar(gid)', 'ib_group_bar(gid, %d)' % self.G) for ln in src]
         stats = dict(tag=t, cid=self.cid, L=L, kind='group', G=self.G, orient=self.orient, nodes=self.nvar,
                      lane_flops=self.flops, nacc=NE * NF)
         return '\n'.join(src), stats

@@ -62,10 +62,50 @@ static void init_comp_tab(void) {
   comp_tab_ready = 1;
 }
 
+/* Off (the default): the reference's Boys function below.  On: an accurate
+ * one, for checking the recurrences apart from the reference's Boys error.
+ * The reference's 7-term Taylor steps on a 0.1 grid truncate at about 1e-13
+ * relative (2.7e-14 measured at m = 0 against 30-digit mpmath values) and its
+ * x >= 35 branch drops exp(-x) (3.8e-6 relative at m = 12, x = 35); the VRR's
+ * cancellations carry such errors into the f-shell classes' integrals at up to
+ * 1e-9 relative.  Accurate mode: below x = 50 the series
+ *   F_n(x) = exp(-x) sum_k (2x)^k / ((2n+1)(2n+3)...(2n+2k+1))
+ * (positive terms, summed until they stop changing the sum) for F_nmax, then
+ * downward recursion; from x = 50 the asymptotic F_0 and the exact upward
+ * recursion F_{m+1} = ((m+1/2) F_m - exp(-x)/2) / x. */
+static int oracle_boys_exact_mode = 0;
+void oracle_set_boys_exact(int on) { oracle_boys_exact_mode = on; }
+
+static void oracle_boys_accurate(double *f, int ifskip, int nmin, int nmax, double x) {
+  double ex = exp(-x);
+  if (x < 50.0) {
+    double term = 1.0 / (2.0 * nmax + 1.0), sum = term;
+    for (int k = 1; k < 2000; ++k) {
+      term *= 2.0 * x / (2.0 * nmax + 2.0 * k + 1.0);
+      double next = sum + term;
+      if (next == sum) break;
+      sum = next;
+    }
+    f[nmax * ifskip] = ex * sum;
+    for (int m = nmax - 1; m >= nmin; --m)
+      f[m * ifskip] = (2.0 * x * f[(m + 1) * ifskip] + ex) / (2.0 * m + 1.0);
+  } else {
+    double oox = 1.0 / x, g = 0.5 * sqrt(3.141592653589793 * oox);
+    for (int m = 0; m <= nmax; ++m) {
+      if (m >= nmin) f[m * ifskip] = g;
+      g = ((double)m + 0.5) * oox * g - 0.5 * ex * oox;
+    }
+  }
+}
+
 /* generator_boys_function.py:98-205: small x (<=15) 7-term Taylor about the
  * nearest 0.1 grid point then downward recursion; 15<x<35 F_0 Taylor then upward
  * recursion; x>=35 asymptotic F_0 and upward recursion without exp(-x). */
 void oracle_boys(double *f, int ifskip, int nmin, int nmax, double x) {
+  if (oracle_boys_exact_mode) {
+    oracle_boys_accurate(f, ifskip, nmin, nmax, x);
+    return;
+  }
   if (x <= 15.0) {
     int i = (int)round(x * 10.0);
     double dx = (double)i * 0.1 - x;

@@ -41,6 +41,8 @@ def load_oracle():
         lib = C.CDLL(_ORACLE_SO)
         lib.oracle_boys.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double]
         lib.oracle_boys.restype = None
+        lib.oracle_set_boys_exact.argtypes = [C.c_int]
+        lib.oracle_set_boys_exact.restype = None
         lib.oracle_eri_work_array_size.argtypes = [C.c_int] * 12
         lib.oracle_eri_work_array_size.restype = C.c_int
         lib.oracle_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp, _dp]
@@ -123,11 +125,17 @@ def twoidx_batch(kind, pairs, lib=None):
     return out
 
 
-def boys(nmax, x, lib=None):
+def boys(nmax, x, lib=None, exact=False):
     lib = lib or load_oracle()
     f = np.zeros(nmax + 1)
-    fn = lib.oracle_boys if hasattr(lib, 'oracle_boys') else lib.intception_boys
-    fn(_ptr(f), 1, 0, nmax, float(x))
+    if hasattr(lib, 'oracle_boys'):
+        lib.oracle_set_boys_exact(1 if exact else 0)
+        try:
+            lib.oracle_boys(_ptr(f), 1, 0, nmax, float(x))
+        finally:
+            lib.oracle_set_boys_exact(0)
+    else:
+        lib.intception_boys(_ptr(f), 1, 0, nmax, float(x))
     return f
 
 
@@ -149,14 +157,20 @@ def _batch_args(b):
     return q, sl, sk, sp, xyz, e, c, off
 
 
-def oracle_batch(b, sphT=None):
-    """Evaluate a ShellBatch with the C restatement (single thread)."""
+def oracle_batch(b, sphT=None, exact_boys=False):
+    """Evaluate a ShellBatch with the C restatement (single thread).
+    exact_boys: an accurate Boys function in place of the reference's (see
+    oracle_set_boys_exact in eri_oracle.c)."""
     lib = load_oracle()
     q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
     out = np.zeros(b.out_size)
     tab, keep = _sph_table(sphT) if b.spherical else (None, None)
-    lib.oracle_eri_batch(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz),
-                         _ptr(e), _ptr(c), tab, _ptr(off, _lp), _ptr(out))
+    lib.oracle_set_boys_exact(1 if exact_boys else 0)
+    try:
+        lib.oracle_eri_batch(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz),
+                             _ptr(e), _ptr(c), tab, _ptr(off, _lp), _ptr(out))
+    finally:
+        lib.oracle_set_boys_exact(0)
     return out
 
 

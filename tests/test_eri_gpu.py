@@ -210,6 +210,47 @@ def test_every_l2_class_vs_oracle(sph):
     assert np.abs(out - ref).max() <= tolerance(ref)
 
 
+# (exponent range, box edge in bohr, max abs error allowed).  The last range is
+# a stress case: normalised f shells with exponents down to 0.1 three bohr
+# apart, where the contracted [e0|f0] intermediates reach 2e3 for blocks of
+# 1e-2.  Both horizontal recurrences then cancel six digits, and the FP64
+# result carries up to 5.5e-12 of rounding error (a 40-digit evaluation of the
+# worst elements confirms it is rounding).  The reference builds the ket by
+# vertical recurrences on c and d, with no ket HRR, and stays within 2e-14
+# there.
+F_DISTS = [(0.3, 5.0, 3.0, 1e-12), (0.3, 5.0, 6.0, 1e-12), (0.1, 40.0, 1.0, 1e-12), (0.5, 20.0, 4.0, 1e-12),
+           (0.1, 40.0, 3.0, 2e-11)]
+
+
+@pytest.mark.parametrize('sph', [False, True])
+@pytest.mark.parametrize('dist', range(len(F_DISTS)))
+def test_every_f_class_vs_oracle(dist, sph):
+    """All 175 (la,lb,lc,ld) orderings with l <= 3 and at least one f shell,
+    (ff|ff) included, two copies each with fresh shells and K 1..3."""
+    lo, hi, box, tol = F_DISTS[dist]
+    rng = np.random.default_rng(57 + sph + 10 * dist)
+    quartets = []
+    ls = []
+    for _ in range(2):
+        for la in range(4):
+            for lb in range(4):
+                for lc in range(4):
+                    for ld in range(4):
+                        if max(la, lb, lc, ld) < 3:
+                            continue
+                        base = len(ls)
+                        ls += [la, lb, lc, ld]
+                        quartets.append([base, base + 1, base + 2, base + 3])
+    ks = rng.integers(1, 4, len(ls)).astype(np.int32)
+    l_, k_, p_, xyz, e, c = basis.make_shells(rng, np.array(ls, np.int32), ks, lo, hi, box)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    b = basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    out = run_batch(b)
+    assert np.abs(out - ref).max() <= tol * max(1.0, float(np.abs(ref).max()))
+
+
 def test_boys_dropin_vs_reference():
     z = np.load(GOLDEN + '/boys.npz')
     nmax = int(z['nmax'])

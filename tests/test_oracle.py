@@ -50,7 +50,26 @@ def test_oracle_boys_accuracy():
         assert np.abs(f - ex).max() < 2e-14
 
 
-@pytest.mark.parametrize('ls', [(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 1, 1), (2, 1, 0, 1), (0, 2, 2, 1), (2, 2, 1, 1)])
+def test_oracle_accurate_boys_mode():
+    """The oracle's accurate Boys mode (series + downward recursion below 50,
+    exact upward recursion above) agrees with scipy to a few ulps in relative
+    terms up to m = 24, where the reference's scheme loses digits (Taylor
+    truncation on the 0.1 grid; exp(-x) dropped from x = 35); the default mode
+    stays the reference's."""
+    worst_acc = worst_ref = 0.0
+    for x in np.concatenate([np.linspace(0.0, 70.0, 141), [1e-9, 1e-4, 34.99, 35.0, 35.5, 49.99, 50.0]]):
+        ex = np.array([md_eri.boys(m, x) for m in range(25)])
+        acc = loader.boys(24, x, exact=True)
+        ref = loader.boys(24, x)
+        worst_acc = max(worst_acc, float((np.abs(acc - ex) / ex).max()))
+        worst_ref = max(worst_ref, float((np.abs(ref - ex) / ex).max()))
+    assert worst_acc < 1e-13
+    assert worst_ref > 1e-6  # the reference's own error at high m: the mode is a real switch
+    z = np.load(GOLDEN + '/boys.npz')
+    assert np.abs(loader.boys(int(z['nmax']), float(z['x'][0])) - z['F'][0]).max() <= 1e-15
+
+
+@pytest.mark.parametrize('ls',[(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 1, 1), (2, 1, 0, 1), (0, 2, 2, 1), (2, 2, 1, 1)])
 def test_oracle_vs_mcmurchie_davidson(ls):
     rng = np.random.default_rng(sum(ls) * 7 + 3)
     shells = []
