@@ -40,6 +40,7 @@ WORKLOAD = ('1e6 quartets, l<=2 per shell (81 classes uniform), K in 1..6, alpha
 SKIP_BELOW = 1e-12      # Schwarz screening: blocks with a smaller bound are written as zeros
 FP32_BELOW = 1e-4       # mixed path: FP32 VRR attempted below this bound ...
 MIXED_TOL = 5e-11       # ... and kept only where its rounding-error bound is below this; else FP64
+PRIM_TOL = 1e-18        # screened paths: primitive quartets with Q_ab Q_cd below this skipped
 FP32_SWEEP = (0.0, 1e-10, 1e-8, 1e-6, 1e-4)  # candidate FP32-tier bounds (0 = tier off), tuned per run
 FP32_CHOSEN = [0.0]
 ERR_BAR = 1e-10
@@ -58,7 +59,7 @@ def parse():
     ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx'],
                     help='eri: the headline; *_2idx: the example script\'s two-index classes')
     ap.add_argument('--npairs', type=int, default=4_000_000)
-    ap.add_argument('--only', default=None, choices=['fp64', 'screened'],
+    ap.add_argument('--only', default=None, choices=['fp64', 'screened', 'screened_prim'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time')
     return ap.parse_args()
 
@@ -396,8 +397,9 @@ def run_only(args, eng, out):
     import torch
     from intception_b200 import eri
     bounds, skip = None, 0.0
-    if args.only == 'screened':
+    if args.only in ('screened', 'screened_prim'):
         bounds, skip = eng.quartet_bounds(), SKIP_BELOW
+    eri.set_prim_tol(PRIM_TOL if args.only == 'screened_prim' else 0.0)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         eng.compute(out=out, bounds=bounds, skip_below=skip)
@@ -472,6 +474,7 @@ def main():
     # ---------------- Schwarz bounds (per shell pair, once per basis), then the screened paths
     mixed = None
     screened = None
+    screened_prim = None
     if not args.no_mixed:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -484,6 +487,15 @@ def main():
         err_s = max_over_ranks(float((out - ref64).abs().max().item()), world)
         screened = {'value': args.nq * world / (ms_s * 1e-3), 'ms_per_step': ms_s, 'max_abs_err_vs_fp64': err_s,
                     'screened_quartets_per_s': n_kept * world / (ms_s * 1e-3)}
+        # primitive screening on top (kept for every path below): a primitive
+        # quartet whose Schwarz-type bound Q_ab Q_cd is below PRIM_TOL moves
+        # no element by more than PRIM_TOL, so a block by at most K^4 PRIM_TOL
+        eri.set_prim_tol(PRIM_TOL)
+        ms_p = timed(lambda: step(eri.PREC_FP64, bounds, SKIP_BELOW))
+        err_p = max_over_ranks(float((out - ref64).abs().max().item()), world)
+        screened_prim = {'value': args.nq * world / (ms_p * 1e-3), 'ms_per_step': ms_p, 'max_abs_err_vs_fp64': err_p,
+                         'prim_tol': PRIM_TOL, 'error_bound_per_element': 1296 * PRIM_TOL,
+                         'screened_quartets_per_s': n_kept * world / (ms_p * 1e-3)}
         # precision tiers: zeros below SKIP_BELOW, FP32 VRR (with its rounding-error
         # bound, rejected quartets redone in FP64) below fp32_below, FP64 above.
         # fp32_below is tuned here; 0 switches the FP32 tier off.
@@ -504,7 +516,7 @@ def main():
         err = best['max_abs_err_vs_fp64']
         mixed = {'value': args.nq * world / (msmx * 1e-3), 'ms_per_step': msmx, 'max_abs_err_vs_fp64': err,
                  'screened_quartets_per_s': n_kept * world / (msmx * 1e-3),
-                 'kept_fraction': n_kept / args.nq, 'skip_below': SKIP_BELOW, 'fp32_below': fb,
+                 'kept_fraction': n_kept / args.nq, 'skip_below': SKIP_BELOW, 'prim_tol': PRIM_TOL, 'fp32_below': fb,
                  'mixed_tol': MIXED_TOL, 'fp32_tier_active': fb > 0, 'fp32_sweep': sweep,
                  'schwarz_ms': schwarz_ms, 'schwarz_note': 'per-pair Schwarz factors, computed once per basis '
                  'on the GPU (intception_b200_schwarz), outside the timed step; this workload has no pair reuse'}
@@ -529,8 +541,8 @@ def main():
         # the tuned tier path, measured three ways: the sweep's best setting,
         # its graph replay, and (FP32 tier off) the screened FP64 run above
         cands = [mixed['ms_per_step'], ms_graph]
-        if FP32_CHOSEN[0] == 0 and screened is not None:
-            cands.append(screened['ms_per_step'])
+        if FP32_CHOSEN[0] == 0 and screened_prim is not None:
+            cands.append(screened_prim['ms_per_step'])
         ms = min(cands)
         value = args.nq * world / (ms * 1e-3)
     else:
@@ -596,6 +608,7 @@ def main():
                'api': 'eri.HostPipeline (pinned host inputs -> blocks in pinned host memory, depth 2)'}
 
     clk.__exit__(None, None, None)
+    eri.set_prim_tol(0.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds)
@@ -607,11 +620,13 @@ def main():
                 'vs_baseline': None, 'dtype': 'f64+f32' if (headline_mixed and FP32_CHOSEN[0] > 0) else 'f64', 'data': 'synthetic',
                 'config': {'workload': WORKLOAD, 'nq_per_gpu': args.nq,
                            'l2': 'inputs+outputs ~1 GB per step, larger than L2; no flush',
-                           'headline_path': ('precision tiers: screened zeros below %.0e, FP32 below %g, FP64 above'
-                                             % (SKIP_BELOW, FP32_CHOSEN[0])) if headline_mixed else 'fp64'},
+                           'headline_path': ('precision tiers: screened zeros below %.0e, FP32 below %g, FP64 above; '
+                                             'primitive quartets with bound below %.0e skipped'
+                                             % (SKIP_BELOW, FP32_CHOSEN[0], PRIM_TOL)) if headline_mixed else 'fp64'},
                 'fp64': {'value': value64, 'ms_per_step': ms64, 'note': 'every quartet evaluated in FP64'},
                 'cuda_graph_ms_per_step': ms_graph,
                 'fp64_screened': screened,
+                'fp64_screened_prim': screened_prim,
                 'mixed': mixed,
                 'mixed_over_fp64': (mixed['value'] / value64) if mixed else None,
                 'mixed_over_fp64_screened': (mixed['value'] / screened['value']) if mixed else None,

@@ -203,6 +203,17 @@ int intception_b200_last_fp32_rejections(void);
  * rounding for every cap.  New: the reference's functions have no such knob. */
 int intception_b200_set_slice_cap(int cid, int cap);
 
+/* Primitive screening for the batch entries (intception_b200_eri_batch and its
+ * graph form): a primitive quartet whose bound Q_ab Q_cd is below tol is not
+ * evaluated.  Q is a Schwarz-type bound on the Coulomb norm of a primitive
+ * pair's charge distributions (times the spherical transform's largest
+ * coefficient sum), so each skipped primitive quartet moves an element of its
+ * block by at most tol; a block moves by at most Ka Kb Kc Kd x tol.  0 (the
+ * default) skips only primitive quartets whose prefactor is exactly zero.
+ * tol outside [0, 1e-6] returns IB_ERR_ARG.  The drop-in functions never
+ * screen.  New: the reference evaluates every primitive quartet. */
+int intception_b200_set_prim_tol(double tol);
+
 /* Tuning: register budget of the kernel of canonical class cid for variant v4
  * (0 FP64 Cartesian, 1 FP64 spherical, 2 FP32 Cartesian, 3 FP32 spherical):
  * the kernel compiled for minb (1, 3, 4 or 5) resident blocks per SM; 0

@@ -49,6 +49,7 @@ struct IbLaunch {
   int max_slices;          // class kernels: cap on lane groups sharing one quartet (0: lane groups per block)
   int slice_boost;         // class kernels: choose slices as if the grid had this many times its lane groups (>= 1)
   int* counter;            // class kernels: next quartet of the range (zero before the launch; one per launch)
+  double prim_tol;         // class kernels: skip primitive quartets whose bound is below this (0: exact zeros only)
 };
 
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
@@ -307,6 +308,117 @@ __device__ __forceinline__ int ib_live_pairs(const IbLaunch& a, const IbQuartet&
     cnt += __popc(bal);
   }
   return cnt;
+}
+
+// ---- Primitive screening.  For a primitive pair (exponents x0, x1 on
+// centres A, B; P the product centre, zeta = x0 + x1) every Cartesian
+// component of the product is bounded pointwise,
+//   |c0 c1 (x-A_x)^i .. (x-B_x)^j ..| exp(-x0|r-A|^2 - x1|r-B|^2)
+//     <= K (rho + |PA|)^l0 (rho + |PB|)^l1 exp(-zeta rho^2),   rho = |r - P|,
+// K = |c0 c1| exp(-x0 x1 |AB|^2 / zeta).  The Coulomb norm ||f|| = (f|f)^1/2
+// is monotone for positive f and obeys the triangle inequality, and
+// ||rho^n exp(-zeta rho^2)|| = N_n zeta^-(2n+5)/4 with N_n^2 the self-energy of
+// r^n exp(-r^2) (N_0^2 = sqrt(2) pi^5/2; the others by quadrature, 30
+// digits).  So the primitive pair's charge distributions have Coulomb norm
+//   Q <= K sum_ij C(l0,i) C(l1,j) |PA|^(l0-i) |PB|^(l1-j) N_(i+j) zeta^-(2(i+j)+5)/4,
+// times, for spherical output, the largest sum of |coefficients| of a
+// spherical function over Cartesians (per shell).  By Cauchy-Schwarz a
+// primitive quartet changes no element of its block by more than
+// Q_ab Q_cd: skipping those below a tolerance t moves an element by at most
+// (number skipped) x t.
+__host__ __device__ inline constexpr double ib_rn_norm(int n) {
+  return n == 0 ? 4.9738746919472297 : n == 1 ? 5.1652368552576019 : n == 2 ? 6.4612527577002005
+       : n == 3 ? 9.2648431767816622 : n == 4 ? 14.794795287711256 : n == 5 ? 25.818805439099522
+       : n == 6 ? 48.591021989124202 : n == 7 ? 97.655519373091779 : n == 8 ? 208.00183355514711
+       : n == 9 ? 466.71786414003641 : n == 10 ? 1097.8288726985819 : n == 11 ? 2696.1716819638506
+       : 6889.8632213814936;
+}
+__host__ __device__ inline constexpr double ib_binom(int n, int k) {
+  return k == 0 || k == n ? 1.0 : ib_binom(n - 1, k - 1) + ib_binom(n - 1, k);
+}
+// largest sum of |Cartesian coefficients| of one spherical function of the
+// library's transformation matrices, l = 0..6 (rounded up)
+__host__ __device__ inline constexpr double ib_sph_colsum(int l) {
+  return l <= 1 ? 1.0 : l == 2 ? 2.0 : l == 3 ? 4.0 : l == 4 ? 8.9442719099991597 : l == 5 ? 20.493901531919201
+       : 47.096974425115671;
+}
+
+template <int L0, int L1, bool SPH>
+__device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa, double pb) {
+  const double s = 1.0 / sqrt(zeta);  // zeta^-1/2
+  double poly = 0.0;
+#pragma unroll
+  for (int i = 0; i <= L0; ++i) {
+#pragma unroll
+    for (int j = 0; j <= L1; ++j) {
+      double t = ib_binom(L0, i) * ib_binom(L1, j) * ib_rn_norm(i + j);
+#pragma unroll
+      for (int k = 0; k < L0 - i; ++k) t *= pa;
+#pragma unroll
+      for (int k = 0; k < L1 - j; ++k) t *= pb;
+#pragma unroll
+      for (int k = 0; k < i + j; ++k) t *= s;
+      poly += t;
+    }
+  }
+  // zeta^-5/4; the factor 1 + 1e-6 covers the rounding of the bound itself
+  const double sph = SPH ? ib_sph_colsum(L0) * ib_sph_colsum(L1) : 1.0;
+  return 1.000001 * sph * K * s * s * sqrt(s) * poly;
+}
+
+// Bound Q of primitive pair i0 * k1 + i1 of two shells (exponent/coefficient
+// runs at ptr0, ptr1; squared centre distance r2).
+template <int L0, int L1, bool SPH>
+__device__ __forceinline__ double ib_pair_q(const double* __restrict__ pe, const double* __restrict__ pc, int ptr0,
+                                            int ptr1, int k1, double r2, int p) {
+  const int i0 = p / k1, i1 = p - i0 * k1;
+  const double x0 = __ldg(pe + ptr0 + i0), c0 = __ldg(pc + ptr0 + i0);
+  const double x1 = __ldg(pe + ptr1 + i1), c1 = __ldg(pc + ptr1 + i1);
+  const double z = x0 + x1, oz = 1.0 / z, R = sqrt(r2);
+  const double K = fabs(ib_pair_factor(x0, c0, x1, c1, oz, r2));
+  return ib_pair_bound<L0, L1, SPH>(K, z, x1 * oz * R, x0 * oz * R);
+}
+
+// Live-pair lists of one 64 x 64 pair tile with primitive screening (tol > 0):
+// pair ab (tile offset t, pair p0 + t of shells a, b) stays if Q_ab times the
+// largest Q_cd of the tile reaches tol, and likewise for cd; every primitive
+// quartet dropped this way has Q_ab Q_cd < tol.  Run by the nb builder lanes
+// of one warp as ib_live_pairs (lane rank b, lanes bmask starting at bbase);
+// the largest bounds are reduced over those lanes as floats rounded up.  The
+// class kernels call it before their accumulators are live.  Returns (n0, n1).
+template <int LA, int LB, int LC, int LD, bool SPH>
+__device__ __forceinline__ int2 ib_live_pairs_screened(const double* __restrict__ pe, const double* __restrict__ pc,
+                                                    int pa, int pb, int kb, int pcs, int pd, int kd, double rab2,
+                                                    double rcd2, int p0, int m0, int p1, int m1,
+                                                    unsigned char* __restrict__ lst, int b, int nb, unsigned bmask,
+                                                    int bbase, double tol) {
+  double q0 = 0.0, q1 = 0.0;
+  for (int t = b; t < m0; t += nb) q0 = fmax(q0, ib_pair_q<LA, LB, SPH>(pe, pc, pa, pb, kb, rab2, p0 + t));
+  for (int t = b; t < m1; t += nb) q1 = fmax(q1, ib_pair_q<LC, LD, SPH>(pe, pc, pcs, pd, kd, rcd2, p1 + t));
+  const double M0 = (double)__uint_as_float(__reduce_max_sync(bmask, __float_as_uint(__double2float_ru(q0))));
+  const double M1 = (double)__uint_as_float(__reduce_max_sync(bmask, __float_as_uint(__double2float_ru(q1))));
+  int n[2];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const int p = side ? p1 : p0, m = side ? m1 : m0;
+    const double other = side ? M0 : M1;
+    unsigned char* __restrict__ l = lst + 64 * side;
+    int cnt = 0;
+    for (int t0 = 0; t0 < m; t0 += nb) {
+      const int t = t0 + b;
+      bool live = false;
+      if (t < m) {
+        const double q = side ? ib_pair_q<LC, LD, SPH>(pe, pc, pcs, pd, kd, rcd2, p + t)
+                              : ib_pair_q<LA, LB, SPH>(pe, pc, pa, pb, kb, rab2, p + t);
+        live = q > 0.0 && q * other >= tol;
+      }
+      const unsigned bal = __ballot_sync(bmask, live) >> bbase;
+      if (live) l[cnt + __popc(bal & ((1u << b) - 1u))] = (unsigned char)t;
+      cnt += __popc(bal);
+    }
+    n[side] = cnt;
+  }
+  return make_int2(n[0], n[1]);
 }
 
 template <typename R>

@@ -115,6 +115,7 @@ struct Context {
   // 4 shortens the last, thinly occupied waves (screened step -17 %, full
   // FP64 step -5 %) and 8 is slower again.
   int slice_boost = 4;
+  double prim_tol = 0.0;  // batch entries: primitive-quartet screening tolerance (0: exact zeros only)
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
@@ -191,10 +192,36 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
   }
 }
 
+// Smallest primitive exponent of shell s.
+__device__ __forceinline__ double ib_min_exp(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                             const double* __restrict__ prim_exp, int s) {
+  const int k = __ldg(shell_k + s), p0 = __ldg(shell_ptr + s);
+  double m = __ldg(prim_exp + p0);
+  for (int i = 1; i < k; ++i) m = fmin(m, __ldg(prim_exp + p0 + i));
+  return m;
+}
+
+// Within a pair of equal l, the shell the vertical recurrence builds on comes
+// first: the more compact one (larger smallest exponent).  The product centre
+// then lies near it, the [e0| and |f0] intermediates stay small, and the
+// horizontal recurrence cancels fewer digits (measured: intermediates of 2e3
+// for a block of 1e-2 with the diffuse shell first, 6e-2 with the compact one).
+__device__ __forceinline__ void ib_compact_first(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                                 const double* __restrict__ prim_exp, int* s, const int* l, int* st) {
+  for (int i = 0; i < 4; i += 2) {
+    if (l[i] != l[i + 1] || s[i] == s[i + 1]) continue;
+    if (ib_min_exp(shell_k, shell_ptr, prim_exp, s[i]) < ib_min_exp(shell_k, shell_ptr, prim_exp, s[i + 1])) {
+      int t = s[i]; s[i] = s[i + 1]; s[i + 1] = t;
+      t = st[i]; st[i] = st[i + 1]; st[i + 1] = t;
+    }
+  }
+}
+
 __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __restrict__ order, int nq,
                                const int* __restrict__ quartets, const int* __restrict__ shell_l,
-                               const long long* __restrict__ out_off, int spherical, IbItem* __restrict__ items,
-                               int* __restrict__ ranges) {
+                               const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                               const double* __restrict__ prim_exp, const long long* __restrict__ out_off,
+                               int spherical, IbItem* __restrict__ items, int* __restrict__ ranges) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
     const int q = order[p];
     int s[4], l[4], n[4];
@@ -205,6 +232,7 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     }
     int st[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
     ib_canon(s, l, st);
+    ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);
     IbItem it;
     for (int i = 0; i < 4; ++i) {
       it.s[i] = s[i];
@@ -603,6 +631,10 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     swp(0, 2);
     swp(1, 3);
   }
+  // within a pair of equal l the more compact shell first (as the batch entries do)
+  auto min_exp = [&](int i) { return *std::min_element(sh[i].x, sh[i].x + sh[i].nprim); };
+  for (int i = 0; i < 4; i += 2)
+    if (lperm[i] == lperm[i + 1] && min_exp(sperm[i]) < min_exp(sperm[i + 1])) swp(i, i + 1);
   const int pb = pair_index_h(lperm[0], lperm[1]), pk = pair_index_h(lperm[2], lperm[3]);
   const int cid = pb * (pb + 1) / 2 + pk;
   int b = 0;
@@ -838,8 +870,8 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
                                           c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
   ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
-                                      out_off, spherical ? 1 : 0, c->items.as<IbItem>(),
-                                      c->ranges.as<int>());
+                                      basis->shell_k, basis->shell_ptr, basis->prim_exp, out_off,
+                                      spherical ? 1 : 0, c->items.as<IbItem>(), c->ranges.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());
   IbLaunch a = base_launch(c);
@@ -852,6 +884,7 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   a.prim_exp = basis->prim_exp;
   a.prim_coef = basis->prim_coef;
   a.out = out;
+  a.prim_tol = c->prim_tol;
   if (precision == IB_PREC_MIXED) {
     IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
     IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
@@ -1133,6 +1166,19 @@ int intception_b200_set_slice_cap(int cid, int cap) {
   if (cid >= IB_NCLASS || cap < 0) return set_status(IB_ERR_ARG, "set_slice_cap: class id or cap out of range");
   for (int k = 0; k < IB_NCLASS; ++k)
     if (cid < 0 || k == cid) c->slice_cap[k] = cap;
+  return set_status(IB_OK, "");
+}
+
+// Primitive screening in the batch entries' class kernels: a primitive
+// quartet whose Coulomb-norm bound Q_ab Q_cd is below tol is skipped, which
+// moves no element of its block by more than tol (0 restores exact-zero
+// culling only; the drop-in functions never screen).
+int intception_b200_set_prim_tol(double tol) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  if (!(tol >= 0.0) || tol > 1e-6) return set_status(IB_ERR_ARG, "set_prim_tol: tolerance outside [0, 1e-6]");
+  c->prim_tol = tol;
   return set_status(IB_OK, "");
 }
 

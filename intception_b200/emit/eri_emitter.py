@@ -408,10 +408,9 @@ class Emitter:
 def emitted_classes():
     """Canonical classes with an unrolled kernel: every class with l <= 2
     (FP64 and FP32-VRR variants), and every class with an f shell and the rest
-    <= f whose smaller side fits a 64-lane group (FP64 only) -- all l <= 3
-    classes but (ff|ff), which the generic kernel serves (the nuclear-gradient
-    batches of an l <= 2 basis reach the one-f classes; an f basis reaches
-    them all)."""
+    <= f (FP64 only; (ff|ff) with 128-lane groups) -- the nuclear-gradient
+    batches of an l <= 2 basis reach the one-f classes, an f basis reaches
+    them all."""
     from .group_emitter import orientation
     out = [(c, True) for c in canonical_classes(LMAX_EMIT)]
     for c in canonical_classes(3):

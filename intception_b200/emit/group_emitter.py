@@ -226,6 +226,21 @@ class GroupEmitter:
         order = [(cc, mm) for cc in comps(k) for mm in range(1, self.C_hi - k + 1)]
         return order.index((c, m))
 
+    def builder_lanes(self):
+        """Declarations of the list-building lanes: the first min(SG, 32) lanes
+        of the quartet, their warp mask and first lane."""
+        out = ['        const int nbld = min(SG, 32);']
+        if self.wide:
+            out += ['        const unsigned bmask = 0xffffffffu;', '        const int bbase = 0;']
+        else:
+            out += ['        const unsigned bmask = SG >= 32 ? 0xffffffffu : sgmask;',
+                    '        const int bbase = SG >= 32 ? 0 : lane - r;']
+        return out
+
+    def lcls(self):
+        """The class's angular momenta as template arguments (canonical order)."""
+        return '%d, %d, %d, %d' % (self.la, self.lb, self.lc, self.ld)
+
     def n_slots(self):
         return max(len(comps(k)) * (self.C_hi - k) for k in range(self.C_hi + 1))
 
@@ -601,6 +616,19 @@ class GroupEmitter:
         src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // uniform over the quartet\'s lanes')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
+        src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
+        src.append('    const int kab = g.k[0] * kb_, kcd = g.k[2] * kd_;')
+        # primitive screening (a.prim_tol > 0) for quartets of one pair tile a
+        # side: the screened lists are built here, before the accumulators
+        # are live; larger quartets keep exact-zero culling only
+        src.append('    const bool pre = a.prim_tol > 0.0 && kab <= 64 && kcd <= 64;  // uniform over the quartet')
+        src.append('    if (pre && r < 32) {')
+        src += ['  ' + ln for ln in self.builder_lanes()]
+        src.append('      const int2 nn = ib_live_pairs_screened<%s, SPH>(a.prim_exp, a.prim_coef, g.ptr[0], g.ptr[1], '
+                   'kb_, g.ptr[2], g.ptr[3], kd_, g.RAB2, g.RCD2, 0, kab, 0, kcd, lst, r, nbld, bmask, bbase, '
+                   'a.prim_tol);' % self.lcls())
+        src.append('      if (r == 0) { lcnt[0] = nn.x; lcnt[1] = nn.y; }')
+        src.append('    }')
         src.append('    double acc[%d];' % NT)
         src.append('#pragma unroll')
         src.append('    for (int k = 0; k < %d; ++k) acc[k] = 0.0;' % NT)
@@ -616,8 +644,6 @@ class GroupEmitter:
         # min(SG, 32) lanes of the quartet list the pairs whose prefactor is
         # not zero (ib_live_pairs), and the slices run over live x live
         # primitive quartets only (the others are exactly zero)
-        src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
-        src.append('    const int kab = g.k[0] * kb_, kcd = g.k[2] * kd_;')
         src.append('    // exact small-integer quotients: (x + 0.5) / k is >= 1/128 away from an integer')
         src.append('    const float rkb = 1.0f / (float)kb_, rkd = 1.0f / (float)kd_;')
         # FP32 tier: growth of an accumulator's error through the HRRs and
@@ -627,14 +653,8 @@ class GroupEmitter:
         src.append('    (void)famp;')
         src.append('    for (int ab0 = 0; ab0 < kab; ab0 += 64)')
         src.append('    for (int cd0 = 0; cd0 < kcd; cd0 += 64) {')
-        src.append('      if (r < 32) {')
-        src.append('        const int nbld = min(SG, 32);')
-        if self.wide:
-            src.append('        const unsigned bmask = 0xffffffffu;')
-            src.append('        const int bbase = 0;')
-        else:
-            src.append('        const unsigned bmask = SG >= 32 ? 0xffffffffu : sgmask;')
-            src.append('        const int bbase = SG >= 32 ? 0 : lane - r;')
+        src.append('      if (r < 32 && !pre) {')
+        src += self.builder_lanes()
         src.append('        const int n0 = ib_live_pairs(a, g, 0, ab0, min(64, kab - ab0), lst, r, nbld, bmask, bbase);')
         src.append('        const int n1 = ib_live_pairs(a, g, 1, cd0, min(64, kcd - cd0), lst + 64, r, nbld, bmask, bbase);')
         src.append('        if (r == 0) { lcnt[0] = n0; lcnt[1] = n1; }')

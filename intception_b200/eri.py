@@ -107,6 +107,8 @@ def load():
     lib.intception_b200_fma_peak.restype = C.c_int
     lib.intception_b200_set_slice_cap.argtypes = [C.c_int, C.c_int]
     lib.intception_b200_set_slice_cap.restype = C.c_int
+    lib.intception_b200_set_prim_tol.argtypes = [C.c_double]
+    lib.intception_b200_set_prim_tol.restype = C.c_int
     lib.intception_b200_set_class_minb.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.intception_b200_set_class_minb.restype = C.c_int
     lib.intception_b200_set_class_fp32.argtypes = [C.c_int, C.c_int]
@@ -151,6 +153,14 @@ def set_slice_cap(cap, cls=None):
     in the class kernels: every class, or the canonical class (la,lb,lc,ld)."""
     cid = -1 if cls is None else class_id(*cls)
     _check(load().intception_b200_set_slice_cap(cid, int(cap)))
+
+
+def set_prim_tol(tol):
+    """Primitive screening in the batch path (EriEngine.compute, graphs):
+    primitive quartets whose Coulomb-norm bound Q_ab Q_cd is below tol are
+    skipped, so an element moves by at most Ka Kb Kc Kd * tol; 0 (default)
+    skips only exact-zero prefactors.  The drop-ins never screen."""
+    _check(load().intception_b200_set_prim_tol(float(tol)))
 
 
 def set_class_minb(cls, variant, minb):
