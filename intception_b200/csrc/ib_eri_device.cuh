@@ -379,13 +379,32 @@ __device__ __forceinline__ double ib_pair_q(const double* __restrict__ pe, const
   return ib_pair_bound<L0, L1, SPH>(K, z, x1 * oz * R, x0 * oz * R);
 }
 
+// Power-of-two exponent e with Q <= 2^e (Q >= 0), clamped to [-127, 127];
+// 127 stands for "not small" (Q >= 2^126 never occurs for normalised shells,
+// and a primitive quartet with it is never skipped).
+__device__ __forceinline__ signed char ib_q_exp(double q) {
+  if (!(q > 0.0)) return -127;
+  const int e = ilogb(q) + 1;  // q < 2^(ilogb(q) + 1)
+  return (signed char)max(-127, min(e, 127));
+}
+
+// A primitive quartet of the screened lists (list positions qa, qc) whose
+// bound Q_ab Q_cd <= 2^(e_ab + e_cd) is below tol.
+__device__ __forceinline__ bool ib_quartet_negligible(const unsigned char* __restrict__ lst, int qa, int qc,
+                                                      double tol) {
+  const int ea = (signed char)lst[128 + qa], ec = (signed char)lst[192 + qc];
+  return ea < 127 && ec < 127 && ldexp(1.0, ea + ec) < tol;
+}
+
 // Live-pair lists of one 64 x 64 pair tile with primitive screening (tol > 0):
 // pair ab (tile offset t, pair p0 + t of shells a, b) stays if Q_ab times the
 // largest Q_cd of the tile reaches tol, and likewise for cd; every primitive
-// quartet dropped this way has Q_ab Q_cd < tol.  Run by the nb builder lanes
-// of one warp as ib_live_pairs (lane rank b, lanes bmask starting at bbase);
-// the largest bounds are reduced over those lanes as floats rounded up.  The
-// class kernels call it before their accumulators are live.  Returns (n0, n1).
+// quartet dropped this way has Q_ab Q_cd < tol.  Beside each list entry
+// (lst[128 + pos] side 0, lst[192 + pos] side 1) goes the exponent of its
+// pair's bound, for ib_quartet_negligible.  Run by the nb builder lanes of one
+// warp as ib_live_pairs (lane rank b, lanes bmask starting at bbase); the
+// largest bounds are reduced over those lanes as floats rounded up.  The class
+// kernels call it before their accumulators are live.  Returns (n0, n1).
 template <int LA, int LB, int LC, int LD, bool SPH>
 __device__ __forceinline__ int2 ib_live_pairs_screened(const double* __restrict__ pe, const double* __restrict__ pc,
                                                     int pa, int pb, int kb, int pcs, int pd, int kd, double rab2,
@@ -407,13 +426,18 @@ __device__ __forceinline__ int2 ib_live_pairs_screened(const double* __restrict_
     for (int t0 = 0; t0 < m; t0 += nb) {
       const int t = t0 + b;
       bool live = false;
+      double q = 0.0;
       if (t < m) {
-        const double q = side ? ib_pair_q<LC, LD, SPH>(pe, pc, pcs, pd, kd, rcd2, p + t)
-                              : ib_pair_q<LA, LB, SPH>(pe, pc, pa, pb, kb, rab2, p + t);
+        q = side ? ib_pair_q<LC, LD, SPH>(pe, pc, pcs, pd, kd, rcd2, p + t)
+                 : ib_pair_q<LA, LB, SPH>(pe, pc, pa, pb, kb, rab2, p + t);
         live = q > 0.0 && q * other >= tol;
       }
       const unsigned bal = __ballot_sync(bmask, live) >> bbase;
-      if (live) l[cnt + __popc(bal & ((1u << b) - 1u))] = (unsigned char)t;
+      if (live) {
+        const int pos = cnt + __popc(bal & ((1u << b) - 1u));
+        l[pos] = (unsigned char)t;
+        l[128 + pos] = (unsigned char)ib_q_exp(q);
+      }
       cnt += __popc(bal);
     }
     n[side] = cnt;

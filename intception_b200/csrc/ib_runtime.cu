@@ -232,7 +232,9 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     }
     int st[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
     ib_canon(s, l, st);
-    ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);
+    const unsigned key = keys[p];
+    const int slot = (int)(key >> 12);  // skip*2048 + generic*1024 + fp32*512 + cid
+    if (!(slot >> 11)) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);  // evaluated quartets only
     IbItem it;
     for (int i = 0; i < 4; ++i) {
       it.s[i] = s[i];
@@ -240,8 +242,6 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     }
     it.off = out_off[q];
     items[p] = it;
-    const unsigned key = keys[p];
-    const int slot = (int)(key >> 12);  // skip*2048 + generic*1024 + fp32*512 + cid
     const int prev = p > 0 ? (int)(keys[p - 1] >> 12) : -1;
     const int next = p + 1 < nq ? (int)(keys[p + 1] >> 12) : -1;
     if (slot >> 11) {  // screened out: one range for all of them, sorted last

@@ -579,7 +579,9 @@ class GroupEmitter:
         loop_len = xb_len + (nfield * self.G if self.G > 1 else 0)
         per_group = max(smem_group, loop_len)
         self.list_off = per_group
-        per_group += 18  # live-pair lists of the quartet's current tile (2 x 64 bytes), their counts, the grab slot
+        # live-pair lists of the quartet's current tile (2 x 64 bytes), the
+        # screening exponents of their pairs (2 x 64 bytes), the counts, the grab slot
+        per_group += 34
         self.red_off = per_group  # partial sums of a multi-warp or packed group's FP32 bound
         per_group += self.G if self.packed else (self.G // 32 if self.wide else 0)
         per_group += 1  # this slice's FP32 error bound, summed over the slices
@@ -595,7 +597,7 @@ class GroupEmitter:
             src.append('  int* __restrict__ pz = reinterpret_cast<int*>(sb + %d);' % (xb_len + (17 + self.L + 1) * self.G))
         self.per_group = per_group
         src.append('  unsigned char* __restrict__ lst = reinterpret_cast<unsigned char*>(sb0 + %d);' % self.list_off)
-        src.append('  int* __restrict__ lcnt = reinterpret_cast<int*>(sb0 + %d);' % (self.list_off + 16))
+        src.append('  int* __restrict__ lcnt = reinterpret_cast<int*>(sb0 + %d);' % (self.list_off + 32))
         # lane constants read once and pinned in registers: a divergent
         # constant-bank load re-issued inside the primitive loop would be
         # serialised per distinct lane address
@@ -669,6 +671,7 @@ class GroupEmitter:
             src.append('      IbBraPair bp;')
             src.append('      for (int u = w; u < npl; u += W) {')
             src.append('        const int qa = (int)(((float)u + 0.5f) * rn1), qc = u - qa * nl1;')
+            src.append('        if (pre && ib_quartet_negligible(lst, qa, qc, a.prim_tol)) continue;')
             src.append('        const int ab = ab0 + lst[qa], cd = cd0 + lst[64 + qc];')
             src.append('        if (ab != ab_last) {')
             src.append('          const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
@@ -700,10 +703,13 @@ class GroupEmitter:
             src.append('            const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
             src.append('            const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
             src.append('            IbBraPair bp;')
-            src.append('            ib_bra_pair(a, g, ia, ib, bp);')
             src.append('            IbPrimQuartet<R> pq;')
             src.append('            double F[%d];' % (L + 1))
-            src.append('            const bool live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
+            src.append('            bool live = !(pre && ib_quartet_negligible(lst, qa, qc, a.prim_tol));')
+            src.append('            if (live) {')
+            src.append('              ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('              live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
+            src.append('            }')
             src.append('            if (live) {')
             for k, f in enumerate(fields):
                 src.append('              ps[%d * %d + j] = pq.%s;' % (k, self.G, f))
@@ -711,7 +717,7 @@ class GroupEmitter:
                 src.append('              ps[%d * %d + j] = (R)F[%d];' % (len(fields) + m, self.G, m))
             src.append('              if (sizeof(R) == 4) est += %s;' % self.err_expr())
             src.append('            }')
-            src.append('            pz[j] = live ? 1 : 0;  // 0 only where the two pair prefactors multiply to zero')
+            src.append('            pz[j] = live ? 1 : 0;  // 0: pair prefactors multiply to zero, or screened out')
             src.append('          }')
             src.append('        }')
             src.append('        %s;' % sync)
