@@ -116,6 +116,8 @@ struct Context {
   // FP64 step -5 %) and 8 is slower again.
   int slice_boost = 4;
   double prim_tol = 0.0;  // batch entries: primitive-quartet screening tolerance (0: exact zeros only)
+  int zero_bps = 4;       // zero fill of screened blocks: blocks per SM (INTCEPTION_B200_ZERO_BPS)
+  int zero_last = 0;      // 1: launch it after the class kernels (INTCEPTION_B200_ZERO_LAST)
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
@@ -262,30 +264,32 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
 }
 
 // Screened-out quartets (bound below the skip threshold, so |(ab|cd)| <= bound):
-// their blocks are written as zeros, 32 quartets per warp.
-__global__ void ib_zero_blocks(const IbItem* __restrict__ items, const int* __restrict__ ranges,
-                               const int* __restrict__ shell_l, int spherical, double* __restrict__ out) {
-  // A quartet's block is the contiguous range [off, off + na nb nc nd) whatever
-  // the canonical permutation (it only reorders the four indices).  Each lane
-  // fetches one quartet's offset and size; the warp then writes the 32 blocks
-  // with coalesced stores.
-  const int beg = ranges[kSlotSkip], end = ranges[kSlotSkip + 1];
+// their blocks are written as zeros.  The kernel walks the quartets in the
+// caller's order (the classify keys, unsorted, carry the skip bit), so that
+// consecutive blocks usually lie next to each other in memory and the stores
+// of one warp fill whole sectors.  Each lane fetches one quartet's offset and
+// size (0 when it is evaluated); the warp then writes the 32 blocks.
+__global__ void ib_zero_screened(const unsigned* __restrict__ keys, int nq, const int* __restrict__ quartets,
+                                 const int* __restrict__ shell_l, const long long* __restrict__ out_off,
+                                 int spherical, double* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (int base = beg + wg * 32; base < end; base += nw * 32) {  // warp-uniform
-    const int p = base + lane;
+  for (int base = wg * 32; base < nq; base += nw * 32) {  // warp-uniform
+    const int q = base + lane;
     long long off = 0;
     int tot = 0;
-    if (p < end) {
-      const IbItem it = items[p];
+    if (q < nq && (keys[q] >> 23)) {
       tot = 1;
       for (int i = 0; i < 4; ++i) {
-        const int l = min(max(shell_l[it.s[i]], 0), IB_LMAX);
+        const int l = min(max(shell_l[quartets[4 * q + i]], 0), IB_LMAX);
         tot *= spherical ? 2 * l + 1 : ib_ncart_d(l);
       }
-      off = it.off;
+      off = out_off[q];
     }
-    for (int k = 0; k < 32; ++k) {
+    unsigned any = __ballot_sync(0xffffffffu, tot > 0);
+    while (any) {
+      const int k = __ffs(any) - 1;
+      any &= any - 1;
       const long long o = __shfl_sync(0xffffffffu, off, k);
       const int n = __shfl_sync(0xffffffffu, tot, k);
       double* __restrict__ d = out + o;
@@ -293,6 +297,14 @@ __global__ void ib_zero_blocks(const IbItem* __restrict__ items, const int* __re
     }
   }
 }
+
+struct ZeroFill {  // the caller's quartets whose blocks the screened path writes as zeros
+  const unsigned* keys;
+  int nq;
+  const int* quartets;
+  const int* shell_l;
+  const long long* out_off;
+};
 
 // Diagonal quartets (a,b|a,b) of a chunk of shell pairs, their block sizes, and
 // afterwards sqrt(max |(ij|ij)|) over the diagonal of each block.
@@ -400,6 +412,8 @@ int get_context(Context** out) {
     IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     if (const char* env = std::getenv("INTCEPTION_B200_STREAMS")) c->nside = std::max(1, std::min(kNSideMax, std::atoi(env)));
+    if (const char* env = std::getenv("INTCEPTION_B200_ZERO_BPS")) c->zero_bps = std::max(1, std::min(32, std::atoi(env)));
+    if (const char* env = std::getenv("INTCEPTION_B200_ZERO_LAST")) c->zero_last = std::atoi(env) != 0;
     for (int i = 0; i < c->nside; ++i) {
       IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
       IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
@@ -475,15 +489,19 @@ int class_lmax(int cid) {
 // Launch the emitted kernels for the given variants and the generic kernel;
 // items/ranges already on the device.  Returns the number of kernels launched.
 int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
-             int lmax, int* nlaunch, const int* zero_fill_shell_l = nullptr) {
+             int lmax, int* nlaunch, const ZeroFill* zf = nullptr) {
   IB_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < c->nside; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
   int k = 0;
-  if (zero_fill_shell_l) {  // screened quartets: zero blocks, concurrent with the class kernels
-    ib_zero_blocks<<<c->nsm * 4, 256, 0, c->side[c->nside - 1]>>>(a.items, a.ranges, zero_fill_shell_l, sph ? 1 : 0,
-                                                                   a.out);
+  // screened quartets: zero blocks, concurrent with the class kernels
+  auto zero_fill = [&]() {
+    if (!zf) return;
+    ib_zero_screened<<<c->nsm * c->zero_bps, 256, 0, c->side[c->nside - 1]>>>(zf->keys, zf->nq, zf->quartets,
+                                                                              zf->shell_l, zf->out_off, sph ? 1 : 0,
+                                                                              a.out);
     ++*nlaunch;
-  }
+  };
+  if (!c->zero_last) zero_fill();
   for (int prec = 0; prec < 2; ++prec) {
     if ((prec == 0 && !fp64_present) || (prec == 1 && !fp32_present)) continue;
     IbLaunch ap = a;
@@ -513,6 +531,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       }
     }
   }
+  if (c->zero_last) zero_fill();
   if (lmax > ib_lmax_emitted && fp64_present) {
     const long long slice = generic_slice(lmax);
     long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
@@ -839,7 +858,7 @@ int resolve_stream(Context* c, void* stream, cudaStream_t* s) {
 // The batch pipeline on stream s; the caller holds the context lock.
 int batch_impl(Context* c, const intception_b200_basis* basis, const int* quartets, const long long* out_off, int nq,
                int spherical, int precision, const double* bounds, double skip_below, double fp32_below,
-               double mixed_tol, double* out, cudaStream_t s, int* nl) {
+               double mixed_tol, double* out, cudaStream_t s, int* nl, bool screen_prims = true) {
   if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out)))
     return set_status(IB_ERR_ARG, "eri_batch: null argument");
   if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "eri_batch: basis lmax out of range");
@@ -884,15 +903,16 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   a.prim_exp = basis->prim_exp;
   a.prim_coef = basis->prim_coef;
   a.out = out;
-  a.prim_tol = c->prim_tol;
+  a.prim_tol = screen_prims ? c->prim_tol : 0.0;
   if (precision == IB_PREC_MIXED) {
     IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
     IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
     a.flags = c->flags.as<int>();
     a.mixed_tol = mixed_tol;
   }
+  const ZeroFill zf = {c->keys.as<unsigned>(), nq, quartets, basis->shell_l, out_off};
   return dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, nl,
-                  use_bounds && skip_below > 0.0 ? basis->shell_l : nullptr);
+                  use_bounds && skip_below > 0.0 ? &zf : nullptr);
 }
 }  // namespace
 
@@ -1063,7 +1083,8 @@ int intception_b200_schwarz(const intception_b200_basis* basis, const int* pairs
     IB_CUDA(c->sw_blocks.ensure((size_t)total * sizeof(double)));
     int nl = 0;
     st = batch_impl(c, basis, c->sw_quartets.as<int>(), c->sw_off.as<long long>(), n, spherical, IB_PREC_FP64,
-                    nullptr, 0.0, 0.0, 0.0, c->sw_blocks.as<double>(), s, &nl);
+                    nullptr, 0.0, 0.0, 0.0, c->sw_blocks.as<double>(), s, &nl,
+                    false);
     if (st) return st;
     ib_diag_max<<<grid, 256, 0, s>>>(pairs + 2 * (size_t)p0, n, basis->shell_l, spherical ? 1 : 0,
                                      c->sw_off.as<long long>(), c->sw_blocks.as<double>(), q + p0);

@@ -111,3 +111,19 @@ def test_prim_tol_rejects_out_of_range():
         with pytest.raises(Exception):
             eri.set_prim_tol(bad)
     eri.set_prim_tol(0.0)
+
+
+def test_schwarz_factors_ignore_prim_tol():
+    """The Schwarz factors bound the quartets that screening zeroes, so they
+    are computed without primitive screening whatever the setting."""
+    import torch
+    b = basis.config_mixed_l2(nq=4000, seed=8, spherical=True)
+    eng = eri.EriEngine(b)
+    q0 = eng.quartet_bounds()
+    eri.set_prim_tol(1e-6)
+    try:
+        q1 = eng.quartet_bounds()
+        torch.cuda.synchronize()
+    finally:
+        eri.set_prim_tol(0.0)
+    assert torch.equal(q0, q1)
