@@ -405,6 +405,9 @@ class Emitter:
         return '\n'.join(src), stats
 
 
+DEFAULT_SLICE_CAP = 8
+
+
 def emitted_classes():
     """Canonical classes with an unrolled kernel: every class with l <= 2
     (FP64 and FP32-VRR variants), and every class with an f shell and the rest
@@ -475,7 +478,11 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
     # register-budget index, per class the slice cap and whether the FP32 tier
     # uses the class's FP32 kernel (where it measured faster than FP64)
     minb = [[0] * 4 for _ in range(NCLASS_TOTAL)]
-    scap = [0] * NCLASS_TOTAL
+    # at most 8 lane groups per quartet unless tuned otherwise: measured on the
+    # screened l <= 2 step (3.4 % of 1e6 quartets kept, primitive screening at
+    # 1e-18), a cap of 8 gave 1.18 ms per step against 1.30 uncapped, 1.36 at 2
+    # and 1.64 at 1; a class with many quartets runs one group each anyway
+    scap = [DEFAULT_SLICE_CAP] * NCLASS_TOTAL
     fp32on = [1] * NCLASS_TOTAL
     tpath = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'tuning.json')
     if os.path.exists(tpath):
@@ -485,7 +492,7 @@ def emit_all(outdir, lmax=LMAX_EMIT, ngroups=8):
         for tag, ent in tun.get('classes', {}).items():
             cid = class_id(*(int(ch) for ch in tag))
             minb[cid] = [int(x) for x in ent.get('minb', [0, 0, 0, 0])]
-            scap[cid] = int(ent.get('slice_cap', 0))
+            scap[cid] = int(ent.get('slice_cap', DEFAULT_SLICE_CAP))
             fp32on[cid] = 1 if ent.get('fp32', True) else 0
     disp.append('extern const int ib_tuned_minb[%d][4] = {%s};'
                 % (NCLASS_TOTAL, ', '.join('{%s}' % ', '.join(map(str, r)) for r in minb)))
