@@ -56,9 +56,11 @@ def parse():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
-    ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx'],
-                    help='eri: the headline; *_2idx: the example script\'s two-index classes')
+    ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx', 'lattice_l3'],
+                    help='eri: the headline; *_2idx: the example script\'s two-index classes; lattice_l3: '
+                         'a sample of the 200-atom l <= 3 lattice\'s screened quartets')
     ap.add_argument('--npairs', type=int, default=4_000_000)
+    ap.add_argument('--nq-lattice', type=int, default=2_000_000)
     ap.add_argument('--only', default=None, choices=['fp64', 'screened', 'screened_prim'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time')
     return ap.parse_args()
@@ -250,6 +252,120 @@ def run_reference_arm(args, rank, world):
 
 
 TWOIDX_METRIC = 'primitive %s pair blocks/s (example_input.py class, l<=2)'
+LATTICE_WORKLOAD = ('200-atom jittered cubic lattice (2.6-bohr spacing, +-0.3 bohr jitter), per atom s(K=6) s(K=3) '
+                    'p(K=3) d(K=1) f(K=1), alpha log-uniform [0.1,1e3], seed 2; unique quartets with Schwarz bound '
+                    '>= 1e-12; a uniform sample of %d of them, spherical')
+
+
+def lattice_batch(nq, seed=2):
+    """The 200-atom l <= 3 lattice: shells, Schwarz factors of every shell pair
+    (on the GPU), and a uniform sample of nq of the unique quartets (pair
+    i >= pair j in Schwarz order) whose bound q_i q_j reaches 1e-12.  Returns
+    (batch, number of such quartets)."""
+    import torch
+    from intception_b200 import basis, eri
+    rng = np.random.default_rng(seed)
+    natom, spacing, jitter = 200, 2.6, 0.3
+    n = int(np.ceil(natom ** (1.0 / 3.0) - 1e-9))
+    sites = np.array([(i, j, k) for i in range(n) for j in range(n) for k in range(n)][:natom], np.float64)
+    xyz = sites * spacing + rng.uniform(-jitter, jitter, (natom, 3))
+    shells = ((0, 6), (0, 3), (1, 3), (2, 1), (3, 1))
+    ls = np.array([l for _ in range(natom) for (l, _) in shells], np.int32)
+    ks = np.array([k for _ in range(natom) for (_, k) in shells], np.int32)
+    centres = np.repeat(xyz, len(shells), axis=0)
+    l_, k_, p_, cxyz, e, c = basis.make_shells(rng, ls, ks, 0.1, 1e3, 1.0, centres=centres)
+    ns = len(l_)
+    a, b = np.tril_indices(ns)
+    pairs = np.stack([a, b], axis=1).astype(np.int32)
+    one = np.zeros((1, 4), np.int32)
+    b0 = basis.ShellBatch(l_, k_, p_, cxyz, e, c, one, *basis.packed_offsets(l_, one, True)[:1], True,
+                          basis.packed_offsets(l_, one, True)[1])
+    q = eri.EriEngine(b0).schwarz(torch.from_numpy(pairs).cuda()).cpu().numpy()
+    order = np.argsort(-q, kind='stable')
+    qs, pr = q[order], pairs[order]
+    # row i pairs with the rows j <= i whose q_j >= 1e-12 / q_i (a prefix: q sorted)
+    cnt = np.searchsorted(-qs, -(1e-12 / np.maximum(qs, 1e-300)), side='right')
+    m = np.minimum(cnt, np.arange(1, len(qs) + 1))
+    cm = np.cumsum(m)
+    total = int(cm[-1])
+    pos = np.sort(rng.choice(total, size=min(nq, total), replace=False))
+    row = np.searchsorted(cm, pos, side='right')
+    col = pos - (cm[row] - m[row])
+    quartets = np.ascontiguousarray(np.concatenate([pr[row], pr[col]], axis=1).astype(np.int32))
+    off, tot = basis.packed_offsets(l_, quartets, True)
+    return basis.ShellBatch(l_, k_, p_, cxyz, e, c, quartets, off, True, tot), total
+
+
+def run_lattice(args, rank, world, local):
+    """The lattice sample: FP64 exact, FP64 with primitive screening, and the
+    precision tiers (FP32 VRR below bound 1e-4, its error bound checked), one
+    JSON line; value = the fastest path within 1e-10 of exact FP64."""
+    import torch
+    from intception_b200 import eri
+    batch, total = lattice_batch(args.nq_lattice)
+    eng = eri.EriEngine(batch)
+    out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        assert eng.device_status() == 0
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+
+    clk = ClockSampler(local).__enter__()
+    eri.set_prim_tol(0.0)
+    ms64 = timed(lambda: eng.compute(out=out))
+    ref = out.clone()
+    bounds = eng.quartet_bounds()
+    eri.set_prim_tol(PRIM_TOL)
+    msp = timed(lambda: eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW))
+    errp = max_over_ranks(float((out - ref).abs().max().item()), world)
+    msm = timed(lambda: eng.compute(out=out, precision=eri.PREC_MIXED, bounds=bounds, skip_below=SKIP_BELOW,
+                                    fp32_below=FP32_BELOW, mixed_tol=MIXED_TOL))
+    errm = max_over_ranks(float((out - ref).abs().max().item()), world)
+    rej = eng.fp32_rejected()
+    nfp32 = int((bounds < FP32_BELOW).sum().item())
+    launches = eri.EriEngine.last_launch_count()
+    eri.set_prim_tol(0.0)
+    clk.__exit__(None, None, None)
+    cands = [(ms64, 0.0, 'fp64'), (msp, errp, 'fp64 + primitive screening'), (msm, errm, 'precision tiers')]
+    ok = [c for c in cands if c[1] <= ERR_BAR] or cands
+    ms, err, path = min(ok)
+    nq = batch.nq * world
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds)
+        cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
+    if rank == 0:
+        print(json.dumps({
+            'metric': 'contracted ERI quartets/s on B200, 200-atom l<=3 lattice (screened quartets, sample)',
+            'value': nq / (ms * 1e-3), 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64+f32' if path == 'precision tiers' else 'f64', 'data': 'synthetic',
+            'config': {'workload': LATTICE_WORKLOAD % batch.nq, 'screened_quartets_total': total,
+                       'headline_path': path, 'prim_tol': PRIM_TOL, 'fp32_below': FP32_BELOW,
+                       'mixed_tol': MIXED_TOL, 'l2': 'outputs %.0f MB per step, larger than L2; no flush'
+                       % (batch.out_size * 8 / 1e6)},
+            'max_abs_err_vs_fp64': err,
+            'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'exact, no screening'},
+            'fp64_prim': {'ms_per_step': msp, 'max_abs_err_vs_fp64': errp},
+            'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm, 'fp32_attempted': nfp32,
+                      'fp32_rejected': rej},
+            'estimated_full_lattice_s': total / (nq / (ms * 1e-3)),
+            'cpu_baseline': cpu, 'gpu_launches': launches * args.steps, 'clocks': clk.summary()}), flush=True)
+
+
 TWOIDX_WORKLOAD = ('%d primitive pairs%s, la and lb uniform in 0..2, alpha log-uniform [0.05,1e4], A in a 30-bohr '
                    'cube, B%s within 2 bohr of A, seed 1')
 
@@ -422,12 +538,23 @@ def main():
         # host cores only: no process group; rank 0 runs the reference, the
         # other ranks of a multi-GPU launch exit at once
         rank, world = int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1'))
+        if args.workload == 'lattice_l3':
+            if rank == 0:  # the sample is drawn with the GPU's Schwarz factors; its line carries cpu_baseline
+                print(json.dumps({'impl': 'reference', 'unavailable': 'lattice_l3 draws its quartet sample with '
+                                  'GPU Schwarz factors; the reference C99 is timed in that line\'s cpu_baseline'}))
+            return
         if args.workload != 'eri':
             run_twoidx(args, rank, world, 0)
         else:
             run_reference_arm(args, rank, world)
         return
     rank, world, local = dist_init(args.gpus)
+    if args.workload == 'lattice_l3':
+        run_lattice(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload != 'eri':
         run_twoidx(args, rank, world, local)
         if world > 1:
