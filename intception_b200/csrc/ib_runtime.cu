@@ -2,10 +2,10 @@
 //
 // Batch pipeline (all on the device, stream-ordered, no host round trip):
 //   1. ib_classify   : per quartet, canonical class id (la>=lb, lc>=ld,
-//                      bra pair >= ket pair), precision bit, primitive-pair
-//                      counts -> 22-bit sort key
-//   2. CUB radix sort: quartets grouped by (precision, class, Kab, Kcd) so a warp
-//                      sees one class and one loop shape
+//                      bra pair >= ket pair), screening and precision bits,
+//                      log2 of the primitive quartet count -> 16-bit sort key
+//   2. CUB radix sort: quartets grouped by (screening, precision, class), the
+//                      longest first within a class
 //   3. ib_build_items: permuted shells + output strides per sorted quartet, and
 //                      the [begin,end) range of every (precision, class)
 //   4. per-class persistent kernels (unrolled, emitted) fanned out over side
@@ -48,7 +48,7 @@ constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (
 constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
 constexpr int kNRanges = 4 * IB_NCLASS + 4;
 constexpr int kNCounters = 3 * IB_NCLASS;      // quartet counters: FP64 pass, FP32 pass, FP64 recheck pass
-constexpr int kKeyBits = 24;                    // skip(1) generic(1) fp32(1) class(9) Kab(6) Kcd(6)
+constexpr int kKeyBits = 16;                    // skip(1) generic(1) fp32(1) class(9) work(4): two radix passes
 constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
 
 thread_local int tl_status = IB_OK;
@@ -182,14 +182,16 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     ib_canon(s, l, st);
     const int pb = ib_pair_d(l[0], l[1]), pk = ib_pair_d(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
-    const int kab = min(shell_k[s[0]] * shell_k[s[1]], 63), kcd = min(shell_k[s[2]] * shell_k[s[3]], 63);
+    const int nprim = shell_k[s[0]] * shell_k[s[1]] * shell_k[s[2]] * shell_k[s[3]];
+    const int work = min(15, 31 - __clz(max(nprim, 1)));  // floor(log2) of the primitive quartet count
     const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
     const int k = kind[cid];
     const int gen = (!skip && k == 0) ? 1 : 0;
     const int fp32 = (!skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
-    // primitive-pair counts descending inside a class: the longest quartets start first
-    keys[q] = (unsigned(skip) << 23) | (unsigned(gen) << 22) | (unsigned(fp32) << 21) | (unsigned(cid) << 12) |
-              (unsigned(63 - kab) << 6) | unsigned(63 - kcd);
+    // primitive quartet counts (powers of two) descending inside a class: the
+    // longest quartets start first
+    keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | (unsigned(cid) << 4) |
+              unsigned(15 - work);
     vals[q] = q;
   }
 }
@@ -235,7 +237,7 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     int st[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
     ib_canon(s, l, st);
     const unsigned key = keys[p];
-    const int slot = (int)(key >> 12);  // skip*2048 + generic*1024 + fp32*512 + cid
+    const int slot = (int)(key >> 4);  // skip*2048 + generic*1024 + fp32*512 + cid
     if (!(slot >> 11)) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);  // evaluated quartets only
     IbItem it;
     for (int i = 0; i < 4; ++i) {
@@ -244,8 +246,8 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     }
     it.off = out_off[q];
     items[p] = it;
-    const int prev = p > 0 ? (int)(keys[p - 1] >> 12) : -1;
-    const int next = p + 1 < nq ? (int)(keys[p + 1] >> 12) : -1;
+    const int prev = p > 0 ? (int)(keys[p - 1] >> 4) : -1;
+    const int next = p + 1 < nq ? (int)(keys[p + 1] >> 4) : -1;
     if (slot >> 11) {  // screened out: one range for all of them, sorted last
       if (prev < 0 || !(prev >> 11)) ranges[kSlotSkip] = p;
       if (next < 0) ranges[kSlotSkip + 1] = p + 1;
@@ -278,7 +280,7 @@ __global__ void ib_zero_screened(const unsigned* __restrict__ keys, int nq, cons
     const int q = base + lane;
     long long off = 0;
     int tot = 0;
-    if (q < nq && (keys[q] >> 23)) {
+    if (q < nq && (keys[q] >> 15)) {
       tot = 1;
       for (int i = 0; i < 4; ++i) {
         const int l = min(max(shell_l[quartets[4 * q + i]], 0), IB_LMAX);
