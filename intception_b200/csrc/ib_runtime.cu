@@ -116,8 +116,6 @@ struct Context {
   // FP64 step -5 %) and 8 is slower again.
   int slice_boost = 4;
   double prim_tol = 0.0;  // batch entries: primitive-quartet screening tolerance (0: exact zeros only)
-  int zero_bps = 4;       // zero fill of screened blocks: blocks per SM (INTCEPTION_B200_ZERO_BPS)
-  int zero_last = 0;      // 1: launch it after the class kernels (INTCEPTION_B200_ZERO_LAST)
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
@@ -414,8 +412,6 @@ int get_context(Context** out) {
     IB_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
     IB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     if (const char* env = std::getenv("INTCEPTION_B200_STREAMS")) c->nside = std::max(1, std::min(kNSideMax, std::atoi(env)));
-    if (const char* env = std::getenv("INTCEPTION_B200_ZERO_BPS")) c->zero_bps = std::max(1, std::min(32, std::atoi(env)));
-    if (const char* env = std::getenv("INTCEPTION_B200_ZERO_LAST")) c->zero_last = std::atoi(env) != 0;
     for (int i = 0; i < c->nside; ++i) {
       IB_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
       IB_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
@@ -495,15 +491,14 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   IB_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < c->nside; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
   int k = 0;
-  // screened quartets: zero blocks, concurrent with the class kernels
-  auto zero_fill = [&]() {
-    if (!zf) return;
-    ib_zero_screened<<<c->nsm * c->zero_bps, 256, 0, c->side[c->nside - 1]>>>(zf->keys, zf->nq, zf->quartets,
-                                                                              zf->shell_l, zf->out_off, sph ? 1 : 0,
-                                                                              a.out);
+  // screened quartets: zero blocks, concurrent with the class kernels (launched
+  // first with 4 blocks per SM: measured no slower than 1 or 2 blocks per SM, or
+  // than launching it after the class kernels)
+  if (zf) {
+    ib_zero_screened<<<c->nsm * 4, 256, 0, c->side[c->nside - 1]>>>(zf->keys, zf->nq, zf->quartets, zf->shell_l,
+                                                                     zf->out_off, sph ? 1 : 0, a.out);
     ++*nlaunch;
-  };
-  if (!c->zero_last) zero_fill();
+  }
   for (int prec = 0; prec < 2; ++prec) {
     if ((prec == 0 && !fp64_present) || (prec == 1 && !fp32_present)) continue;
     IbLaunch ap = a;
@@ -533,7 +528,6 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       }
     }
   }
-  if (c->zero_last) zero_fill();
   if (lmax > ib_lmax_emitted && fp64_present) {
     const long long slice = generic_slice(lmax);
     long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
