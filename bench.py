@@ -259,39 +259,18 @@ LATTICE_WORKLOAD = ('200-atom jittered cubic lattice (2.6-bohr spacing, +-0.3 bo
 
 def lattice_batch(nq, seed=2):
     """The 200-atom l <= 3 lattice: shells, Schwarz factors of every shell pair
-    (on the GPU), and a uniform sample of nq of the unique quartets (pair
-    i >= pair j in Schwarz order) whose bound q_i q_j reaches 1e-12.  Returns
-    (batch, number of such quartets)."""
+    (on the GPU), and a uniform sample of nq of the unique quartets whose bound
+    reaches 1e-12.  Returns (batch, number of such quartets)."""
     import torch
     from intception_b200 import basis, eri
-    rng = np.random.default_rng(seed)
-    natom, spacing, jitter = 200, 2.6, 0.3
-    n = int(np.ceil(natom ** (1.0 / 3.0) - 1e-9))
-    sites = np.array([(i, j, k) for i in range(n) for j in range(n) for k in range(n)][:natom], np.float64)
-    xyz = sites * spacing + rng.uniform(-jitter, jitter, (natom, 3))
-    shells = ((0, 6), (0, 3), (1, 3), (2, 1), (3, 1))
-    ls = np.array([l for _ in range(natom) for (l, _) in shells], np.int32)
-    ks = np.array([k for _ in range(natom) for (_, k) in shells], np.int32)
-    centres = np.repeat(xyz, len(shells), axis=0)
-    l_, k_, p_, cxyz, e, c = basis.make_shells(rng, ls, ks, 0.1, 1e3, 1.0, centres=centres)
-    ns = len(l_)
-    a, b = np.tril_indices(ns)
+    rng, l_, k_, p_, cxyz, e, c = basis.lattice_shells(seed=seed)
+    a, b = np.tril_indices(len(l_))
     pairs = np.stack([a, b], axis=1).astype(np.int32)
     one = np.zeros((1, 4), np.int32)
-    b0 = basis.ShellBatch(l_, k_, p_, cxyz, e, c, one, *basis.packed_offsets(l_, one, True)[:1], True,
-                          basis.packed_offsets(l_, one, True)[1])
+    off1, tot1 = basis.packed_offsets(l_, one, True)
+    b0 = basis.ShellBatch(l_, k_, p_, cxyz, e, c, one, off1, True, tot1)
     q = eri.EriEngine(b0).schwarz(torch.from_numpy(pairs).cuda()).cpu().numpy()
-    order = np.argsort(-q, kind='stable')
-    qs, pr = q[order], pairs[order]
-    # row i pairs with the rows j <= i whose q_j >= 1e-12 / q_i (a prefix: q sorted)
-    cnt = np.searchsorted(-qs, -(1e-12 / np.maximum(qs, 1e-300)), side='right')
-    m = np.minimum(cnt, np.arange(1, len(qs) + 1))
-    cm = np.cumsum(m)
-    total = int(cm[-1])
-    pos = np.sort(rng.choice(total, size=min(nq, total), replace=False))
-    row = np.searchsorted(cm, pos, side='right')
-    col = pos - (cm[row] - m[row])
-    quartets = np.ascontiguousarray(np.concatenate([pr[row], pr[col]], axis=1).astype(np.int32))
+    quartets, total = basis.sample_screened_quartets(q, pairs, nq, rng, SKIP_BELOW)
     off, tot = basis.packed_offsets(l_, quartets, True)
     return basis.ShellBatch(l_, k_, p_, cxyz, e, c, quartets, off, True, tot), total
 

@@ -243,3 +243,41 @@ def config_mixed_l2(nq=1_000_000, seed=1, spherical=True):
     spherical output."""
     return independent_quartet_batch(seed, nq, [0, 1, 2], [1, 2, 3, 4, 5, 6], 0.05, 1.0e4, 30.0,
                                      spherical)
+
+
+def lattice_shells(natom=200, seed=2, spacing=2.6, jitter=0.3,
+                   shells=((0, 6), (0, 3), (1, 3), (2, 1), (3, 1)), alpha=(0.1, 1e3)):
+    """Jittered cubic lattice: the first natom sites (row-major) of the smallest
+    cube holding them, spacing bohr apart, each moved by a uniform +-jitter;
+    per atom the given (l, K) shells, exponents log-uniform in alpha,
+    coefficients uniform [0.1, 1] then normalised.  Returns (rng, shell_l,
+    shell_k, shell_ptr, shell_xyz, prim_exp, prim_coef); rng continues the
+    seeded stream for sampling."""
+    rng = np.random.default_rng(seed)
+    n = int(np.ceil(natom ** (1.0 / 3.0) - 1e-9))
+    sites = np.array([(i, j, k) for i in range(n) for j in range(n) for k in range(n)][:natom], np.float64)
+    xyz = sites * spacing + rng.uniform(-jitter, jitter, (natom, 3))
+    ls = np.array([l for _ in range(natom) for (l, _) in shells], np.int32)
+    ks = np.array([k for _ in range(natom) for (_, k) in shells], np.int32)
+    centres = np.repeat(xyz, len(shells), axis=0)
+    return (rng,) + make_shells(rng, ls, ks, alpha[0], alpha[1], 1.0, centres=centres)
+
+
+def sample_screened_quartets(q, pairs, nq, rng, threshold=1e-12):
+    """Uniform sample of nq of the unique quartets (pair i, pair j), j <= i in
+    the order of decreasing Schwarz factor q, whose bound q_i q_j reaches the
+    threshold.  q: per pair factor, pairs: [npair, 2] shell indices.  Returns
+    (quartets [n, 4] int32, number of such quartets)."""
+    order = np.argsort(-q, kind='stable')
+    qs, pr = q[order], pairs[order]
+    # row i pairs with the rows j <= i whose q_j >= threshold / q_i (a prefix: q sorted)
+    cnt = np.searchsorted(-qs, -(threshold / np.maximum(qs, 1e-300)), side='right')
+    m = np.minimum(cnt, np.arange(1, len(qs) + 1))
+    cm = np.cumsum(m)
+    total = int(cm[-1]) if len(cm) else 0
+    pos = np.sort(rng.choice(total, size=min(nq, total), replace=False))
+    row = np.searchsorted(cm, pos, side='right')
+    col = pos - (cm[row] - m[row])
+    quartets = np.concatenate([pr[row], pr[col]], axis=1).astype(np.int32)
+    return np.ascontiguousarray(quartets), total
+
