@@ -68,3 +68,39 @@ def test_pair_bound_covers_diagonal_integrals(sph):
                 if qb > 0.0:
                     worst = max(worst, lhs / qb)
     assert worst > 1e-3  # the bound is not vacuous
+
+
+def _device_constants(name):
+    """The literals of a constexpr chain `n == k ? v : ...` in the device header."""
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), '..', 'intception_b200', 'csrc', 'ib_eri_device.cuh')).read()
+    body = src[src.index(name):]
+    body = body[:body.index(';')]
+    return [float(x) for x in re.findall(r'[0-9]+\.[0-9]+(?:e[-+]?[0-9]+)?', body)]
+
+
+def test_device_norms_match_quadrature():
+    """The device's N_n (sqrt of the Coulomb self-energy of r^n exp(-r^2)) for
+    n = 0..12, against a direct quadrature of the spherical self-energy
+    4 pi int g(r) V(r) r^2 dr, V(r) = 4 pi (int_0^r g s^2 ds / r + int_r^inf g s ds)."""
+    from scipy import integrate
+    vals = _device_constants('ib_rn_norm(int n)')
+    assert len(vals) == 13
+    assert np.allclose(vals[:7], RN_NORM, rtol=1e-15)
+    for n in (0, 1, 3, 6, 9, 12):
+        g = lambda r, n=n: r ** n * np.exp(-r * r)  # noqa: E731
+        inner = lambda r: integrate.quad(lambda t: g(t) * t * t, 0, r, epsabs=0, epsrel=1e-13)[0]  # noqa: E731
+        outer = lambda r: integrate.quad(lambda t: g(t) * t, r, np.inf, epsabs=0, epsrel=1e-13)[0]  # noqa: E731
+        V = lambda r: 4 * np.pi * ((inner(r) / r if r > 0 else 0.0) + outer(r))  # noqa: E731
+        u = integrate.quad(lambda r: g(r) * V(r) * 4 * np.pi * r * r, 0, 12, epsabs=0, epsrel=1e-11, limit=200)[0]
+        assert abs(np.sqrt(u) - vals[n]) <= 1e-9 * vals[n], n
+
+
+def test_device_sph_colsums_cover_library_matrices():
+    vals = _device_constants('ib_sph_colsum(int l)')
+    # the chain lists l <= 1, 2, 3, 4, 5 and the l = 6 fallback
+    want = [float(np.abs(np.asarray(basis.sph_matrix(l))).sum(axis=0).max()) for l in range(1, 7)]
+    assert len(vals) == 6
+    for v, w in zip(vals, want):
+        assert v >= w and v <= w * (1 + 1e-12)
