@@ -380,10 +380,12 @@ __device__ __forceinline__ double ib_pair_q(const double* __restrict__ pe, const
 }
 
 // Power-of-two exponent e with Q <= 2^e (Q >= 0), clamped to [-127, 127];
-// 127 stands for "not small" (Q >= 2^126 never occurs for normalised shells,
-// and a primitive quartet with it is never skipped).
+// 127 stands for "not small": Q >= 2^126, infinite or NaN (never for
+// normalised shells; a primitive quartet with it is never skipped, so a NaN
+// input still reaches the result as on the exact path).
 __device__ __forceinline__ signed char ib_q_exp(double q) {
-  if (!(q > 0.0)) return -127;
+  if (q == 0.0) return -127;
+  if (!(q < 0x1p126)) return 127;
   const int e = ilogb(q) + 1;  // q < 2^(ilogb(q) + 1)
   return (signed char)max(-127, min(e, 127));
 }
@@ -430,7 +432,7 @@ __device__ __forceinline__ int2 ib_live_pairs_screened(const double* __restrict_
       if (t < m) {
         q = side ? ib_pair_q<LC, LD, SPH>(pe, pc, pcs, pd, kd, rcd2, p + t)
                  : ib_pair_q<LA, LB, SPH>(pe, pc, pa, pb, kb, rab2, p + t);
-        live = q > 0.0 && q * other >= tol;
+        live = !(q == 0.0 || q * other < tol);  // dropped only when provably small (NaN stays)
       }
       const unsigned bal = __ballot_sync(bmask, live) >> bbase;
       if (live) {
