@@ -69,7 +69,8 @@ def test_oracle_accurate_boys_mode():
     assert np.abs(loader.boys(int(z['nmax']), float(z['x'][0])) - z['F'][0]).max() <= 1e-15
 
 
-@pytest.mark.parametrize('ls',[(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 1, 1), (2, 1, 0, 1), (0, 2, 2, 1), (2, 2, 1, 1)])
+@pytest.mark.parametrize('ls', [(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 1, 1), (2, 1, 0, 1), (0, 2, 2, 1), (2, 2, 1, 1),
+                                (3, 0, 1, 0), (0, 3, 0, 1), (3, 1, 1, 0), (1, 0, 3, 2)])
 def test_oracle_vs_mcmurchie_davidson(ls):
     rng = np.random.default_rng(sum(ls) * 7 + 3)
     shells = []
