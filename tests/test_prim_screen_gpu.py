@@ -127,3 +127,23 @@ def test_schwarz_factors_ignore_prim_tol():
     finally:
         eri.set_prim_tol(0.0)
     assert torch.equal(q0, q1)
+
+
+def test_screened_with_fp32_tier_meets_error_bar():
+    """Primitive screening together with the FP32 tier (every class's FP32
+    kernel on, all quartets in the tier): within 1e-10 of the oracle."""
+    import torch
+    b = _orderings(151, 2, True, 0.05, 1e4, 6.0, 6)
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    eri.set_prim_tol(1e-18)
+    eri.set_class_fp32(True)
+    try:
+        eng = eri.EriEngine(b)
+        bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+        out = eng.compute(precision=eri.PREC_MIXED, bounds=bounds, fp32_below=2.0, mixed_tol=5e-11)
+        torch.cuda.synchronize()
+        assert eng.device_status() == 0
+    finally:
+        eri.set_prim_tol(0.0)
+        eri.set_class_fp32(None)
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-10
