@@ -171,9 +171,9 @@ def live_pairs(batch, i, j):
 
 
 def alg_flops(batch):
-    """Algorithmic FP64 work of one step (see DESIGN: per primitive quartet the
-    emitted VRR count plus geometry and Boys; per quartet the HRR and the
-    spherical transform), from the emitter's per-class counts."""
+    """Algorithmic FP64 work of one step: per live primitive quartet the
+    canonical VRR count plus 74 + 2L for geometry and Boys; per quartet the HRR
+    and the spherical transform counts; from the emitter's per-class table."""
     with open(os.path.join(ROOT, 'intception_b200', 'class_stats.json')) as fh:
         stats = {s['cid']: s for s in json.load(fh)}
     ls = batch.shell_l[batch.quartets].astype(np.int64)

@@ -245,9 +245,21 @@ int intception_b200_batch_status(void);
  * device looks up those arrays and copies the Boys and spherical tables into
  * them (a synchronous copy): make that first call before any stream capture.
  * Calls share the arrays, so calls whose work overlaps on the GPU (unordered
- * streams) race; order them.  Asynchronous on stream (NULL = legacy default). */
+ * streams) race; order them.  Asynchronous on stream (NULL = legacy default).
+ * The return value covers the host-side checks and the launches; errors found
+ * on the device go to a status word of its own, read with
+ * intception_b200_noalloc_status.  A quartet with an l outside
+ * [0, basis->lmax] sets IB_ERR_ARG there and, as in intception_b200_eri_batch,
+ * is evaluated as (ss|ss) of its shells: the first element of its block is
+ * written, nothing else. */
 int intception_b200_eri_batch_noalloc(const intception_b200_basis *basis, const int *quartets,
                                       const long long *out_off, int nq, int spherical, double *out, void *stream);
+
+/* Device status word of intception_b200_eri_batch_noalloc on the current
+ * device (IB_OK, IB_ERR_ARG for an l out of range, IB_ERR_SCRATCH): waits for
+ * stream, then reads the word of the last call.  Allocates nothing; IB_OK
+ * before the first call.  No counterpart in the reference. */
+int intception_b200_noalloc_status(void *stream);
 
 /* Density digestion (device pointers, asynchronous on stream).  quartets are
  * unique shell quartets (a>=b, c>=d, each pair-pair once), standing for their
@@ -283,6 +295,15 @@ int intception_b200_jk_force(const int *quartets, const int *qidx, const long lo
 int intception_b200_twoidx_batch(int kind, int n, int lmax, const double *xa, const double *ca, const int *la,
                                  const double *xb, const double *cb, const int *lb, const double *cc,
                                  const long long *off, double *out, int *status, void *stream);
+
+/* Testing the two-index kernel's bounded waits (no counterpart in the
+ * reference): the next intception_b200_twoidx_batch call announces chunk
+ * `chunk`'s bytes (IB2 chunks of 512 pairs, fetched by bulk copies when every
+ * input array is 16-byte aligned) on its barrier but issues no copy for it,
+ * and polls wait_iters times (1 .. 1 << 22) before it gives up.  The block
+ * owning that chunk then stores IB_ERR_TIMEOUT in *status, waits for its other
+ * copies in flight and returns without writing its pairs.  One-shot. */
+int intception_b200_twoidx_test_stall(long long chunk, int wait_iters);
 
 /* The library's Cartesian->spherical matrix for l (host memory,
  * T[icart + isph*ncart], ncart x (2l+1)). */

@@ -51,10 +51,11 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
   for (int p = beg + blockIdx.x; p < end; p += gridDim.x) {
     if (tid == 0) {
       const IbItem it = a.items[p];
+      const bool bad = it.st[0] == 0;  // an l out of range: evaluated as (ss|ss), the status already says so
       int l[4];
       for (int i = 0; i < 4; ++i) {
         const int s = it.s[i];
-        l[i] = a.shell_l[s];
+        l[i] = bad ? 0 : a.shell_l[s];
         sh.k[i] = a.shell_k[s];
         sh.ptr[i] = a.shell_ptr[s];
         sh.st[i] = it.st[i];

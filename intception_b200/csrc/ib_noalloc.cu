@@ -16,7 +16,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/intception_b200.h"
@@ -86,22 +88,30 @@ int noalloc_setup(int dev, NoallocDevice** out) {
 __device__ __forceinline__ int na_pair(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
 // One descriptor per quartet, in the caller's order, with the canonical shell
-// permutation (la >= lb, lc >= ld, bra pair >= ket pair) and the output strides
-// that undo it; the generic range covers all of them.
+// permutation (la >= lb, lc >= ld, bra pair >= ket pair; within a pair of
+// equal l the more compact shell first, as the batch path orders them) and the
+// output strides that undo it; the generic range covers all of them.  A
+// quartet with an l outside [0, lmax] sets IB_ERR_ARG and is marked
+// (st[0] = 0): the generic kernel then writes the (ss|ss) value of its shells
+// into the first element of its block, as the batch path does.
 __global__ void ib_noalloc_items_kernel(const int* __restrict__ quartets, const int* __restrict__ shell_l,
-                                        const long long* __restrict__ out_off, int nq, int spherical, int lmax,
-                                        IbItem* __restrict__ items, int* __restrict__ ranges, int* status) {
+                                        const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                        const double* __restrict__ prim_exp, const long long* __restrict__ out_off,
+                                        int nq, int spherical, int lmax, IbItem* __restrict__ items,
+                                        int* __restrict__ ranges, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], n[4];
+    bool bad = false;
     for (int i = 0; i < 4; ++i) {
       s[i] = quartets[4 * q + i];
       l[i] = shell_l[s[i]];
-      if (l[i] < 0 || l[i] > lmax) {
-        atomicExch(status, IB_ERR_ARG);
-        l[i] = 0;
-      }
-      n[i] = spherical ? 2 * l[i] + 1 : (l[i] + 1) * (l[i] + 2) / 2;
+      bad |= (l[i] < 0) | (l[i] > lmax);
     }
+    if (bad) {
+      atomicExch(status, IB_ERR_ARG);
+      for (int i = 0; i < 4; ++i) l[i] = 0;
+    }
+    for (int i = 0; i < 4; ++i) n[i] = spherical ? 2 * l[i] + 1 : (l[i] + 1) * (l[i] + 2) / 2;
     int st[4] = {1, n[0], n[0] * n[1], n[0] * n[1] * n[2]};
     if (l[0] < l[1]) {
       int t = s[0]; s[0] = s[1]; s[1] = t;
@@ -120,11 +130,13 @@ __global__ void ib_noalloc_items_kernel(const int* __restrict__ quartets, const 
         t = st[k]; st[k] = st[k + 2]; st[k + 2] = t;
       }
     }
+    if (!bad) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);
     IbItem it;
     for (int i = 0; i < 4; ++i) {
       it.s[i] = s[i];
       it.st[i] = st[i];
     }
+    if (bad) it.st[0] = 0;
     it.off = out_off[q];
     items[q] = it;
     if (q == 0) {
@@ -145,27 +157,37 @@ long long noalloc_slice(int lmax) {
 
 }  // namespace
 
+int ib_runtime_set_status(int st, const char* msg);
+
 extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* basis, const int* quartets,
                                                  const long long* out_off, int nq, int spherical, double* out,
                                                  void* stream) {
-  if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out))) return IB_ERR_ARG;
-  if (nq > IB_NOALLOC_MAX_QUARTETS) return IB_ERR_ARG;  // more quartets than the static descriptor array holds
-  if (basis->lmax < 0 || basis->lmax > IB_LMAX) return IB_ERR_ARG;
-  if (nq == 0) return IB_OK;
+  if (!basis || nq < 0 || (nq > 0 && (!quartets || !out_off || !out)))
+    return ib_runtime_set_status(IB_ERR_ARG, "eri_batch_noalloc: null argument");
+  if (nq > IB_NOALLOC_MAX_QUARTETS)  // more quartets than the static descriptor array holds
+    return ib_runtime_set_status(IB_ERR_ARG, "eri_batch_noalloc: more than 65536 quartets");
+  if (basis->lmax < 0 || basis->lmax > IB_LMAX)
+    return ib_runtime_set_status(IB_ERR_ARG, "eri_batch_noalloc: basis lmax out of range");
+  if (nq == 0) return ib_runtime_set_status(IB_OK, "");
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IB_ERR_NODEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return ib_runtime_set_status(IB_ERR_NODEVICE, "eri_batch_noalloc: no CUDA device");
   NoallocDevice* d = nullptr;
   int st = noalloc_setup(dev, &d);
-  if (st) return st;
+  if (st) return ib_runtime_set_status(st, "eri_batch_noalloc: set-up of the static arrays failed");
   const long long slice = noalloc_slice(basis->lmax);
   const long long fit = (long long)(IB_NOALLOC_SCRATCH_DOUBLES / (size_t)slice);
-  if (fit < 1) return IB_ERR_SCRATCH;  // one quartet's recurrence levels exceed the static scratch
+  if (fit < 1)  // one quartet's recurrence levels exceed the static scratch
+    return ib_runtime_set_status(IB_ERR_SCRATCH, "eri_batch_noalloc: one quartet needs more than 32 MiB");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (cudaMemsetAsync(d->status, 0, sizeof(int), s) != cudaSuccess) return IB_ERR_CUDA;
+  if (cudaMemsetAsync(d->status, 0, sizeof(int), s) != cudaSuccess)
+    return ib_runtime_set_status(IB_ERR_CUDA, "eri_batch_noalloc: clearing the status word failed");
   const int tb = 256, nb = std::min((nq + tb - 1) / tb, 4 * d->nsm);
-  ib_noalloc_items_kernel<<<nb, tb, 0, s>>>(quartets, basis->shell_l, out_off, nq, spherical ? 1 : 0, basis->lmax,
-                                            d->items, d->ranges, d->status);
+  ib_noalloc_items_kernel<<<nb, tb, 0, s>>>(quartets, basis->shell_l, basis->shell_k, basis->shell_ptr,
+                                            basis->prim_exp, out_off, nq, spherical ? 1 : 0, basis->lmax, d->items,
+                                            d->ranges, d->status);
   IbLaunch a;
+  memset(&a, 0, sizeof(a));
   a.items = d->items;
   a.ranges = d->ranges;
   a.shell_l = basis->shell_l;
@@ -178,7 +200,33 @@ extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* ba
   a.sph = d->sph;
   a.out = out;
   a.status = d->status;
+  a.slice_boost = 1;
   const long long grid = std::min<long long>({(long long)nq, 2LL * d->nsm, fit});
   ib_eri_generic<<<(int)grid, IB_GEN_BLOCK, 0, s>>>(a, kNoallocSlot, spherical ? 1 : 0, d->scratch, slice);
-  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return ib_runtime_set_status(IB_ERR_CUDA, (std::string("eri_batch_noalloc: ") + cudaGetErrorString(e)).c_str());
+  return ib_runtime_set_status(IB_OK, "");
+}
+
+// Device status word of the allocation-free entry on the current device: waits
+// for stream, then reads it (IB_OK, IB_ERR_ARG for an l out of range,
+// IB_ERR_SCRATCH).  Allocates nothing.
+extern "C" int intception_b200_noalloc_status(void* stream) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return ib_runtime_set_status(IB_ERR_NODEVICE, "noalloc_status: no CUDA device");
+  NoallocDevice* d = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_dev[dev].ready) return ib_runtime_set_status(IB_OK, "");  // no call on this device yet
+    d = &g_dev[dev];
+  }
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d->status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess)
+    return ib_runtime_set_status(IB_ERR_CUDA, (std::string("noalloc_status: ") + cudaGetErrorString(e)).c_str());
+  ib_runtime_set_status(IB_OK, "");
+  return h;
 }

@@ -122,6 +122,7 @@ struct Context {
   DevBuf counters;  // per class kernel launch of a batch: the next quartet (FP64, FP32, FP64 recheck passes)
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;                                             // FP32 rejections of the last mixed batch
+  int flags_nq = 0;                                         // its quartet count (flags beyond it are stale)
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
   int kind_h[IB_NCLASS] = {};  // host copy of kind: 2 where the class has FP32 kernels and the FP32 tier uses them
   DevBuf d_stage, d_cart, d_res;
@@ -191,31 +192,6 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | (unsigned(cid) << 4) |
               unsigned(15 - work);
     vals[q] = q;
-  }
-}
-
-// Smallest primitive exponent of shell s.
-__device__ __forceinline__ double ib_min_exp(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
-                                             const double* __restrict__ prim_exp, int s) {
-  const int k = __ldg(shell_k + s), p0 = __ldg(shell_ptr + s);
-  double m = __ldg(prim_exp + p0);
-  for (int i = 1; i < k; ++i) m = fmin(m, __ldg(prim_exp + p0 + i));
-  return m;
-}
-
-// Within a pair of equal l, the shell the vertical recurrence builds on comes
-// first: the more compact one (larger smallest exponent).  The product centre
-// then lies near it, the [e0| and |f0] intermediates stay small, and the
-// horizontal recurrence cancels fewer digits (measured: intermediates of 2e3
-// for a block of 1e-2 with the diffuse shell first, 6e-2 with the compact one).
-__device__ __forceinline__ void ib_compact_first(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
-                                                 const double* __restrict__ prim_exp, int* s, const int* l, int* st) {
-  for (int i = 0; i < 4; i += 2) {
-    if (l[i] != l[i + 1] || s[i] == s[i + 1]) continue;
-    if (ib_min_exp(shell_k, shell_ptr, prim_exp, s[i]) < ib_min_exp(shell_k, shell_ptr, prim_exp, s[i + 1])) {
-      int t = s[i]; s[i] = s[i + 1]; s[i + 1] = t;
-      t = st[i]; st[i] = st[i + 1]; st[i + 1] = t;
-    }
   }
 }
 
@@ -903,6 +879,7 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   if (precision == IB_PREC_MIXED) {
     IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
     IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
+    c->flags_nq = nq;
     a.flags = c->flags.as<int>();
     a.mixed_tol = mixed_tol;
   }
@@ -1164,9 +1141,10 @@ int intception_b200_eri_graph_destroy(void* handle) {
 int intception_b200_last_fp32_rejections(void) {
   Context* c = nullptr;
   if (get_context(&c)) return -1;
-  if (!c->flags.p) return 0;
+  if (!c->flags.p || c->flags_nq <= 0) return 0;
   IB_CUDA(cudaDeviceSynchronize());
-  const size_t n = c->flags.cap / sizeof(int);
+  // only the last mixed batch's flags: the buffer keeps stale entries past them
+  const size_t n = std::min((size_t)c->flags_nq, c->flags.cap / sizeof(int));
   std::vector<int> h(n);
   IB_CUDA(cudaMemcpy(h.data(), c->flags.p, n * sizeof(int), cudaMemcpyDeviceToHost));
   int k = 0;

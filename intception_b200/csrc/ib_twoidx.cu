@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "../../include/intception_b200.h"
@@ -59,6 +60,8 @@ struct Ib2Args {
   int* status;
   int lthr;  // lane-group kernels: pairs with max(la, lb) <= lthr belong to the thread-per-pair kernels
   int bulk_ok;  // thread-per-pair kernel: every input array 16-byte aligned (complete chunks by bulk copy)
+  long long stall_chunk;  // testing: this chunk's barrier is armed but its copies are not issued (-1: none)
+  int wait_iters;         // iterations of a bounded wait for a chunk's copies (1 << 22: about 0.4 s)
 };
 
 __host__ __device__ __forceinline__ int ib2_ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -499,6 +502,7 @@ __device__ __forceinline__ void ib2_issue(const Ib2Args& a, Ib2Buf<KIND>& bf, lo
   const unsigned bytes = 3 * n8 + 2 * n4 + 2 * n24 + (KIND == 1 ? n24 : 0);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+  if (ch == a.stall_chunk) return;  // testing: bytes announced that no copy delivers; the wait gives up
 #define IB2_BULK(dst, src, nb)                                                                                  \
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"( \
                    ib2_smem_addr(dst)),                                                                         \
@@ -515,11 +519,12 @@ __device__ __forceinline__ void ib2_issue(const Ib2Args& a, Ib2Buf<KIND>& bf, lo
 #undef IB2_BULK
 }
 
-// Bounded wait for phase `parity` of the mbarrier at mb: false after about
-// 0.4 s without completion (a copy that never lands), so that the block can
-// report the error and return instead of spinning on.
-__device__ __forceinline__ bool ib2_wait(unsigned mb, unsigned parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+// Bounded wait for phase `parity` of the mbarrier at mb: false after `iters`
+// polls without completion (1 << 22 of them, about 0.4 s: a copy that never
+// lands), so that the block can report the error and return instead of
+// spinning on.
+__device__ __forceinline__ bool ib2_wait(unsigned mb, unsigned parity, int iters) {
+  for (int it = 0; it < iters; ++it) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}"
@@ -600,12 +605,12 @@ __global__ void __launch_bounds__(IB2_TPB, 2) ib2_thread_kernel(const Ib2Args a)
     const int p0 = (int)(ch * IB2_CHUNK);
     const int np = min(IB2_CHUNK, a.n - p0);
     if (ch < nfull) {
-      const bool ok = ib2_wait(mb_this, (k >> 1) & 1);
+      const bool ok = ib2_wait(mb_this, (k >> 1) & 1, a.wait_iters);
       if (__syncthreads_or(!ok)) {  // uniform: report, drain the copies still in flight, stop
         if (threadIdx.x == 0) {
           if (a.status) atomicExch(a.status, IB_ERR_TIMEOUT);
-          ib2_wait(mb_this, (k >> 1) & 1);
-          if (nxt < nfull) ib2_wait(mb_next, ((k + 1) >> 1) & 1);
+          ib2_wait(mb_this, (k >> 1) & 1, a.wait_iters);
+          if (nxt < nfull) ib2_wait(mb_next, ((k + 1) >> 1) & 1, a.wait_iters);
         }
         return;
       }
@@ -777,6 +782,13 @@ int grid_for(K kernel, size_t smem, int n, int groups, int nsm) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+// Testing knob for the bounded waits (intception_b200_twoidx_test_stall): the
+// next intception_b200_twoidx_batch call leaves one chunk's copies unissued
+// and waits `iters` polls for them.  Read and cleared by that call.
+std::atomic<long long> g_stall_chunk{-1};
+std::atomic<int> g_stall_iters{0};
+constexpr int kWaitIters = 1 << 22;
+
 int launch(int kind, const Ib2Args& a0, int nsm, cudaStream_t s) {
   // every pair passes the thread-per-pair kernel (which also flags invalid
   // pairs); pairs with max(la, lb) > IB2_LT then take the lane-group kernel
@@ -867,7 +879,9 @@ void single_pair(int kind, double xa, const double* cA, int la, int na, int iski
   h.l[0] = la;
   h.l[1] = lb;
   h.off = 0;
-  Ib2Args a;
+  Ib2Args a = {};
+  a.stall_chunk = -1;
+  a.wait_iters = kWaitIters;
   a.lthr = -1;
   a.n = 1;
   a.lmax = std::max(la, lb);
@@ -953,7 +967,10 @@ int intception_b200_twoidx_batch(int kind, int n, int lmax, const double* xa, co
   TwoIdxDevice* d = nullptr;
   int st = twoidx_setup(&d);
   if (st) return st;
-  Ib2Args a;
+  Ib2Args a = {};
+  a.stall_chunk = g_stall_chunk.exchange(-1);
+  a.wait_iters = g_stall_iters.exchange(0);
+  if (a.wait_iters <= 0) a.wait_iters = kWaitIters;
   a.lthr = -1;
   a.n = n;
   a.lmax = lmax;
@@ -970,6 +987,15 @@ int intception_b200_twoidx_batch(int kind, int n, int lmax, const double* xa, co
   a.status = status;
   st = launch(kind, a, d->nsm, static_cast<cudaStream_t>(stream));
   if (st) return ib_runtime_set_status(st, "twoidx_batch: launch failed");
+  return ib_runtime_set_status(IB_OK, "");
+}
+
+// Testing the bounded waits: see the header.
+int intception_b200_twoidx_test_stall(long long chunk, int wait_iters) {
+  if (chunk < 0 || wait_iters < 1 || wait_iters > kWaitIters)
+    return ib_runtime_set_status(IB_ERR_ARG, "twoidx_test_stall: chunk >= 0, 1 <= wait_iters <= 1 << 22");
+  g_stall_iters.store(wait_iters);
+  g_stall_chunk.store(chunk);
   return ib_runtime_set_status(IB_OK, "");
 }
 

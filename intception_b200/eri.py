@@ -103,6 +103,8 @@ def load():
     lib.intception_b200_eri_batch_noalloc.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int,
                                                       C.c_int, C.c_void_p, C.c_void_p]
     lib.intception_b200_eri_batch_noalloc.restype = C.c_int
+    lib.intception_b200_noalloc_status.argtypes = [C.c_void_p]
+    lib.intception_b200_noalloc_status.restype = C.c_int
     lib.intception_b200_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
     lib.intception_b200_fma_peak.restype = C.c_int
     lib.intception_b200_set_slice_cap.argtypes = [C.c_int, C.c_int]

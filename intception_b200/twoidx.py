@@ -37,6 +37,8 @@ def _lib():
             f.restype = C.c_int
         lib.intception_b200_twoidx_batch.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 11
         lib.intception_b200_twoidx_batch.restype = C.c_int
+        lib.intception_b200_twoidx_test_stall.argtypes = [C.c_longlong, C.c_int]
+        lib.intception_b200_twoidx_test_stall.restype = C.c_int
         _bound.append(True)
     return lib
 

@@ -15,8 +15,10 @@ is the C99 it emits for an ERI input script.  This recipe
      across several objects) together with the OpenMP batch driver
      ``oracle/ref_batch.c`` into ``oracle/_ref/libref_eri_{cart,sph}.so``.
 
-Usage:  python oracle/gen_ref.py [--reference /root/reference] [--lmax 6]
-Nothing here runs on the GPU box: the built ``oracle/_ref`` travels with the tree.
+Usage:  python oracle/gen_ref.py [--reference PATH] [--lmax 6]
+The reference tree is --reference, else $INTCEPTION_REFERENCE, else the
+read-only mount this recipe was written for (``reference_root()``).  Nothing
+here runs on the GPU box: the built ``oracle/_ref`` travels with the tree.
 """
 import argparse
 import os
@@ -25,6 +27,13 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, '_ref')
+_DEFAULT_REFERENCE = '/root/reference'  # where this recipe reads the reference tree unless told otherwise
+
+
+def reference_root():
+    """The reference source tree: $INTCEPTION_REFERENCE, else the default
+    mount.  Callers check os.path.isdir(<root>/src/intception) themselves."""
+    return os.environ.get('INTCEPTION_REFERENCE', _DEFAULT_REFERENCE)
 
 
 def generate(reference, variant, lmax):
@@ -51,10 +60,10 @@ def compile_variant(outdir, variant):
             fh.write('#include "%s"\n' % s)
         # OpenMP batch driver: the emitted per-quartet function called from C,
         # no Python in the timed loop
-        fh.write('#include "%s"\n' % os.path.join(HERE, 'ref_batch.c'))
+        fh.write('#include "ref_batch.c"\n')
     so = os.path.join(REF_OUT, 'libref_eri_%s.so' % variant)
     cmd = ['gcc', '-std=gnu99', '-O3', '-march=native', '-fPIC', '-shared', '-fopenmp', '-w',
-           '-DREF_VARIANT_%s' % variant.upper(), '-I', outdir, unity, '-o', so, '-lm']
+           '-DREF_VARIANT_%s' % variant.upper(), '-I', outdir, '-I', HERE, unity, '-o', so, '-lm']
     subprocess.run(cmd, check=True)
     return so
 
@@ -76,16 +85,16 @@ def build_example(reference):
         fh.write('#include <math.h>\n')
         for s in srcs:
             fh.write('#include "%s"\n' % s)
-        fh.write('#include "%s"\n' % os.path.join(HERE, 'ref_batch_2idx.c'))
+        fh.write('#include "ref_batch_2idx.c"\n')
     so = os.path.join(REF_OUT, 'libref_2idx.so')
     subprocess.run(['gcc', '-std=gnu99', '-O3', '-march=native', '-fPIC', '-shared', '-fopenmp', '-w', '-I', outdir,
-                    unity, '-o', so, '-lm'], check=True)
+                    '-I', HERE, unity, '-o', so, '-lm'], check=True)
     return so
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', default=reference_root())
     ap.add_argument('--lmax', type=int, default=6)
     args = ap.parse_args()
     if not os.path.isdir(os.path.join(args.reference, 'src', 'intception')):

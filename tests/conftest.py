@@ -34,8 +34,8 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
-BATCH_FIXTURES = ['pppp_k3_cart', 'mixed_l2_sph_c2', 'mixed_l2_sph_compact', 'mixed_l2_cart_compact', 'l4_cart',
-                  'l4_sph', 'l6_cart', 'l6_sph', 'edge_cart', 'edge_sph']
+BATCH_FIXTURES = ['pppp_k3_cart', 'c1_pppp_k3_cart_4096', 'mixed_l2_sph_c2', 'mixed_l2_sph_compact',
+                  'mixed_l2_cart_compact', 'l4_cart', 'l4_sph', 'l6_cart', 'l6_sph', 'edge_cart', 'edge_sph']
 
 
 def load_batch(name):
@@ -71,6 +71,8 @@ def load_dropin_cases():
 
 
 def tolerance(ref):
-    """FP64 parity bar: 1e-12 absolute, loosened only relative to the block's
-    magnitude for the high-l fixtures whose values exceed 1."""
-    return 1e-12 * max(1.0, float(np.abs(ref).max()))
+    """FP64 parity bar: a flat 1e-12 absolute wherever max |I| <= 10 (every ERI
+    fixture: the largest, edge_*, reaches 1.63); above 10 the bar becomes
+    1e-13 relative to max |I| (1e-12 absolute would ask for 16 digits)."""
+    m = float(np.abs(ref).max()) if np.size(ref) else 0.0
+    return 1e-12 if m <= 10.0 else 1e-13 * m

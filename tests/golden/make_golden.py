@@ -2,7 +2,8 @@
 
 Run in a container that has the reference tree (it builds oracle/_ref first):
     python oracle/gen_ref.py && python tests/golden/make_golden.py
-(``make_golden.py twoidx`` writes only twoidx.npz.)
+(``make_golden.py twoidx`` writes only twoidx.npz, ``make_golden.py c1`` only
+c1_pppp_k3_cart_4096.npz.)
 
 Every fixture stores seeded inputs (shell table, quartets, spherical matrices)
 and the outputs of intception_integral_eri_abcd_m_cont_{cart,sph}_main as
@@ -223,9 +224,21 @@ def twoidx():
           % (np.abs(ov).max(), np.abs(nu).max()))
 
 
+def c1():
+    """c1_pppp_k3_cart_4096.npz: the (pp|pp) K=3 Cartesian configuration at its
+    full size, 4096 quartets of four fresh shells, seed 0, through the
+    reference's emitted _cont_cart function."""
+    T = basis.sph_matrices(6)
+    b = basis.config_pppp_k3(nq=4096, seed=0)
+    save_batch('c1_pppp_k3_cart_4096.npz', b, T, ref(b, T))
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['twoidx']:
         twoidx()
+    elif sys.argv[1:] == ['c1']:
+        c1()
     else:
         main()
         twoidx()
+        c1()

@@ -43,3 +43,19 @@ def test_exported_symbols_have_c_linkage():
 def test_load_binds_every_entry_point():
     lib = eri.load()  # sets argtypes on the entry points the Python layer calls; no device work
     assert lib.intception_b200_set_slice_cap.restype is ctypes.c_int
+
+
+def test_library_work_array_size_matches_reference_golden():
+    """The library's own exported ..._work_array_size (the drop-in callers size
+    work_array with it, contracted_general.py:240-502) on the 1875 argument
+    sets the reference's emitted C99 answered in tests/golden/work_array_size.npz;
+    host-only, no device work."""
+    import numpy as np
+    from conftest import GOLDEN
+    t = np.load(os.path.join(GOLDEN, 'work_array_size.npz'))['table']
+    lib = eri.load()
+    for v in ('cart', 'sph'):
+        f = getattr(lib, 'intception_integral_eri_abcd_m_cont_%s_work_array_size' % v)
+        got = np.array([f(*map(int, r[:12])) for r in t])
+        assert np.array_equal(got, t[:, 12]), v
+        assert eri.work_array_size(*map(int, t[7, :12]), spherical=(v == 'sph')) == t[7, 12]

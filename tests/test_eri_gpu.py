@@ -432,3 +432,49 @@ def test_host_pipeline_matches_direct_batches():
     pipe.submit(h, o, skip_below=1e-12)
     pipe.synchronize()
     assert np.array_equal(o.numpy(), ref)
+
+
+def test_fp32_rejection_count_covers_only_the_last_batch():
+    """intception_b200_last_fp32_rejections counts the flags of the last mixed
+    batch only: a large batch whose every FP32 attempt is rejected, then a
+    smaller one that rejects nothing, must report 0 (the flag buffer still
+    holds the large batch's flags past the small batch's end)."""
+    import torch
+    big = _all_l2_orderings(123, True, kmax=4, copies=4)
+    small = big.subset(np.arange(40))
+    try:
+        eri.set_class_fp32(True)
+        for b, tol, want_any in ((big, 1e-300, True), (small, 1.0, False)):
+            eng = eri.EriEngine(b)
+            bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+            eng.compute(precision=eri.PREC_MIXED, bounds=bounds, fp32_below=2.0, mixed_tol=tol)
+            torch.cuda.synchronize()
+            assert eng.device_status() == 0
+            n = eng.fp32_rejected()
+            assert (n > 0) if want_any else (n == 0), n
+            assert n <= b.nq
+    finally:
+        eri.set_class_fp32(None)
+
+
+def test_c1_every_quartet_through_the_dropin():
+    """The (pp|pp) K=3 Cartesian configuration at its full size (4096
+    quartets, seed 0): every quartet through the drop-in
+    intception_integral_eri_abcd_m_cont_cart_main, one call per quartet as the
+    reference's caller makes them, against the reference's emitted C99 at a
+    flat 1e-12 absolute; the batch entry covers the same fixture in
+    test_batch_matches_reference_golden."""
+    b, T, ref = load_batch('c1_pppp_k3_cart_4096')
+    assert b.nq == 4096
+    worst = 0.0
+    for q in range(b.nq):
+        shells = []
+        for i, s in enumerate(b.quartets[q]):
+            p0, k = int(b.shell_ptr[s]), int(b.shell_k[s])
+            shells.append(dict(x=b.prim_exp[p0:p0 + k], cen=b.shell_xyz[s], coef=b.prim_coef[p0:p0 + k], l=1, n=3,
+                               iskip=3 ** i, nprim=k, ncont=1, iskip_cont=81))
+        out = np.zeros(81)
+        eri.cont_cart_main(shells, out)
+        r = ref[b.out_off[q]:b.out_off[q] + 81]
+        worst = max(worst, float(np.abs(out - r).max()))
+    assert worst <= 1e-12, worst

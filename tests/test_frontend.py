@@ -11,7 +11,10 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SRC = '/root/reference/src'
+sys.path.insert(0, ROOT)
+from oracle import gen_ref  # noqa: E402
+
+REF_SRC = os.path.join(gen_ref.reference_root(), 'src')
 
 pytestmark = pytest.mark.skipif(not os.path.isdir(os.path.join(REF_SRC, 'intception')),
                                 reason='reference generator not available here')

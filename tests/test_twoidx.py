@@ -256,3 +256,38 @@ def test_batch_bulk_copied_chunks_vs_oracle(kind):
     got2 = batch.compute(kind).cpu().numpy()
     assert batch.device_status() == 0
     assert np.array_equal(got, got2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('kind', [0, 1])
+def test_bounded_wait_gives_up_and_reports_timeout(kind):
+    """The thread kernel's wait for a chunk's bulk copies is bounded: with the
+    testing knob, chunk 0's bytes are announced on its barrier but never
+    copied, the block gives up after 2^14 polls, stores IB_ERR_TIMEOUT, drains
+    its other copies and returns.  Chunk 0's pairs stay untouched, every other
+    chunk is correct, and the knob is one-shot."""
+    import torch
+    from intception_b200 import twoidx
+    from oracle import loader
+    pairs = twoidx.make_pairs(8 * 512, 2, seed=5, box=6.0)
+    pairs['off'], pairs['size'] = twoidx.block_offsets(pairs['la'], pairs['lb'])
+    ref = loader.twoidx_batch(kind, {k: np.asarray(v).reshape(-1) if k in ('ca', 'cb', 'cc') else v
+                                     for k, v in pairs.items()})
+    batch = twoidx.TwoIndexBatch(pairs)
+    out = torch.full((batch.size,), -7.0, dtype=torch.float64, device='cuda')
+    assert twoidx._lib().intception_b200_twoidx_test_stall(0, 1 << 14) == 0
+    batch.compute(kind, out=out)
+    torch.cuda.synchronize()
+    assert batch.device_status() == twoidx._eri.IB_ERR_TIMEOUT
+    got = out.cpu().numpy()
+    blocks = _blocks(pairs)
+    for i, (b, e) in enumerate(blocks):
+        if i < 512:
+            assert np.all(got[b:e] == -7.0)
+        else:
+            assert np.abs(got[b:e] - ref[b:e]).max() <= 1e-12 * max(1.0, float(np.abs(ref[b:e]).max()))
+    batch.status.zero_()
+    batch.compute(kind, out=out)
+    torch.cuda.synchronize()
+    assert batch.device_status() == 0
+    _assert_blocks(out.cpu().numpy(), ref, pairs, 1e-12)
