@@ -1,25 +1,41 @@
-"""Benchmark: contracted ERI quartets/s on one B200 (or N, weak scaling).
+"""Benchmark: contracted ERI quartets/s on one B200 (or N, one batch split).
 
 Workload (one step = one pass of the ERI path over one batch):
   1e6 shell quartets, l in {0,1,2} per shell (class uniform over the 81
   (la,lb,lc,ld) classes), K uniform in {1..6} per shell, exponents log-uniform
   in [0.05, 1e4], coefficients uniform [0.1, 1] then normalised, centres
-  uniform in a 30-bohr cube, spherical output, seed 1 (rank r uses seed 1+r).
-  Synthetic data with the shapes of that configuration.
+  uniform in a 30-bohr cube, spherical output, seed 1.  Synthetic data with
+  the shapes of that configuration.  With N GPUs the same batch is split into
+  N cost-balanced contiguous shards of its class-sorted quartet list
+  (intception_b200.shard), one per rank: strong scaling, no collective on the
+  data path.
+
+Paths timed per step, every step a complete pass (screening bounds included):
+  fp64_exact     every quartet evaluated in FP64 (the drop-ins' semantics)
+  fp64_screened  analytic quartet bounds on the device, blocks with bound
+                 < 1e-12 written as zeros, primitive quartets with bound
+                 < 1e-18 skipped, the rest in FP64
+  mixed          the same screening, FP32 VRR for kept quartets with bound
+                 below fp32_below (tuned over a sweep, then measured again),
+                 its rounding-error bound checked, rejected quartets in FP64
+value = the mixed path (the product's batched path); mixed_over_fp64 compares
+it with fp64_screened, which does the same screening.
 
 --workload nuclear_2idx | overlap_2idx times the reference example script's
-two-index classes instead (4e6 primitive pairs, l <= 2; one launch per step).
+two-index classes instead (4e6 primitive pairs, l <= 2; one launch per step);
+--workload lattice_l3 a sample of the 200-atom l <= 3 lattice.
 
 Arms:
-  default          : this library, FP64 path and mixed-precision path
+  default          : this library
   --impl reference : the reference's own CPU implementation of the path (the
                      C99 its generator emits, oracle/_ref, OpenMP over the
-                     box's cores) on a bounded sample of the same workload.
+                     box's cores) behind the same screening, on a bounded
+                     sample of the same workload.
 
-Prints one JSON line (rank 0).  value = quartets/s of the headline path over
-all ranks, device-timed with inputs resident in HBM (inputs + outputs ~1 GB,
-larger than L2, so no flush is needed); e2e = the same through the public API
-with host buffers and the H2D/D2H copies inside the timed region.
+Prints one JSON line (rank 0).  Device-timed with inputs resident in HBM
+(inputs + outputs ~1 GB, larger than L2, so no flush is needed); e2e = the
+same through the public API with host buffers and the H2D/D2H copies inside
+the timed region.
 """
 import argparse
 import json
@@ -37,7 +53,7 @@ sys.path.insert(0, ROOT)
 METRIC = 'contracted ERI quartets/s on B200: mixed-prec vs FP64 at <=1e-10 max abs err'
 WORKLOAD = ('1e6 quartets, l<=2 per shell (81 classes uniform), K in 1..6, alpha log-uniform [0.05,1e4], '
             '30-bohr cube, spherical, seed 1')
-SKIP_BELOW = 1e-12      # Schwarz screening: blocks with a smaller bound are written as zeros
+SKIP_BELOW = 1e-12      # screening: blocks whose bound is smaller are written as zeros
 FP32_BELOW = 1e-4       # mixed path: FP32 VRR attempted below this bound ...
 MIXED_TOL = 5e-11       # ... and kept only where its rounding-error bound is below this; else FP64
 PRIM_TOL = 1e-18        # screened paths: primitive quartets with Q_ab Q_cd below this skipped
@@ -56,11 +72,14 @@ def parse():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
-    ap.add_argument('--workload', default='eri', choices=['eri', 'nuclear_2idx', 'overlap_2idx', 'lattice_l3'],
+    ap.add_argument('--workload', default='eri',
+                    choices=['eri', 'nuclear_2idx', 'overlap_2idx', 'lattice_l3', 'c5'],
                     help='eri: the headline; *_2idx: the example script\'s two-index classes; lattice_l3: '
-                         'a sample of the 200-atom l <= 3 lattice\'s screened quartets')
+                         'a sample of the 200-atom l <= 3 lattice\'s screened quartets; c5: a sample of the '
+                         'l <= 4, K <= 8 screened-quartet workload')
     ap.add_argument('--npairs', type=int, default=4_000_000)
     ap.add_argument('--nq-lattice', type=int, default=2_000_000)
+    ap.add_argument('--nq-c5', type=int, default=50_000)
     ap.add_argument('--only', default=None, choices=['fp64', 'screened', 'screened_prim'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time')
     return ap.parse_args()
@@ -200,9 +219,11 @@ def alg_flops(batch):
     return float((nprim * vrr[cid] + hrr[cid]).sum()), cid
 
 
-def cpu_reference(batch, seconds, step_index=0):
+def cpu_reference(batch, seconds, step_index=0, skip_below=SKIP_BELOW):
     """Time the reference's emitted C99 (oracle/_ref) -- or, when it was not
-    built, the oracle port -- on all host cores over a bounded sample.
+    built, the oracle port -- on all host cores over a bounded random sample of
+    the batch, behind the same analytic screening as the GPU's screened paths
+    (bounds computed in the timed call; skip_below 0 evaluates every quartet).
     Returns (quartets/s, kind, cores, sample description)."""
     from intception_b200 import basis
     from oracle import loader
@@ -217,17 +238,44 @@ def cpu_reference(batch, seconds, step_index=0):
         sub = batch.subset(np.sort(idx))
         t0 = time.perf_counter()
         if lib is not None:
-            loader.ref_batch(sub, T, nthreads=cores)
+            if skip_below > 0:
+                loader.ref_batch_screened(sub, T, skip_below, nthreads=cores)
+            else:
+                loader.ref_batch(sub, T, nthreads=cores)
         else:
             loader.oracle_batch(sub, T)
         return time.perf_counter() - t0
 
-    n = 2000
+    n = 2000 if skip_below == 0 else 20000
     dt = run(n)
     n2 = int(min(batch.nq, max(n, n * seconds / max(dt, 1e-3))))
     dt2 = run(n2)
     used = cores if lib is not None else 1
-    return n2 / dt2, kind, used, '%d random quartets of the workload (uniform sample)' % n2
+    what = ('analytic bounds, zeros below %.0e, the rest through the emitted function' % skip_below
+            if skip_below > 0 else 'every quartet through the emitted function')
+    return n2 / dt2, kind, used, '%d random quartets of the workload (uniform sample); %s' % (n2, what)
+
+
+def reference_error(batch, outs, nsample=20000, seed=123):
+    """Max |GPU - reference C99| over a seeded sample of the batch's quartets:
+    outs maps a path name to that path's device output for the whole batch.
+    The reference evaluates every sampled quartet (no screening), so a
+    screened path's figure includes its screening error."""
+    from intception_b200 import basis
+    from oracle import loader
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(batch.nq, min(nsample, batch.nq), replace=False))
+    sub = batch.subset(idx)
+    ref = loader.ref_batch(sub, basis.sph_matrices(6), nthreads=os.cpu_count() or 1)
+    kind = 'reference'
+    if ref is None:
+        ref, kind = loader.oracle_batch(sub, basis.sph_matrices(6)), 'port'
+    sizes = basis.block_sizes(batch.shell_l, batch.quartets[idx], batch.spherical)
+    gather = np.concatenate([np.arange(o, o + n) for o, n in zip(batch.out_off[idx], sizes)])
+    res = {name: float(np.abs(out[gather] - ref).max()) for name, out in outs.items()}
+    res['sample'] = '%d seeded random quartets of this rank\'s batch vs the %s C99, unscreened' % (len(idx), kind)
+    res['max_abs_reference'] = float(np.abs(ref).max())
+    return res
 
 
 def run_reference_arm(args, rank, world):
@@ -243,8 +291,10 @@ def run_reference_arm(args, rank, world):
     v = float(np.median(vals))
     line = {'metric': METRIC, 'value': v, 'unit': 'quartets/s', 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * args.nq / v, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': {'workload': WORKLOAD, 'nq': args.nq, 'parallelism': 'openmp host cores'},
+            'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'nq': args.nq, 'parallelism': 'openmp host cores',
+                       'screening': 'the GPU arm\'s: analytic quartet bounds in the step, zero blocks below %.0e'
+                       % SKIP_BELOW},
             'impl': 'reference',
             'cpu_baseline': {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample},
             'e2e': {'value': v, 'unit': 'quartets/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -273,6 +323,141 @@ def lattice_batch(nq, seed=2):
     quartets, total = basis.sample_screened_quartets(q, pairs, nq, rng, SKIP_BELOW)
     off, tot = basis.packed_offsets(l_, quartets, True)
     return basis.ShellBatch(l_, k_, p_, cxyz, e, c, quartets, off, True, tot), total
+
+
+C5_WORKLOAD = ('l in 0..4 per shell, K uniform in 1..8, alpha log-uniform [0.02,1e5], centres uniform in a '
+               '10-bohr cube, spherical, seed 4; candidates screened with the analytic bounds at 1e-12; a sample of '
+               '%d kept quartets standing for the 5e7-quartet batch')
+
+
+def c5_batch(nq, seed=4):
+    """nq quartets of the l <= 4 workload that pass the 1e-12 screen: candidate
+    quartets (four fresh shells each) are drawn in rounds and kept by their
+    analytic bound, computed on the GPU.  Returns (batch, kept fraction)."""
+    import torch
+    from intception_b200 import basis, eri
+    rng_seed, kept, drawn, parts = seed, [], 0, []
+    while sum(len(k) for k in kept) < nq:
+        cand = basis.independent_quartet_batch(rng_seed, max(nq, 20000), [0, 1, 2, 3, 4], [1, 2, 3, 4, 5, 6, 7, 8],
+                                               0.02, 1.0e5, 10.0, True)
+        rng_seed += 1000
+        bnd = eri.EriEngine(cand).analytic_bounds().cpu().numpy()
+        idx = np.nonzero(bnd >= SKIP_BELOW)[0]
+        drawn += cand.nq
+        kept.append(idx)
+        parts.append(cand)
+    # keep the first nq survivors (in draw order) in one shell table
+    qs = []
+    need = nq
+    for cand, idx in zip(parts, kept):
+        take = idx[:need]
+        need -= len(take)
+        qs.append(cand.subset(take))
+        if need == 0:
+            break
+    ls = np.concatenate([b.shell_l for b in qs])
+    ks = np.concatenate([b.shell_k for b in qs])
+    xyz = np.concatenate([b.shell_xyz for b in qs])
+    e = np.concatenate([b.prim_exp for b in qs])
+    c = np.concatenate([b.prim_coef for b in qs])
+    ptr = np.concatenate([[0], np.cumsum(ks)[:-1]]).astype(np.int32)
+    quart, base = [], 0
+    for b in qs:
+        quart.append(b.quartets + base)
+        base += len(b.shell_l)
+    quart = np.concatenate(quart).astype(np.int32)
+    off, total = basis.packed_offsets(ls, quart, True)
+    b = basis.ShellBatch(ls, ks, ptr, xyz, e, c, quart, off, True, total)
+    frac = sum(len(k) for k in kept) / drawn
+    return b, frac
+
+
+def run_c5(args, rank, world, local):
+    """The l <= 4 workload on a sample of its screened quartets: FP64 (every
+    sampled quartet) and the mixed path (analytic bounds in the step, FP32
+    tier below 1e-4 where a class has FP32 kernels), its CUDA-graph replay;
+    the reference C99 on the host cores beside it."""
+    import torch
+    from intception_b200 import eri
+    batch, frac = c5_batch(args.nq_c5)
+    eng = eri.EriEngine(batch)
+    out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+    bounds = torch.empty(batch.nq, dtype=torch.float64, device='cuda')
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        assert eng.device_status() == 0
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+
+    def screened_step(precision):
+        eng.analytic_bounds(out=bounds)
+        eng.compute(out=out, precision=precision, bounds=bounds, skip_below=SKIP_BELOW, fp32_below=FP32_BELOW,
+                    mixed_tol=MIXED_TOL)
+
+    clk = ClockSampler(local).__enter__()
+    eri.set_prim_tol(0.0)
+    ms64 = timed(lambda: eng.compute(out=out))
+    ref = out.clone()
+    host = {'fp64_exact': ref.cpu().numpy()}
+    eri.set_prim_tol(PRIM_TOL)
+    mss = timed(lambda: screened_step(eri.PREC_FP64))
+    errs = max_over_ranks(float((out - ref).abs().max().item()), world)
+    msm = timed(lambda: screened_step(eri.PREC_MIXED))
+    errm = max_over_ranks(float((out - ref).abs().max().item()), world)
+    host['mixed'] = out.cpu().numpy()
+    launches = eri.EriEngine.last_launch_count() + 1
+    graph = eng.graph(out, precision=eri.PREC_MIXED, bounds=bounds, skip_below=SKIP_BELOW, fp32_below=FP32_BELOW,
+                      mixed_tol=MIXED_TOL)
+
+    def graph_step():
+        eng.analytic_bounds(out=bounds)
+        graph.launch()
+
+    msg = timed(graph_step)
+    errg = max_over_ranks(float((out - ref).abs().max().item()), world)
+    graph.close()
+    eri.set_prim_tol(0.0)
+    clk.__exit__(None, None, None)
+    # live primitive quartets of the sample (the per-primitive cost against (ff|ff))
+    nprim = float((live_pairs(batch, 0, 1) * live_pairs(batch, 2, 3)).sum())
+    cpu, ref_err = None, None
+    if rank == 0:
+        ref_err = reference_error(batch, host, nsample=2000)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds, skip_below=0.0)
+        cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
+    if rank == 0:
+        nq = batch.nq * world
+        print(json.dumps({
+            'metric': 'contracted ERI quartets/s on B200, l<=4 K<=8 screened quartets (sample of the 5e7 batch)',
+            'value': nq / (msm * 1e-3), 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': msm, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64+f32', 'data': 'synthetic',
+            'config': {'workload': C5_WORKLOAD % batch.nq, 'kept_fraction_of_candidates': frac,
+                       'prim_tol': PRIM_TOL, 'fp32_below': FP32_BELOW, 'mixed_tol': MIXED_TOL,
+                       'l2': 'outputs %.0f MB per step; no flush' % (batch.out_size * 8 / 1e6)},
+            'max_abs_err_vs_fp64': errm, 'max_abs_err_vs_reference': ref_err,
+            'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'every sampled quartet, FP64',
+                     'ns_per_live_primitive_quartet': ms64 * 1e6 / nprim},
+            'fp64_screened': {'ms_per_step': mss, 'value': nq / (mss * 1e-3), 'max_abs_err_vs_fp64': errs,
+                              'note': 'the mixed path\'s screening, FP64 throughout'},
+            'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm},
+            'cuda_graph': {'ms_per_step': msg, 'max_abs_err_vs_fp64': errg},
+            'mixed_over_fp64': mss / msm, 'live_primitive_quartets': nprim,
+            'estimated_5e7_quartets_s': 5e7 / (nq / (msm * 1e-3)),
+            'cpu_baseline': cpu, 'gpu_launches': launches * args.steps, 'clocks': clk.summary()}), flush=True)
 
 
 def run_lattice(args, rank, world, local):
@@ -306,25 +491,46 @@ def run_lattice(args, rank, world, local):
     eri.set_prim_tol(0.0)
     ms64 = timed(lambda: eng.compute(out=out))
     ref = out.clone()
+    host = {'fp64_exact': ref.cpu().numpy()}
+    # Schwarz factors are per basis (computed once, reused by every batch of
+    # this lattice's quartets); the sample holds only quartets above 1e-12
     bounds = eng.quartet_bounds()
     eri.set_prim_tol(PRIM_TOL)
-    msp = timed(lambda: eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW))
+
+    def prim_step():
+        eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW)
+
+    def mixed_step():
+        eng.compute(out=out, precision=eri.PREC_MIXED, bounds=bounds, skip_below=SKIP_BELOW, fp32_below=FP32_BELOW,
+                    mixed_tol=MIXED_TOL)
+
+    msp = timed(prim_step)
     errp = max_over_ranks(float((out - ref).abs().max().item()), world)
-    msm = timed(lambda: eng.compute(out=out, precision=eri.PREC_MIXED, bounds=bounds, skip_below=SKIP_BELOW,
-                                    fp32_below=FP32_BELOW, mixed_tol=MIXED_TOL))
+    host['fp64_prim'] = out.cpu().numpy()
+    msm = timed(mixed_step)
     errm = max_over_ranks(float((out - ref).abs().max().item()), world)
+    host['mixed'] = out.cpu().numpy()
     rej = eng.fp32_rejected()
     nfp32 = int((bounds < FP32_BELOW).sum().item())
+    # the fastest path within 1e-10 of exact FP64, then measured again on its own
+    cands = [(ms64, 0.0, 'fp64'), (msp, errp, 'fp64 + primitive screening'), (msm, errm, 'precision tiers')]
+    ok = [c for c in cands if c[1] <= ERR_BAR] or cands
+    _, _, path = min(ok)
+    if path == 'fp64':
+        eri.set_prim_tol(0.0)
+    fn = {'fp64': lambda: eng.compute(out=out), 'fp64 + primitive screening': prim_step,
+          'precision tiers': mixed_step}[path]
+    ms = timed(fn)
+    err = max_over_ranks(float((out - ref).abs().max().item()), world)
     launches = eri.EriEngine.last_launch_count()
     eri.set_prim_tol(0.0)
     clk.__exit__(None, None, None)
-    cands = [(ms64, 0.0, 'fp64'), (msp, errp, 'fp64 + primitive screening'), (msm, errm, 'precision tiers')]
-    ok = [c for c in cands if c[1] <= ERR_BAR] or cands
-    ms, err, path = min(ok)
     nq = batch.nq * world
-    cpu = None
+    cpu, ref_err = None, None
+    if rank == 0:
+        ref_err = reference_error(batch, host, nsample=10000)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds)
+        v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds, skip_below=0.0)
         cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
     if rank == 0:
         print(json.dumps({
@@ -335,8 +541,10 @@ def run_lattice(args, rank, world, local):
             'config': {'workload': LATTICE_WORKLOAD % batch.nq, 'screened_quartets_total': total,
                        'headline_path': path, 'prim_tol': PRIM_TOL, 'fp32_below': FP32_BELOW,
                        'mixed_tol': MIXED_TOL, 'l2': 'outputs %.0f MB per step, larger than L2; no flush'
-                       % (batch.out_size * 8 / 1e6)},
+                       % (batch.out_size * 8 / 1e6),
+                       'bounds': 'Schwarz factors, once per basis (outside the step)'},
             'max_abs_err_vs_fp64': err,
+            'max_abs_err_vs_reference': ref_err,
             'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'exact, no screening'},
             'fp64_prim': {'ms_per_step': msp, 'max_abs_err_vs_fp64': errp},
             'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm, 'fp32_attempted': nfp32,
@@ -488,73 +696,50 @@ def run_twoidx(args, rank, world, local):
 
 def run_only(args, eng, out):
     """One step kind alone (for profilers): the FP64 step over every quartet,
-    or the screened FP64 step (bounds computed first, outside the timing)."""
+    or the screened FP64 step (analytic bounds inside the step)."""
     import torch
     from intception_b200 import eri
-    bounds, skip = None, 0.0
-    if args.only in ('screened', 'screened_prim'):
-        bounds, skip = eng.quartet_bounds(), SKIP_BELOW
+    screened = args.only in ('screened', 'screened_prim')
+    bounds = torch.empty(eng.nq, dtype=torch.float64, device='cuda') if screened else None
     eri.set_prim_tol(PRIM_TOL if args.only == 'screened_prim' else 0.0)
+
+    def step():
+        if screened:
+            eng.analytic_bounds(out=bounds)
+        eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW if screened else 0.0)
+
     torch.cuda.synchronize()
     for _ in range(args.warmup):
-        eng.compute(out=out, bounds=bounds, skip_below=skip)
+        step()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     for _ in range(args.steps):
-        eng.compute(out=out, bounds=bounds, skip_below=skip)
+        step()
     ev1.record()
     torch.cuda.synchronize()
     assert eng.device_status() == 0
-    print(json.dumps({'only': args.only, 'nq': args.nq, 'steps': args.steps, 'warmup': args.warmup,
+    print(json.dumps({'only': args.only, 'nq': eng.nq, 'steps': args.steps, 'warmup': args.warmup,
                       'ms_per_step': ev0.elapsed_time(ev1) / args.steps,
-                      'kernels_per_step': eri.EriEngine.last_launch_count()}), flush=True)
+                      'kernels_per_step': eri.EriEngine.last_launch_count() + (1 if screened else 0)}), flush=True)
 
 
-def main():
-    args = parse()
-    if args.impl == 'reference':
-        # host cores only: no process group; rank 0 runs the reference, the
-        # other ranks of a multi-GPU launch exit at once
-        rank, world = int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1'))
-        if args.workload == 'lattice_l3':
-            if rank == 0:  # the sample is drawn with the GPU's Schwarz factors; its line carries cpu_baseline
-                print(json.dumps({'impl': 'reference', 'unavailable': 'lattice_l3 draws its quartet sample with '
-                                  'GPU Schwarz factors; the reference C99 is timed in that line\'s cpu_baseline'}))
-            return
-        if args.workload != 'eri':
-            run_twoidx(args, rank, world, 0)
-        else:
-            run_reference_arm(args, rank, world)
-        return
-    rank, world, local = dist_init(args.gpus)
-    if args.workload == 'lattice_l3':
-        run_lattice(args, rank, world, local)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
-    if args.workload != 'eri':
-        run_twoidx(args, rank, world, local)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
+def run_eri(args, rank, world, local):
+    """The headline workload: one C2 batch, split over the ranks."""
     import torch
-    from intception_b200 import basis, eri
-    batch = basis.config_mixed_l2(nq=args.nq, seed=1 + rank, spherical=True)
+    from intception_b200 import basis, eri, shard
+    full = basis.config_mixed_l2(nq=args.nq, seed=1, spherical=True)
+    batch = full if world == 1 else shard.shard_for_rank(full, rank, world)[0]
     eng = eri.EriEngine(batch)
     stream = torch.cuda.current_stream()
     out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+    bounds = torch.empty(batch.nq, dtype=torch.float64, device='cuda')
     if args.only:
         run_only(args, eng, out)
         return
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def step(precision=eri.PREC_FP64, bounds=None, skip=0.0):
-        eng.compute(out=out, precision=precision, bounds=bounds, skip_below=skip, fp32_below=FP32_BELOW,
-                    mixed_tol=MIXED_TOL)
-
-    def timed(fn, clocks=None):
+    def timed(fn):
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
@@ -569,181 +754,189 @@ def main():
         barrier(world)
         return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
 
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # ---------------- FP64 path, every quartet evaluated, device-resident inputs
+    def screened_step(precision, fb):
+        eng.analytic_bounds(out=bounds)  # part of every screened step
+        eng.compute(out=out, precision=precision, bounds=bounds, skip_below=SKIP_BELOW, fp32_below=fb,
+                    mixed_tol=MIXED_TOL)
+
+    def err_vs(ref):
+        return max_over_ranks(float((out - ref).abs().max().item()), world)
+
+    rate = lambda ms: args.nq / (ms * 1e-3)  # noqa: E731  whole job: the full batch over the slowest rank
+
     clk = ClockSampler(local).__enter__()  # sampled over every timed region below
-    ms64 = timed(step)
-    launches = eri.EriEngine.last_launch_count()
-    value64 = args.nq * world / (ms64 * 1e-3)
+    # ---- FP64, every quartet evaluated, no screening of any kind
+    eri.set_prim_tol(0.0)
+    ms64 = timed(lambda: eng.compute(out=out))
+    launches64 = eri.EriEngine.last_launch_count()
     ref64 = out.clone()
-
-    # ---------------- Schwarz bounds (per shell pair, once per basis), then the screened paths
-    mixed = None
-    screened = None
-    screened_prim = None
+    host_fp64 = out.cpu().numpy() if rank == 0 else None
+    # ---- screened FP64: analytic bounds in the step, zeros below SKIP_BELOW, primitive screening
+    eri.set_prim_tol(PRIM_TOL)
+    ms_s = timed(lambda: screened_step(eri.PREC_FP64, 0.0))
+    err_s = err_vs(ref64)
+    n_kept = int((bounds >= SKIP_BELOW).sum().item())  # this rank's quartets kept by the screening
+    # ---- FP32-tier setting: a sweep over fp32_below (0 = tier off), then the
+    # chosen setting measured on its own as the headline
+    sweep = []
     if not args.no_mixed:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        bounds = eng.quartet_bounds()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        schwarz_ms = e0.elapsed_time(e1)
-        n_kept = int((bounds >= SKIP_BELOW).sum().item())
-        ms_s = timed(lambda: step(eri.PREC_FP64, bounds, SKIP_BELOW))
-        err_s = max_over_ranks(float((out - ref64).abs().max().item()), world)
-        screened = {'value': args.nq * world / (ms_s * 1e-3), 'ms_per_step': ms_s, 'max_abs_err_vs_fp64': err_s,
-                    'screened_quartets_per_s': n_kept * world / (ms_s * 1e-3)}
-        # primitive screening on top (kept for every path below): a primitive
-        # quartet whose Schwarz-type bound Q_ab Q_cd is below PRIM_TOL moves
-        # no element by more than PRIM_TOL, so a block by at most K^4 PRIM_TOL
-        eri.set_prim_tol(PRIM_TOL)
-        ms_p = timed(lambda: step(eri.PREC_FP64, bounds, SKIP_BELOW))
-        err_p = max_over_ranks(float((out - ref64).abs().max().item()), world)
-        screened_prim = {'value': args.nq * world / (ms_p * 1e-3), 'ms_per_step': ms_p, 'max_abs_err_vs_fp64': err_p,
-                         'prim_tol': PRIM_TOL, 'error_bound_per_element': 1296 * PRIM_TOL,
-                         'screened_quartets_per_s': n_kept * world / (ms_p * 1e-3)}
-        # precision tiers: zeros below SKIP_BELOW, FP32 VRR (with its rounding-error
-        # bound, rejected quartets redone in FP64) below fp32_below, FP64 above.
-        # fp32_below is tuned here; 0 switches the FP32 tier off.
-        sweep = []
-        for fb in FP32_SWEEP:
-            mode = eri.PREC_MIXED if fb > 0 else eri.PREC_FP64
-            msx = timed(lambda: eng.compute(out=out, precision=mode, bounds=bounds, skip_below=SKIP_BELOW,
-                                            fp32_below=fb, mixed_tol=MIXED_TOL))
-            errx = max_over_ranks(float((out - ref64).abs().max().item()), world)
-            nf = int(((bounds >= SKIP_BELOW) & (bounds < fb)).sum().item()) if fb > 0 else 0
-            rej = eng.fp32_rejected() if fb > 0 else 0
-            sweep.append({'fp32_below': fb, 'ms_per_step': msx, 'max_abs_err_vs_fp64': errx,
-                          'fp32_attempted': nf, 'fp32_rejected': rej})
-        ok = [r for r in sweep if r['max_abs_err_vs_fp64'] <= ERR_BAR] or sweep
-        best = min(ok, key=lambda r: r['ms_per_step'])
-        fb = best['fp32_below']
-        msmx = best['ms_per_step']
-        err = best['max_abs_err_vs_fp64']
-        mixed = {'value': args.nq * world / (msmx * 1e-3), 'ms_per_step': msmx, 'max_abs_err_vs_fp64': err,
-                 'screened_quartets_per_s': n_kept * world / (msmx * 1e-3),
-                 'kept_fraction': n_kept / args.nq, 'skip_below': SKIP_BELOW, 'prim_tol': PRIM_TOL, 'fp32_below': fb,
-                 'mixed_tol': MIXED_TOL, 'fp32_tier_active': fb > 0, 'fp32_sweep': sweep,
-                 'schwarz_ms': schwarz_ms, 'schwarz_note': 'per-pair Schwarz factors, computed once per basis '
-                 'on the GPU (intception_b200_schwarz), outside the timed step; this workload has no pair reuse'}
-        FP32_CHOSEN[0] = fb
+        for fb in FP32_SWEEP[1:]:
+            msx = timed(lambda: screened_step(eri.PREC_MIXED, fb))
+            sweep.append({'fp32_below': fb, 'ms_per_step': msx, 'max_abs_err_vs_fp64': err_vs(ref64),
+                          'fp32_attempted': int(((bounds >= SKIP_BELOW) & (bounds < fb)).sum().item()),
+                          'fp32_rejected': eng.fp32_rejected()})
+    ok = [r for r in sweep if r['max_abs_err_vs_fp64'] <= ERR_BAR]
+    best = min(ok, key=lambda r: r['ms_per_step']) if ok else None
+    fb = best['fp32_below'] if best is not None and best['ms_per_step'] < ms_s else 0.0
+    FP32_CHOSEN[0] = fb
+    prec = eri.PREC_MIXED if fb > 0 else eri.PREC_FP64
+    msm = timed(lambda: screened_step(prec, fb))
+    launches = eri.EriEngine.last_launch_count() + 1  # + the bounds kernel
+    err_m = err_vs(ref64)
+    rej = eng.fp32_rejected() if fb > 0 else 0
+    host_mixed = out.cpu().numpy() if rank == 0 else None
+    value = rate(msm)
+    # ---- the headline configuration replayed from a CUDA graph (bounds kernel
+    # outside the graph, on the same stream)
+    graph = eng.graph(out, precision=prec, bounds=bounds, skip_below=SKIP_BELOW, fp32_below=fb, mixed_tol=MIXED_TOL)
 
-    headline_mixed = mixed is not None and mixed['max_abs_err_vs_fp64'] <= ERR_BAR
-    # the headline configuration replayed from a CUDA graph (sort, items, class
-    # kernels and their side-stream fork/join captured once)
-    if headline_mixed:
-        fb = FP32_CHOSEN[0]
-        graph = eng.graph(out, precision=eri.PREC_MIXED if fb > 0 else eri.PREC_FP64, bounds=bounds,
-                          skip_below=SKIP_BELOW, fp32_below=fb, mixed_tol=MIXED_TOL)
-    else:
-        graph = eng.graph(out)
-    ms_graph = timed(graph.launch)
-    launches = eri.EriEngine.last_launch_count()  # kernels of one replayed step of the headline path
-    err_graph = max_over_ranks(float((out - ref64).abs().max().item()), world)
+    def graph_step():
+        eng.analytic_bounds(out=bounds)
+        graph.launch()
+
+    ms_graph = timed(graph_step)
+    err_graph = err_vs(ref64)
     graph.close()
-    if headline_mixed:
-        mixed['graph_ms_per_step'] = ms_graph
-        mixed['graph_max_abs_err_vs_fp64'] = err_graph
-        # the tuned tier path, measured three ways: the sweep's best setting,
-        # its graph replay, and (FP32 tier off) the screened FP64 run above
-        cands = [mixed['ms_per_step'], ms_graph]
-        if FP32_CHOSEN[0] == 0 and screened_prim is not None:
-            cands.append(screened_prim['ms_per_step'])
-        ms = min(cands)
-        value = args.nq * world / (ms * 1e-3)
-    else:
-        ms = min(ms64, ms_graph)
-        value = args.nq * world / (ms * 1e-3)
 
-    # ---------------- roofline of the FP64 step against the measured FP64 FMA peak
+    # ---- roofline of the FP64 step against the measured FP64 FMA peak
     flops, _ = alg_flops(batch)
-    peak64 = eri.fma_peak(True) if rank == 0 else 0.0
+    peak64 = eri.fma_peak(True)
     achieved = flops / (ms64 * 1e-3)
     roofline = {'bound': 'fp64', 'achieved': achieved / 1e12, 'peak': peak64 / 1e12, 'unit': 'TFLOP/s',
                 'frac': achieved / peak64 if peak64 else None, 'traffic': None,
-                'peak_source': 'measured FP64 FMA-chain kernel (intception_b200_fma_peak), this run',
-                'kernel': 'whole FP64 step (per-class kernels run concurrently)',
+                'peak_source': 'measured FP64 FMA-chain kernel (intception_b200_fma_peak), this run; '
+                               'MEASURED_PEAKS.json has no FP64 figure',
+                'kernel': 'whole FP64 step of this rank (per-class kernels run concurrently)',
                 'alg_flops_per_step': flops}
     prof = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(prof):
         with open(prof) as fh:
             roofline['traffic'] = json.load(fh).get('bytes_per_step')
 
-    # ---------------- e2e through the public API with host buffers: every step
-    # uploads its inputs from pinned host memory, evaluates, and reads its blocks
-    # back; eri.HostPipeline overlaps step i+1's upload and step i-1's read-back
-    # with step i's evaluation
-    e2e = None
-    if rank == 0 or world > 1:
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        h = {'shell_l': pin(batch.shell_l), 'shell_k': pin(batch.shell_k), 'shell_ptr': pin(batch.shell_ptr),
-             'shell_xyz': pin(batch.shell_xyz), 'prim_exp': pin(batch.prim_exp),
-             'prim_coef': pin(batch.prim_coef), 'quartets': pin(batch.quartets.reshape(-1)),
-             'out_off': pin(batch.out_off)}
-        prec = eri.PREC_MIXED if (headline_mixed and FP32_CHOSEN[0] > 0) else eri.PREC_FP64
-        if headline_mixed:  # the per-quartet bounds are an input of the screened path
-            h['bounds'] = bounds.cpu().pin_memory()
-        h_out = [torch.empty(batch.out_size, dtype=torch.float64).pin_memory() for _ in range(2)]
-        h2d = sum(t.numel() * t.element_size() for t in h.values())
-        d2h = h_out[0].numel() * 8
-        pipe = eri.HostPipeline(batch.spherical, depth=2)
-        lmax_b = int(batch.shell_l.max())
+    # ---- e2e through the public API with host buffers: every step uploads its
+    # inputs from pinned host memory, computes the analytic bounds and the
+    # screened blocks on the device, and reads its blocks back;
+    # eri.HostPipeline overlaps step i+1's upload and step i-1's read-back with
+    # step i's evaluation
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h = {'shell_l': pin(batch.shell_l), 'shell_k': pin(batch.shell_k), 'shell_ptr': pin(batch.shell_ptr),
+         'shell_xyz': pin(batch.shell_xyz), 'prim_exp': pin(batch.prim_exp),
+         'prim_coef': pin(batch.prim_coef), 'quartets': pin(batch.quartets.reshape(-1)),
+         'out_off': pin(batch.out_off)}
+    h_out = [torch.empty(batch.out_size, dtype=torch.float64).pin_memory() for _ in range(2)]
+    h2d = sum(t.numel() * t.element_size() for t in h.values())
+    d2h = h_out[0].numel() * 8
+    pipe = eri.HostPipeline(batch.spherical, depth=2)
+    lmax_b = int(batch.shell_l.max())
 
-        def e2e_step(i):
-            pipe.submit(h, h_out[i % 2], precision=prec, skip_below=SKIP_BELOW if headline_mixed else 0.0,
-                        fp32_below=FP32_CHOSEN[0], mixed_tol=MIXED_TOL, lmax=lmax_b)
+    def e2e_step(i):
+        pipe.submit(h, h_out[i % 2], precision=prec, skip_below=SKIP_BELOW, fp32_below=fb, mixed_tol=MIXED_TOL,
+                    lmax=lmax_b)
 
-        for i in range(args.warmup):
-            e2e_step(i)
-        pipe.synchronize()
-        torch.cuda.synchronize()
-        barrier(world)
-        e_start = torch.cuda.Event(enable_timing=True)
-        e_start.record(pipe.s_in)  # the pipeline's first work of the timed region is on its upload stream
-        for i in range(args.steps):
-            e2e_step(args.warmup + i)
-        e_end = pipe.wait_event()
-        pipe.synchronize()
-        torch.cuda.synchronize()
-        barrier(world)
-        mse = max_over_ranks(e_start.elapsed_time(e_end) / args.steps, world)
-        # the last read-back is the reference result of this configuration
-        e2e_err = float(np.abs(h_out[(args.warmup + args.steps - 1) % 2].numpy() - ref64.cpu().numpy()).max())
-        e2e = {'value': args.nq * world / (mse * 1e-3), 'unit': 'quartets/s', 'h2d_bytes_per_step': h2d,
-               'd2h_bytes_per_step': d2h, 'ms_per_step': mse, 'max_abs_err_vs_fp64': e2e_err,
-               'api': 'eri.HostPipeline (pinned host inputs -> blocks in pinned host memory, depth 2)'}
-
+    for i in range(args.warmup):
+        e2e_step(i)
+    pipe.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_start.record(pipe.s_in)  # the pipeline's first work of the timed region is on its upload stream
+    for i in range(args.steps):
+        e2e_step(args.warmup + i)
+    e_end = pipe.wait_event()
+    pipe.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    mse = max_over_ranks(e_start.elapsed_time(e_end) / args.steps, world)
+    e2e_err = float(np.abs(h_out[(args.warmup + args.steps - 1) % 2].numpy() - ref64.cpu().numpy()).max())
+    e2e = {'value': rate(mse), 'unit': 'quartets/s', 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+           'ms_per_step': mse, 'max_abs_err_vs_fp64': max_over_ranks(e2e_err, world),
+           'api': 'eri.HostPipeline (pinned host inputs -> analytic bounds and screened blocks on the device -> '
+                  'blocks in pinned host memory, depth 2)'}
     clk.__exit__(None, None, None)
     eri.set_prim_tol(0.0)
-    cpu = None
+
+    # ---- outside the timing: reference error on a sample, CPU baseline
+    ref_err, cpu, cpu_all = None, None, None
+    if rank == 0:
+        ref_err = reference_error(batch, {'fp64_exact': host_fp64, 'headline': host_mixed})
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds)
         cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
+        v0, kind0, cores0, sample0 = cpu_reference(batch, args.cpu_seconds / 2, skip_below=0.0)
+        cpu_all = {'value': v0, 'unit': 'quartets/s', 'cores': cores0, 'kind': kind0, 'sample': sample0}
 
     if rank == 0:
+        fp64_s = {'value': rate(ms_s), 'ms_per_step': ms_s, 'max_abs_err_vs_fp64': err_s}
         line = {'metric': METRIC, 'value': value, 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
-                'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
-                'vs_baseline': None, 'dtype': 'f64+f32' if (headline_mixed and FP32_CHOSEN[0] > 0) else 'f64', 'data': 'synthetic',
-                'config': {'workload': WORKLOAD, 'nq_per_gpu': args.nq,
+                'warmup': args.warmup, 'ms_per_step': msm, 'higher_is_better': True, 'scaling': 'strong',
+                'vs_baseline': None, 'dtype': 'f64+f32' if fb > 0 else 'f64', 'data': 'synthetic',
+                'config': {'workload': WORKLOAD, 'nq_total': args.nq, 'nq_this_rank': batch.nq,
+                           'split': 'one batch, %d cost-balanced contiguous shards of its class-sorted list' % world,
                            'l2': 'inputs+outputs ~1 GB per step, larger than L2; no flush',
-                           'headline_path': ('precision tiers: screened zeros below %.0e, FP32 below %g, FP64 above; '
-                                             'primitive quartets with bound below %.0e skipped'
-                                             % (SKIP_BELOW, FP32_CHOSEN[0], PRIM_TOL)) if headline_mixed else 'fp64'},
-                'fp64': {'value': value64, 'ms_per_step': ms64, 'note': 'every quartet evaluated in FP64'},
-                'cuda_graph_ms_per_step': ms_graph,
-                'fp64_screened': screened,
-                'fp64_screened_prim': screened_prim,
-                'mixed': mixed,
-                'mixed_over_fp64': (mixed['value'] / value64) if mixed else None,
-                'mixed_over_fp64_screened': (mixed['value'] / screened['value']) if mixed else None,
-                'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
-                'gpu_launches': launches * args.steps,
-                'gpu_launches_per_step': launches,
+                           'headline_path': ('mixed: analytic bounds in the step, zeros below %.0e, primitive '
+                                             'quartets below %.0e skipped, FP32 VRR below bound %g (0: tier off, '
+                                             'all FP64), rounding-error bound %.0e'
+                                             % (SKIP_BELOW, PRIM_TOL, fb, MIXED_TOL))},
+                'max_abs_err_vs_fp64': err_m,
+                'max_abs_err_vs_reference': ref_err,
+                'fp64_exact': {'value': rate(ms64), 'ms_per_step': ms64, 'kernels_per_step': launches64,
+                               'note': 'every quartet evaluated in FP64, no screening'},
+                'fp64_screened': fp64_s,
+                'mixed': {'value': value, 'ms_per_step': msm, 'fp32_below': fb, 'fp32_tier_active': fb > 0,
+                          'fp32_rejected': rej, 'mixed_tol': MIXED_TOL, 'fp32_sweep': sweep,
+                          'note': 'fp32_below chosen by the sweep (fastest within 1e-10), then measured again '
+                                  'on its own; the same screening as fp64_screened'},
+                'mixed_over_fp64': value / rate(ms_s),
+                'screening_gain': rate(ms_s) / rate(ms64),
+                'kept_fraction': n_kept / batch.nq,
+                'cuda_graph': {'ms_per_step': ms_graph, 'max_abs_err_vs_fp64': err_graph},
+                'roofline': roofline, 'cpu_baseline': cpu, 'cpu_baseline_unscreened': cpu_all, 'e2e': e2e,
+                'gpu_launches': launches * args.steps, 'gpu_launches_per_step': launches,
                 'clocks': clk.summary()}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        # host cores only: no process group; rank 0 runs the reference, the
+        # other ranks of a multi-GPU launch exit at once
+        rank, world = int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1'))
+        if args.workload in ('lattice_l3', 'c5'):
+            if rank == 0:  # the sample is drawn with GPU screening bounds; its line carries cpu_baseline
+                print(json.dumps({'impl': 'reference', 'unavailable': '%s draws its quartet sample with GPU '
+                                  'screening bounds; the reference C99 is timed in that line\'s cpu_baseline'
+                                  % args.workload}))
+            return
+        if args.workload != 'eri':
+            run_twoidx(args, rank, world, 0)
+        else:
+            run_reference_arm(args, rank, world)
+        return
+    rank, world, local = dist_init(args.gpus)
+    try:
+        if args.workload == 'lattice_l3':
+            run_lattice(args, rank, world, local)
+        elif args.workload == 'c5':
+            run_c5(args, rank, world, local)
+        elif args.workload != 'eri':
+            run_twoidx(args, rank, world, local)
+        else:
+            run_eri(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
 
 
 if __name__ == '__main__':

@@ -392,6 +392,31 @@ __device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa
   return 1.000001 * sph * K * s * s * sqrt(s) * poly;
 }
 
+// ib_pair_bound for angular momenta known only at run time (l0, l1 <= 6):
+// the sum over i, j of C(l0,i) C(l1,j) |PA|^(l0-i) |PB|^(l1-j) N_(i+j) s^(i+j)
+// regrouped by n = i + j as the coefficients of (pa + t)^l0 (pb + t)^l1.
+__device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double K, double zeta, double pa,
+                                                   double pb) {
+  double c[13];
+  c[0] = 1.0;
+  int deg = 0;
+  for (int r = 0; r < l0 + l1; ++r) {  // multiply by (p + t), p = pa for the first l0 factors
+    const double p = r < l0 ? pa : pb;
+    c[deg + 1] = c[deg];
+    for (int n = deg; n > 0; --n) c[n] = c[n] * p + c[n - 1];
+    c[0] *= p;
+    ++deg;
+  }
+  const double s = 1.0 / sqrt(zeta);
+  double poly = 0.0, sn = 1.0;
+  for (int n = 0; n <= deg; ++n) {
+    poly += c[n] * ib_rn_norm(n) * sn;
+    sn *= s;
+  }
+  const double f = sph ? ib_sph_colsum(l0) * ib_sph_colsum(l1) : 1.0;
+  return 1.000001 * f * K * s * s * sqrt(s) * poly;
+}
+
 // Bound Q of primitive pair i0 * k1 + i1 of two shells (exponent/coefficient
 // runs at ptr0, ptr1; squared centre distance r2).
 template <int L0, int L1, bool SPH>

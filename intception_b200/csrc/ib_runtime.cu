@@ -274,6 +274,52 @@ __global__ void ib_zero_screened(const unsigned* __restrict__ keys, int nq, cons
   }
 }
 
+// Analytic screening bound of every quartet: two lanes per quartet (the bra
+// and the ket pair, neighbours in one warp), each summing the Coulomb-norm
+// bound Q of its pair's primitive pairs (ib_pair_bound_rt; the triangle
+// inequality over the contraction), then bounds[q] = Q_ab Q_cd >= |(ab|cd)| of
+// every element (Cauchy-Schwarz in the Coulomb metric).  An l outside [0, 6]
+// gives +inf (never screened; the batch reports it).
+__global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, const int* __restrict__ shell_l,
+                                  const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                  const double* __restrict__ shell_xyz, const double* __restrict__ prim_exp,
+                                  const double* __restrict__ prim_coef, int spherical, double* __restrict__ bounds) {
+  const long long nthr = 2LL * ((nq + 15) / 16) * 16;  // whole half-warps: both lanes of a quartet stay together
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t - threadIdx.x % 32 < nthr;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t >> 1), side = (int)(t & 1);
+    double Q = 0.0;
+    if (q < nq) {
+      const int s0 = __ldg(quartets + 4 * q + 2 * side), s1 = __ldg(quartets + 4 * q + 2 * side + 1);
+      const int l0 = __ldg(shell_l + s0), l1 = __ldg(shell_l + s1);
+      if (l0 < 0 || l0 > IB_LMAX || l1 < 0 || l1 > IB_LMAX) {
+        Q = __longlong_as_double(0x7ff0000000000000LL);
+      } else {
+        const int k0 = __ldg(shell_k + s0), k1 = __ldg(shell_k + s1);
+        const int p0 = __ldg(shell_ptr + s0), p1 = __ldg(shell_ptr + s1);
+        double r2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          const double u = __ldg(shell_xyz + 3 * s0 + d) - __ldg(shell_xyz + 3 * s1 + d);
+          r2 += u * u;
+        }
+        const double R = sqrt(r2);
+        for (int i = 0; i < k0; ++i) {
+          const double x0 = __ldg(prim_exp + p0 + i), c0 = __ldg(prim_coef + p0 + i);
+          for (int j = 0; j < k1; ++j) {
+            const double x1 = __ldg(prim_exp + p1 + j), c1 = __ldg(prim_coef + p1 + j);
+            const double z = x0 + x1, oz = 1.0 / z;
+            const double K = fabs(ib_pair_factor(x0, c0, x1, c1, oz, r2));
+            if (K != 0.0) Q += ib_pair_bound_rt(l0, l1, spherical != 0, K, z, x1 * oz * R, x0 * oz * R);
+          }
+        }
+        Q *= 1.000001;  // the rounding of the sum
+      }
+    }
+    const double other = __shfl_xor_sync(0xffffffffu, Q, 1);
+    if (q < nq && side == 0) bounds[q] = Q * other * 1.000001;
+  }
+}
+
 struct ZeroFill {  // the caller's quartets whose blocks the screened path writes as zeros
   const unsigned* keys;
   int nq;
@@ -1063,6 +1109,25 @@ int intception_b200_schwarz(const intception_b200_basis* basis, const int* pairs
                                      c->sw_off.as<long long>(), c->sw_blocks.as<double>(), q + p0);
     IB_CUDA(cudaGetLastError());
   }
+  return set_status(IB_OK, "");
+}
+
+int intception_b200_quartet_bounds(const intception_b200_basis* basis, const int* quartets, int nq, int spherical,
+                                   double* bounds, void* stream) {
+  if (!basis || nq < 0 || (nq > 0 && (!quartets || !bounds)))
+    return set_status(IB_ERR_ARG, "quartet_bounds: null argument");
+  if (nq == 0) return set_status(IB_OK, "");
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  cudaStream_t s;
+  resolve_stream(c, stream, &s);
+  const long long threads = 2LL * ((nq + 15) / 16) * 16;
+  const int grid = (int)std::min<long long>((threads + 255) / 256, (long long)c->nsm * 16);
+  ib_quartet_bounds<<<grid, 256, 0, s>>>(quartets, nq, basis->shell_l, basis->shell_k, basis->shell_ptr,
+                                         basis->shell_xyz, basis->prim_exp, basis->prim_coef, spherical ? 1 : 0,
+                                         bounds);
+  IB_CUDA(cudaGetLastError());
   return set_status(IB_OK, "");
 }
 

@@ -408,16 +408,33 @@ class Emitter:
 DEFAULT_SLICE_CAP = 8
 
 
+# shared memory a block may use (B200: 227 KB)
+SMEM_LIMIT = 227 * 1024
+
+
+def group_fits(c):
+    """Whether class c gets a lane-group kernel: the smaller side fits a
+    128-lane group, its base-chain path has at most 6 steps (the lane code
+    packs 6), and a block's shared memory stays within SMEM_LIMIT."""
+    from .group_emitter import GroupEmitter, orientation
+    if orientation(*c) is None or min(c[0] + c[1], c[2] + c[3]) > 6:
+        return False
+    g = GroupEmitter(*c)
+    g.kernel(fp32=False)
+    groups = (128 // g.G) if g.wide else 4 * g.QPW
+    return groups * g.per_group * 8 <= SMEM_LIMIT
+
+
 def emitted_classes():
     """Canonical classes with an unrolled kernel: every class with l <= 2
-    (FP64 and FP32-VRR variants), and every class with an f shell and the rest
-    <= f (FP64 only; (ff|ff) with 128-lane groups) -- the nuclear-gradient
-    batches of an l <= 2 basis reach the one-f classes, an f basis reaches
-    them all."""
-    from .group_emitter import orientation
+    (FP64 and FP32-VRR variants), and every class with an f or g shell and the
+    rest <= g that group_fits (FP64 only; the nuclear-gradient batches of an
+    l <= 2 basis reach the one-f classes, an f basis the rest of the f
+    classes, l <= 4 bases the g classes).  (gf|gf), (gg|gf), (gg|gg) and
+    (gg|ss) stay on the generic kernel."""
     out = [(c, True) for c in canonical_classes(LMAX_EMIT)]
-    for c in canonical_classes(3):
-        if max(c) == 3 and orientation(*c) is not None:
+    for c in canonical_classes(4):
+        if max(c) >= 3 and group_fits(c):
             out.append((c, False))
     out.sort(key=lambda x: class_id(*x[0]))
     return out

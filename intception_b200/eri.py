@@ -92,6 +92,9 @@ def load():
     lib.intception_b200_schwarz.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                             C.c_void_p]
     lib.intception_b200_schwarz.restype = C.c_int
+    lib.intception_b200_quartet_bounds.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                                   C.c_void_p]
+    lib.intception_b200_quartet_bounds.restype = C.c_int
     lib.intception_b200_eri_graph_create.argtypes = [C.POINTER(_Basis), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                                      C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                                      C.c_void_p, C.POINTER(C.c_void_p)]
@@ -316,6 +319,20 @@ class EriEngine:
         q = self.schwarz(pairs, stream)
         return (q[:self.nq] * q[self.nq:]).contiguous()
 
+    def analytic_bounds(self, out=None, stream=None, quartets=None, nq=None):
+        """Per-quartet analytic screening bounds (intception_b200_quartet_bounds):
+        no ERI evaluated, one pass over the primitive pairs."""
+        torch = self.torch
+        q = self.quartets if quartets is None else quartets
+        n = self.nq if nq is None else nq
+        if out is None:
+            out = torch.empty(n, dtype=torch.float64, device=self.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        _check(load().intception_b200_quartet_bounds(C.byref(self._basis), q.data_ptr(), n,
+                                                     1 if self.spherical else 0, out.data_ptr(),
+                                                     C.c_void_p(s.cuda_stream)))
+        return out
+
     @staticmethod
     def last_launch_count():
         return load().intception_b200_last_launch_count()
@@ -383,7 +400,9 @@ class HostPipeline:
         every block of the batch: out_off[q] + na nb nc nd <= out_host.numel()
         for every quartet q (the device buffer is sized from it and the
         kernels write each block at its offset).  lmax: the largest shell l
-        (computed from shell_l when None)."""
+        (computed from shell_l when None).  Screening (skip_below > 0) and
+        PREC_MIXED use h['bounds'] when given, else the analytic bounds
+        (intception_b200_quartet_bounds) computed on the device with the batch."""
         torch = self.torch
         slot = self.slots[self.k % self.depth]
         self.k += 1
@@ -409,6 +428,11 @@ class HostPipeline:
         bas = _Basis(d['shell_l'].data_ptr(), d['shell_k'].data_ptr(), d['shell_ptr'].data_ptr(),
                      d['shell_xyz'].data_ptr(), d['prim_exp'].data_ptr(), d['prim_coef'].data_ptr(),
                      h['shell_l'].numel(), h['prim_exp'].numel(), lmax)
+        if 'bounds' not in d and (skip_below > 0.0 or precision == PREC_MIXED):
+            d['bounds'] = self._buffer(slot, 'bounds_dev', h['shell_xyz'], nq)
+            _check(load().intception_b200_quartet_bounds(C.byref(bas), d['quartets'].data_ptr(), nq,
+                                                         1 if self.spherical else 0, d['bounds'].data_ptr(),
+                                                         C.c_void_p(self.s_run.cuda_stream)))
         st = load().intception_b200_eri_batch(
             C.byref(bas), d['quartets'].data_ptr(), d['out_off'].data_ptr(), nq, 1 if self.spherical else 0,
             precision, d['bounds'].data_ptr() if 'bounds' in d else None, float(skip_below), float(fp32_below),

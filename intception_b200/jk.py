@@ -16,6 +16,12 @@ that index raised (coefficients 2 alpha c, l+1) and lowered (l-1), and
 differentiate, accumulating atom forces; the fourth centre follows from
 translational invariance.  Nothing from the forward pass is stored: backward
 recomputes every integral it needs.
+
+Several GPUs (one process each, torch.distributed initialised): every rank
+enumerates the same screened quartet chunks and digests every world-th quartet
+of each chunk (rank, rank + world, ...: neighbouring quartets cost about the
+same, so the shares balance); the partial E_J, E_K and the partial force array
+are then summed by one all_reduce each.  No quartet block crosses a GPU.
 """
 import ctypes as C
 
@@ -48,12 +54,18 @@ class JKSystem:
     """
 
     def __init__(self, atom_xyz, shell_atom, shell_l, shell_k, prim_exp, prim_coef, P_sph, device='cuda',
-                 screen=1e-15, chunk=1 << 21):
+                 screen=1e-15, chunk=1 << 21, rank=None, world=None, group=None, reduce=True):
         import torch
         self.torch = torch
         self.dev = torch.device(device)
         self.screen = float(screen)
         self.chunk = int(chunk)
+        # quartet shard of this process: rank r of world digests quartets r, r + world, ... of every chunk
+        dist_on = torch.distributed.is_available() and torch.distributed.is_initialized()
+        self.rank = int(rank if rank is not None else (torch.distributed.get_rank(group) if dist_on else 0))
+        self.world = int(world if world is not None else (torch.distributed.get_world_size(group) if dist_on else 1))
+        self.group = group
+        self.reduce = bool(reduce) and self.world > 1  # False: return this rank's partial sums
         l = np.asarray(shell_l, np.int32)
         k = np.asarray(shell_k, np.int32)
         e = np.asarray(prim_exp, np.float64)
@@ -164,23 +176,39 @@ class JKSystem:
                 yield torch.cat([pr[ii], pr[jj]], dim=1).to(torch.int32).contiguous()
             i0 = i1
 
+    # ------------------------------------------------------------------ shards
+    def shard(self, qt):
+        """This rank's quartets of a chunk: rows rank, rank + world, ..."""
+        return qt if self.world == 1 else qt[self.rank::self.world].contiguous()
+
+    def _sum_over_ranks(self, t):
+        """One all_reduce (sum) of a partial result over the ranks."""
+        if self.reduce:
+            self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.SUM, group=self.group)
+        return t
+
     # ------------------------------------------------------------------ energy
     def energy(self, xyz=None):
-        """(E_J, E_K) at the geometry xyz [natom,3]."""
+        """(E_J, E_K) at the geometry xyz [natom,3] (this rank's partial sums
+        when the system was made with reduce=False)."""
         torch = self.torch
         if xyz is not None:
             self.set_geometry(xyz)
         e = torch.zeros(2, dtype=torch.float64, device=self.dev)
-        lib = _lib()
-        stream = C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         for qt in self.quartet_chunks():
-            blocks, off = self._eri(qt, self.lmax)
-            eri._check(lib.intception_b200_jk_energy(qt.data_ptr(), off.data_ptr(), qt.shape[0],
-                                                     self.shell_l.data_ptr(), self.fofs.data_ptr(),
-                                                     self.P.data_ptr(), self.nbf_cart, blocks.data_ptr(),
-                                                     e.data_ptr(), stream))
-        ej, ek = e.tolist()
+            qt = self.shard(qt)
+            if qt.shape[0]:
+                self._energy_chunk(qt, e)
+        ej, ek = self._sum_over_ranks(e).tolist()
         return ej, ek
+
+    def _energy_chunk(self, qt, e):
+        """Adds the J/K energies of the unique quartets qt [n,4] to e[0:2]."""
+        blocks, off = self._eri(qt, self.lmax)
+        eri._check(_lib().intception_b200_jk_energy(
+            qt.data_ptr(), off.data_ptr(), qt.shape[0], self.shell_l.data_ptr(), self.fofs.data_ptr(),
+            self.P.data_ptr(), self.nbf_cart, blocks.data_ptr(), e.data_ptr(),
+            C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)))
 
     def gradient(self, xyz=None):
         """dE/dR [natom,3] of E = E_J + E_K at xyz (FP64)."""
@@ -188,27 +216,34 @@ class JKSystem:
         if xyz is not None:
             self.set_geometry(xyz)
         force = torch.zeros(self.natom * 3, dtype=torch.float64, device=self.dev)
+        for qt in self.quartet_chunks():
+            qt = self.shard(qt)
+            if qt.shape[0]:
+                self._force_chunk(qt, force)
+        return self._sum_over_ranks(force).view(self.natom, 3)
+
+    def _force_chunk(self, qt, force):
+        """Adds the adjoint gradient of the unique quartets qt [n,4] to force."""
+        torch = self.torch
         lib = _lib()
         stream = C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         lorig = self.shell_l[:self.ns]
-        for qt in self.quartet_chunks():
-            n = qt.shape[0]
-            for pos in range(3):
-                for sign in (1, -1):
-                    if sign > 0:
-                        sel = torch.arange(n, device=self.dev, dtype=torch.int32)
-                    else:
-                        sel = torch.nonzero(lorig[qt[:, pos].long()] >= 1).flatten().to(torch.int32)
-                    if sel.numel() == 0:
-                        continue
-                    aux = qt[sel.long()].clone()
-                    aux[:, pos] += self.ns if sign > 0 else 2 * self.ns
-                    blocks, off = self._eri(aux.contiguous(), self.lmax + 1)
-                    eri._check(lib.intception_b200_jk_force(
-                        qt.data_ptr(), sel.data_ptr(), off.data_ptr(), sel.numel(), pos, sign,
-                        self.shell_l.data_ptr(), self.fofs.data_ptr(), self.shell_atom.data_ptr(),
-                        self.P.data_ptr(), self.nbf_cart, self.natom, blocks.data_ptr(), force.data_ptr(), stream))
-        return force.view(self.natom, 3)
+        n = qt.shape[0]
+        for pos in range(3):
+            for sign in (1, -1):
+                if sign > 0:
+                    sel = torch.arange(n, device=self.dev, dtype=torch.int32)
+                else:
+                    sel = torch.nonzero(lorig[qt[:, pos].long()] >= 1).flatten().to(torch.int32)
+                if sel.numel() == 0:
+                    continue
+                aux = qt[sel.long()].clone()
+                aux[:, pos] += self.ns if sign > 0 else 2 * self.ns
+                blocks, off = self._eri(aux.contiguous(), self.lmax + 1)
+                eri._check(lib.intception_b200_jk_force(
+                    qt.data_ptr(), sel.data_ptr(), off.data_ptr(), sel.numel(), pos, sign,
+                    self.shell_l.data_ptr(), self.fofs.data_ptr(), self.shell_atom.data_ptr(),
+                    self.P.data_ptr(), self.nbf_cart, self.natom, blocks.data_ptr(), force.data_ptr(), stream))
 
 
 def _energy_function():
@@ -240,12 +275,12 @@ def jk_energy(xyz, system):
 
 
 def lattice_system(natom=60, seed=3, spacing=2.6, jitter=0.3, shells=((0, 6), (0, 3), (1, 3), (2, 1)),
-                   alpha=(0.1, 1e3), nocc=10, device='cuda', screen=1e-15):
+                   alpha=(0.1, 1e3), nocc=10, device='cuda', screen=1e-15, **shard):
     """Jittered cubic lattice: the first natom sites (row-major) of the smallest
     cube holding them, spacing 2.6 bohr, uniform +-0.3 bohr jitter; per atom the
     given (l, K) shells with exponents log-uniform in alpha and coefficients
     uniform [0.1, 1] then normalised; P = C C^T with C ~ normal(0, 0.1),
-    nbf x nocc."""
+    nbf x nocc.  shard: rank, world, group, reduce of JKSystem."""
     rng = np.random.default_rng(seed)
     n = int(np.ceil(natom ** (1.0 / 3.0) - 1e-9))
     sites = np.array([(i, j, k) for i in range(n) for j in range(n) for k in range(n)][:natom], np.float64)
@@ -257,7 +292,7 @@ def lattice_system(natom=60, seed=3, spacing=2.6, jitter=0.3, shells=((0, 6), (0
     nbf = int((2 * ls + 1).sum())
     Cm = rng.normal(0.0, 0.1, (nbf, nocc))
     P = Cm @ Cm.T
-    return JKSystem(xyz, atom, ls, ks, e, c, P, device=device, screen=screen), xyz
+    return JKSystem(xyz, atom, ls, ks, e, c, P, device=device, screen=screen, **shard), xyz
 
 
 def main(argv=None):

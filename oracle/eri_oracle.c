@@ -32,6 +32,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include "boys_tables.h"
+#include "pair_bound.h"
 
 #define OR_LMAX 8
 
@@ -677,4 +678,12 @@ void oracle_2idx_batch(int kind, int n, const double *xa, const double *ca, cons
     oracle_2idx(kind, xa[p], ca + 3 * p, la[p], na, 1, xb[p], cb + 3 * p, lb[p], nb, na, kind ? cc + 3 * p : NULL,
                 out + off[p]);
   }
+}
+
+/* The library's analytic screening bound of every quartet (pair_bound.h). */
+void oracle_quartet_bounds(int nq, const int *quartets, const int *shell_l, const int *shell_k, const int *shell_ptr,
+                           const double *shell_xyz, const double *prim_exp, const double *prim_coef, int spherical,
+                           double *bounds) {
+  for (int q = 0; q < nq; ++q)
+    bounds[q] = pb_quartet(quartets + 4 * q, shell_l, shell_k, shell_ptr, shell_xyz, prim_exp, prim_coef, spherical);
 }

@@ -47,6 +47,8 @@ def load_oracle():
         lib.oracle_eri_work_array_size.restype = C.c_int
         lib.oracle_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp, _dp]
         lib.oracle_eri_batch.restype = None
+        lib.oracle_quartet_bounds.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int, _dp]
+        lib.oracle_quartet_bounds.restype = None
         idx = [C.c_int] * 6
         per_cart = [_dp, _dp] + idx + [_dp]
         per_sph = per_cart + [_dp]
@@ -78,6 +80,8 @@ def load_ref(variant):
             lib.ref_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp,
                                           _dp, C.c_int]
             lib.ref_eri_batch.restype = C.c_int
+            lib.ref_eri_batch_screened.argtypes = lib.ref_eri_batch.argtypes + [C.c_double]
+            lib.ref_eri_batch_screened.restype = C.c_int
             lib.ref_work_array_size.argtypes = [C.c_int] * 12
             lib.ref_work_array_size.restype = C.c_int
             main = getattr(lib, 'intception_integral_eri_abcd_m_cont_%s_main' % variant)
@@ -172,6 +176,34 @@ def oracle_batch(b, sphT=None, exact_boys=False):
     finally:
         lib.oracle_set_boys_exact(0)
     return out
+
+
+def quartet_bounds(b):
+    """The library's analytic screening bound of every quartet (pair_bound.h),
+    with the C restatement."""
+    lib = load_oracle()
+    q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
+    out = np.zeros(b.nq)
+    lib.oracle_quartet_bounds(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz), _ptr(e),
+                              _ptr(c), 1 if b.spherical else 0, _ptr(out))
+    return out
+
+
+def ref_batch_screened(b, sphT, skip_below, nthreads=0, out=None):
+    """The reference-emitted C99 behind the library's analytic screening:
+    quartets whose bound is below skip_below get zero blocks.  Returns (out,
+    number evaluated), or (None, 0) when oracle/_ref was not built."""
+    lib = load_ref('sph' if b.spherical else 'cart')
+    if lib is None:
+        return None, 0
+    q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
+    if out is None:
+        out = np.zeros(b.out_size)
+    tab, keep = _sph_table(sphT) if b.spherical else (None, None)
+    n = lib.ref_eri_batch_screened(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz),
+                                   _ptr(e), _ptr(c), tab, _ptr(off, _lp), _ptr(out), int(nthreads),
+                                   float(skip_below))
+    return out, n
 
 
 def ref_batch(b, sphT=None, nthreads=0, out=None):

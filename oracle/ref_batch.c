@@ -11,7 +11,10 @@
  * fastest, index = ia + na*(ib + nb*(ic + nc*id)).
  */
 #include <stdlib.h>
+#include <string.h>
 #include <omp.h>
+
+#include "pair_bound.h"
 
 #if defined(REF_VARIANT_SPH)
 #include "intception_integral_eri_abcd_m_cont_sph.h"
@@ -79,4 +82,47 @@ int ref_eri_batch(int nq, const int *quartets, const int *shell_l, const int *sh
     free(work);
   }
   return nq;
+}
+
+/* The same batch with the library's screening in front of the reference's
+ * function: quartets whose analytic bound (pair_bound.h) is below skip_below
+ * get a zero block, the rest are evaluated by the emitted function, exactly as
+ * ref_eri_batch does.  Returns the number evaluated. */
+int ref_eri_batch_screened(int nq, const int *quartets, const int *shell_l, const int *shell_k, const int *shell_ptr,
+                           const double *shell_xyz, const double *prim_exp, const double *prim_coef,
+                           const double *const *sphT, const long long *out_off, double *out, int nthreads,
+                           double skip_below) {
+  if (nthreads <= 0) nthreads = omp_get_num_procs();
+#if defined(REF_VARIANT_SPH)
+  const int sph = 1;
+#else
+  const int sph = 0;
+#endif
+  int *keep = (int *)malloc(sizeof(int) * (size_t)(nq > 0 ? nq : 1));
+  int nkeep = 0;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 256)
+  for (int q = 0; q < nq; ++q) {
+    const int *s = quartets + 4 * q;
+    const double bnd = pb_quartet(s, shell_l, shell_k, shell_ptr, shell_xyz, prim_exp, prim_coef, sph);
+    if (bnd < skip_below) {
+      int tot = 1;
+      for (int i = 0; i < 4; ++i) tot *= sph ? 2 * shell_l[s[i]] + 1 : rb_ncart(shell_l[s[i]]);
+      memset(out + out_off[q], 0, sizeof(double) * (size_t)tot);
+      keep[q] = 0;
+    } else {
+      keep[q] = 1;
+    }
+  }
+  int *kq = (int *)malloc(sizeof(int) * 4 * (size_t)(nq > 0 ? nq : 1));
+  long long *ko = (long long *)malloc(sizeof(long long) * (size_t)(nq > 0 ? nq : 1));
+  for (int q = 0; q < nq; ++q)
+    if (keep[q]) {
+      for (int i = 0; i < 4; ++i) kq[4 * nkeep + i] = quartets[4 * q + i];
+      ko[nkeep++] = out_off[q];
+    }
+  ref_eri_batch(nkeep, kq, shell_l, shell_k, shell_ptr, shell_xyz, prim_exp, prim_coef, sphT, ko, out, nthreads);
+  free(keep);
+  free(kq);
+  free(ko);
+  return nkeep;
 }

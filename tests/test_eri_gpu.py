@@ -248,6 +248,37 @@ def test_every_f_class_vs_oracle(dist, sph):
     assert np.abs(out - ref).max() <= tol * max(1.0, float(np.abs(ref).max()))
 
 
+G_DISTS = [(0.3, 5.0, 3.0), (0.3, 5.0, 6.0), (0.5, 20.0, 4.0), (0.1, 40.0, 3.0)]
+
+
+@pytest.mark.parametrize('sph', [False, True])
+@pytest.mark.parametrize('dist', range(len(G_DISTS)))
+def test_every_g_class_vs_oracle(dist, sph):
+    """All 369 (la,lb,lc,ld) orderings with l <= 4 and at least one g shell:
+    the unrolled lane-group kernels (61 canonical classes) and the generic
+    kernel for (gf|gf), (gg|gf), (gg|gg) and (gg|ss); K 1..2, fresh shells."""
+    lo, hi, box = G_DISTS[dist]
+    rng = np.random.default_rng(157 + sph + 10 * dist)
+    quartets, ls = [], []
+    for la in range(5):
+        for lb in range(5):
+            for lc in range(5):
+                for ld in range(5):
+                    if max(la, lb, lc, ld) < 4:
+                        continue
+                    base = len(ls)
+                    ls += [la, lb, lc, ld]
+                    quartets.append([base, base + 1, base + 2, base + 3])
+    ks = rng.integers(1, 3, len(ls)).astype(np.int32)
+    l_, k_, p_, xyz, e, c = basis.make_shells(rng, np.array(ls, np.int32), ks, lo, hi, box)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    b = basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
+    ref = loader.oracle_batch(b, basis.sph_matrices(6))
+    out = run_batch(b)
+    assert np.abs(out - ref).max() <= tolerance(ref)
+
+
 def test_boys_dropin_vs_reference():
     z = np.load(GOLDEN + '/boys.npz')
     nmax = int(z['nmax'])
@@ -478,3 +509,24 @@ def test_c1_every_quartet_through_the_dropin():
         r = ref[b.out_off[q]:b.out_off[q] + 81]
         worst = max(worst, float(np.abs(out - r).max()))
     assert worst <= 1e-12, worst
+
+
+@pytest.mark.parametrize('sph', [False, True])
+def test_analytic_quartet_bounds_match_oracle_and_cover_blocks(sph):
+    """intception_b200_quartet_bounds against its C restatement (oracle/pair_bound.h)
+    to 1e-12 relative, over l <= 6; every block of the batch path stays within
+    its bound, and screening with it errs by no more than the threshold."""
+    import torch
+    b = basis.independent_quartet_batch(131 + sph, 600, [0, 1, 2, 3, 4, 5, 6], [1, 2, 3, 6], 0.05, 1e4, 8.0, sph)
+    eng = eri.EriEngine(b)
+    dev = eng.analytic_bounds().cpu().numpy()
+    ora = loader.quartet_bounds(b)
+    assert np.all(np.abs(dev - ora) <= 1e-12 * np.abs(ora) + 1e-300)
+    out = run_batch(b)
+    sizes = basis.block_sizes(b.shell_l, b.quartets, b.spherical)
+    for q in range(b.nq):
+        assert np.abs(out[b.out_off[q]:b.out_off[q] + sizes[q]]).max() <= dev[q]
+    thr = float(np.quantile(dev, 0.5))
+    scr = eng.compute(bounds=torch.from_numpy(dev).cuda(), skip_below=thr)
+    torch.cuda.synchronize()
+    assert np.abs(scr.cpu().numpy() - out).max() <= thr

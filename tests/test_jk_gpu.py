@@ -79,3 +79,19 @@ def test_jk_autograd_function():
     g = sys_.gradient(xyz).cpu().numpy()
     assert np.allclose(x.grad.numpy(), g, atol=1e-13, rtol=0)
     assert abs(float(e) - sum(sys_.energy(xyz))) <= 1e-12
+
+
+def test_jk_shards_add_up_on_one_gpu():
+    """The two shards of a world-2 run, evaluated one after the other on this
+    GPU with the all_reduce left out (reduce=False), add up to the one-rank
+    energies and gradient to 1e-12."""
+    one, xyz = small_system()
+    e1 = one.energy(xyz)
+    g1 = one.gradient(xyz).cpu().numpy()
+    parts = [jk.lattice_system(natom=3, seed=7, shells=((0, 3), (1, 2), (2, 1)), alpha=(0.2, 30.0), nocc=4,
+                               screen=1e-16, rank=r, world=2, reduce=False)[0] for r in range(2)]
+    es = [p.energy(xyz) for p in parts]
+    gs = [p.gradient(xyz).cpu().numpy() for p in parts]
+    for k in range(2):
+        assert abs(es[0][k] + es[1][k] - e1[k]) <= 1e-12 * max(1.0, abs(e1[k]))
+    assert np.abs(gs[0] + gs[1] - g1).max() <= 1e-12 * max(1.0, np.abs(g1).max())

@@ -104,3 +104,38 @@ def test_device_sph_colsums_cover_library_matrices():
     assert len(vals) == 6
     for v, w in zip(vals, want):
         assert v >= w and v <= w * (1 + 1e-12)
+
+
+@pytest.mark.parametrize('name', ['mixed_l2_sph_c2', 'mixed_l2_sph_compact', 'mixed_l2_cart_compact', 'l4_cart',
+                                  'l4_sph', 'l6_cart', 'l6_sph', 'edge_cart', 'edge_sph'])
+def test_oracle_quartet_bound_covers_reference_blocks(name):
+    """The analytic screening bound (oracle/pair_bound.h, the restatement of
+    intception_b200_quartet_bounds) is at least max |element| of every block
+    the reference's emitted C99 wrote for the golden fixtures."""
+    from conftest import load_batch
+    b, T, ref = load_batch(name)
+    bd = loader.quartet_bounds(b)
+    sizes = basis.block_sizes(b.shell_l, b.quartets, b.spherical)
+    for q in range(b.nq):
+        m = float(np.abs(ref[b.out_off[q]:b.out_off[q] + sizes[q]]).max())
+        assert m <= bd[q], (q, m, bd[q])
+
+
+def test_oracle_quartet_bound_matches_numpy_restatement():
+    """pair_bound.h against the numpy pair_bound above summed over primitives."""
+    b = basis.config_mixed_l2(nq=200, seed=5, spherical=True)
+    bd = loader.quartet_bounds(b)
+    for q in range(b.nq):
+        qs = []
+        for side in range(2):
+            s0, s1 = b.quartets[q, 2 * side], b.quartets[q, 2 * side + 1]
+            r = float(np.linalg.norm(b.shell_xyz[s0] - b.shell_xyz[s1]))
+            tot = 0.0
+            for i in range(b.shell_k[s0]):
+                for j in range(b.shell_k[s1]):
+                    p0, p1 = b.shell_ptr[s0] + i, b.shell_ptr[s1] + j
+                    tot += pair_bound(int(b.shell_l[s0]), int(b.shell_l[s1]), b.prim_exp[p0], b.prim_coef[p0],
+                                      b.prim_exp[p1], b.prim_coef[p1], r, True)
+            qs.append(tot)
+        want = qs[0] * qs[1] * 1.000001 ** 5  # each stage widened by 1 + 1e-6, as on the device
+        assert abs(bd[q] - want) <= 1e-12 * abs(bd[q]) + 1e-300
