@@ -98,6 +98,14 @@ def group_size(n):
 # pack ten-lane groups three to a warp (False: pad them to 16 lanes, two per warp)
 PACK_TEN = True
 
+# lane sides of 21..63 components whose levels below the top fit in fewer than
+# 32 lanes (the S_hi = 4 sides: 20 low + 15 top components): every warp of the
+# group holds all the low levels plus its share of the top level, so the
+# transfer operands stay inside the warp (shuffles, no per-level barrier); the
+# low levels are evaluated once per warp (False: one copy, transfer operands
+# through shared memory with a named barrier per level)
+DUP_LOW = True
+
 # register budgets offered to the autotuner: __launch_bounds__(IB_BLOCK, MINB)
 # asks for MINB resident blocks per SM (1: no register cap); must match
 # IB_MINB_VALUES in ib_eri_device.cuh
@@ -125,9 +133,19 @@ class GroupEmitter:
         self.packed = PACK_TEN and self.NL == 10
         if self.packed:
             self.G = 10
-        # G = 64 or 128: two or four warps per quartet; transfer operands go
-        # through shared memory, one named barrier per recurrence level
+        # duplicated low levels (DUP_LOW): warp q of the group holds every
+        # component below the top level in lanes 0..nlow-1 and top-level
+        # components q*per .. q*per+per-1 in the others
+        self.dup = DUP_LOW and self.NL > 32 and ncum(self.S_hi - 1) < 32
+        if self.dup:
+            self.nlow = ncum(self.S_hi - 1)
+            self.per = 32 - self.nlow
+            self.ntop = ncart(self.S_hi)
+            self.G = 32 * (-(-self.ntop // self.per))
+        # G = 64 or 128: two or four warps per quartet; without dup, transfer
+        # operands go through shared memory, one named barrier per recurrence level
         self.wide = self.G > 32
+        self.smem_xfer = self.wide and not self.dup
         self.QPW = max(1, 32 // self.G)
         self.tag = '%d%d%d%d' % (la, lb, lc, ld)
         self.cid = class_id(la, lb, lc, ld)
@@ -139,11 +157,22 @@ class GroupEmitter:
         self.shuffles = {}
 
     # -------------------------------------------------------------- lane table
+    def lane_comp(self, j):
+        """(component, index of the lane that serves as lane 0 for its transfer
+        sources) of group lane j."""
+        if self.dup:
+            w, jw = divmod(j, 32)
+            if jw < self.nlow:
+                return comps_range(0, self.S_hi - 1)[jw], jw
+            t = min(w * self.per + jw - self.nlow, self.ntop - 1)  # padding lanes mirror the last one
+            return comps(self.S_hi)[t], jw
+        jj = min(j, self.NL - 1)  # padding lanes mirror the last component
+        return comps_range(0, self.S_hi)[jj], jj
+
     def lane_table(self):
         rows = []
         for j in range(self.G):
-            jj = min(j, self.NL - 1)  # padding lanes mirror the last component
-            c = comps_range(0, self.S_hi)[jj]
+            c, jj = self.lane_comp(j)
             dirs, nbs = [], []
             for d in (2, 1, 0):
                 for k in range(c[d]):
@@ -194,7 +223,7 @@ class GroupEmitter:
             fl += 4
         if self.S_hi > 0:
             # transfer term from the lane owning s - 1i
-            if self.wide:
+            if self.smem_xfer:
                 lvl = sum(cm)
                 slot = self.slot_index(cm, m + 1)
                 expr += ' + tf%s * xb%d[%d * %d + src%s]' % (d, lvl % 2, slot, self.G, 'xyz'.index(d))
@@ -218,6 +247,8 @@ class GroupEmitter:
         relative lanes for power-of-two groups, absolute lanes when packed)."""
         if self.packed:
             return '__shfl_sync(gmask, %s, src%d)' % (name, i)
+        if self.dup:
+            return '__shfl_sync(0xffffffffu, %s, src%d, 32)' % (name, i)
         return '__shfl_sync(gmask, %s, src%d, %d)' % (name, i, self.G)
 
     def slot_index(self, c, m):
@@ -322,7 +353,7 @@ class GroupEmitter:
         """Chain side level by level: the level's transfer operands are fetched
         with back-to-back shuffles first (their latency overlaps), then its
         nodes, then the accumulation of the level's targets."""
-        if self.wide:
+        if self.smem_xfer:
             return self.emit_chain_wide()
         if chain_order(self.tag) == 'dfs':
             return self.emit_chain_dfs()
@@ -554,6 +585,8 @@ class GroupEmitter:
             src.append('  const int gid = threadIdx.x / %d, j = threadIdx.x %% %d;' % (self.G, self.G))
             src.append('  const unsigned gmask = 0xffffffffu;')
             src.append('  const unsigned sgmask = 0xffffffffu;')
+            if self.dup:
+                src.append('  const int jw = j & 31, wq = j >> 5;  // lane in its warp, warp in the group')
         else:
             src.append('  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;')
             src.append('  const int gq = lane / %d, j = lane %% %d;' % (self.G, self.G))
@@ -575,7 +608,7 @@ class GroupEmitter:
         # live only inside the primitive loop, the contracted table only after
         # it (behind the super-group sync that closes the last tile): they
         # share the area at the start of the group's block
-        xb_len = 2 * self.n_slots() * self.G if self.wide else 0
+        xb_len = 2 * self.n_slots() * self.G if self.smem_xfer else 0
         loop_len = xb_len + (nfield * self.G if self.G > 1 else 0)
         per_group = max(smem_group, loop_len)
         self.list_off = per_group
@@ -588,7 +621,7 @@ class GroupEmitter:
         src.append('  double* __restrict__ sb = ib_smem + gid * %d;' % per_group)
         src.append('  double* __restrict__ sb0 = ib_smem + sg * W * %d;  // slice 0'
                    % per_group)
-        if self.wide:
+        if self.smem_xfer:
             src.append('  R* __restrict__ xb0 = reinterpret_cast<R*>(sb);')
             src.append('  R* __restrict__ xb1 = xb0 + %d;' % (self.n_slots() * self.G))
             src.append('  (void)xb1;')
@@ -606,6 +639,8 @@ class GroupEmitter:
         if self.packed:
             src.append('  const int src0 = gq * %d + ((lmisc >> 9) & 127), src1 = gq * %d + ((lmisc >> 16) & 127), '
                        'src2 = gq * %d + ((lmisc >> 23) & 127);' % (self.G, self.G, self.G))
+        elif self.dup:  # lanes of this warp
+            src.append('  const int src0 = (lmisc >> 9) & 31, src1 = (lmisc >> 16) & 31, src2 = (lmisc >> 23) & 31;')
         else:
             src.append('  const int src0 = (lmisc >> 9) & 127, src1 = (lmisc >> 16) & 127, src2 = (lmisc >> 23) & 127;')
         src.append('  const double lcx = (double)(lmisc & 7), lcy = (double)((lmisc >> 3) & 7), '
@@ -693,10 +728,15 @@ class GroupEmitter:
         else:
             # lane j sets up live primitive quartet q0 + j of the chunk; the
             # group then sweeps the chunk reading the shared values (broadcast)
-            sync = 'ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'
-            src.append('      for (int q0 = w * %d; q0 < npl; q0 += W * %d) {' % (self.G, self.G))
+            sync = 'ib_group_bar(gid)' if self.smem_xfer else ('__syncwarp()' if self.dup else '__syncwarp(gmask)')
+            # dup: every warp of the group sets up the same chunk of 32
+            # primitive quartets for itself (its own slots of the table)
+            CH = 32 if self.dup else self.G
+            jl = 'jw' if self.dup else 'j'
+            self.chunk = CH
+            src.append('      for (int q0 = w * %d; q0 < npl; q0 += W * %d) {' % (CH, CH))
             src.append('        {')
-            src.append('          const int q = q0 + j;')
+            src.append('          const int q = q0 + %s;' % jl)
             src.append('          if (q < npl) {')
             src.append('            const int qa = (int)(((float)q + 0.5f) * rn1), qc = q - qa * nl1;')
             src.append('            const int ab = ab0 + lst[qa], cd = cd0 + lst[64 + qc];')
@@ -718,6 +758,8 @@ class GroupEmitter:
             src.append('              if (sizeof(R) == 4) est += %s;' % self.err_expr())
             src.append('            }')
             src.append('            pz[j] = live ? 1 : 0;  // 0: pair prefactors multiply to zero, or screened out')
+            # dup: sums of the bound run over this warp's setup lanes only (every
+            # warp of the group set up the same primitive quartets)
             src.append('          }')
             src.append('        }')
             src.append('        %s;' % sync)
@@ -731,6 +773,8 @@ class GroupEmitter:
                 src.append('          eg = 0.0;')
                 src.append('          for (int v = 0; v < %d; ++v) eg += sb[%d + v];' % (self.G, self.red_off))
                 src.append('          __syncwarp(gmask);')
+            elif self.dup:
+                src.append('          for (int o = 16; o > 0; o >>= 1) eg += __shfl_xor_sync(0xffffffffu, eg, o);')
             elif self.wide:
                 src.append('          for (int o = 16; o > 0; o >>= 1) eg += __shfl_xor_sync(0xffffffffu, eg, o);')
                 src.append('          if ((j & 31) == 0) sb[%d + (j >> 5)] = eg;' % self.red_off)
@@ -742,13 +786,14 @@ class GroupEmitter:
                            % (self.G // 2, self.G))
             src.append('          if (eg * famp > a.mixed_tol) break;  // uniform over the group')
             src.append('        }')
-            src.append('        const int nu = min(%d, npl - q0);' % self.G)
+            src.append('        const int nu = min(%d, npl - q0);' % CH)
+            ub = 'wq * 32 + u' if self.dup else 'u'
             src.append('        for (int u = 0; u < nu; ++u) {')
-            src.append('          if (!pz[u]) continue;  // group-uniform: exact-zero primitive quartet')
+            src.append('          if (!pz[%s]) continue;  // group-uniform: exact-zero primitive quartet' % ub)
             for k, nm in enumerate(names):
-                src.append('          const R %s = ps[%d * %d + u];' % (nm, k, self.G))
+                src.append('          const R %s = ps[%d * %d + %s];' % (nm, k, self.G, ub))
             for m in range(L + 1):
-                src.append('        const R f%d = ps[%d * %d + u];' % (m, len(fields) + m, self.G))
+                src.append('        const R f%d = ps[%d * %d + %s];' % (m, len(fields) + m, self.G, ub))
         if bra:
             src.append('        const R SXx = PAx, SXy = PAy, SXz = PAz, SWx = WPx, SWy = WPy, SWz = WPz;')
             src.append('        const R so2 = o2z, sro = roz;')
@@ -788,7 +833,8 @@ class GroupEmitter:
             src.append('      }')
         else:
             src.append('        }')
-            src.append('        %s;' % ('ib_group_bar(gid)' if self.wide else '__syncwarp(gmask)'))
+            src.append('        %s;' % ('ib_group_bar(gid)' if self.smem_xfer else
+                                        ('__syncwarp()' if self.dup else '__syncwarp(gmask)')))
             src.append('      }')
         src.append('      ib_sg_sync(SG, sg, sgmask);  // every slice is done with the lists before the next tile')
         src.append('    }')
@@ -803,6 +849,8 @@ class GroupEmitter:
         elif self.G > 1 and not self.wide:
             src.append('      for (int o = %d; o > 0; o >>= 1) est += __shfl_xor_sync(gmask, est, o, %d);'
                        % (self.G // 2, self.G))
+        elif self.dup:  # every warp holds the whole group's sum
+            src.append('      for (int o = 16; o > 0; o >>= 1) est += __shfl_xor_sync(0xffffffffu, est, o);')
         elif self.wide:
             src.append('      for (int o = 16; o > 0; o >>= 1) est += __shfl_xor_sync(0xffffffffu, est, o);')
             src.append('      ib_group_bar(gid);')
@@ -824,15 +872,32 @@ class GroupEmitter:
         src.append('      }')
         src.append('    }')
         # accumulators -> shared [e][f]
-        if bra:
-            src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
+        if self.dup:
+            # the row of this lane's component; the low levels are written by
+            # the group's first warp, padding lanes write nothing
+            src.append('    {')
+            src.append('      const int cx = lmisc & 7, cy = (lmisc >> 3) & 7, cz = (lmisc >> 6) & 7, cl = cx + cy + cz;')
+            src.append('      const int crow = cl * (cl + 1) * (cl + 2) / 6 + cz + (cy + cz) * (cy + cz + 1) / 2;')
+            src.append('      const bool mine = jw < %d ? wq == 0 : wq * %d + jw - %d < %d;'
+                       % (self.nlow, self.per, self.nlow, self.ntop))
+            src.append('      if (mine && crow >= %d) {' % s_lo_idx)
             for tt in range(NT):
-                src.append('      sb[(j - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NFP, tt, tt))
+                if bra:
+                    src.append('        sb[(crow - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NFP, tt, tt))
+                else:
+                    src.append('        sb[%d * %d + (crow - %d)] = acc[%d];' % (tt, NFP, s_lo_idx, tt))
+            src.append('      }')
+            src.append('    }')
         else:
-            src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
-            for tt in range(NT):
-                src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NFP, s_lo_idx, tt))
-        src.append('    }')
+            if bra:
+                src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
+                for tt in range(NT):
+                    src.append('      sb[(j - %d) * %d + %d] = acc[%d];' % (s_lo_idx, NFP, tt, tt))
+            else:
+                src.append('    if (j >= %d && j < %d) {' % (s_lo_idx, self.NL))
+                for tt in range(NT):
+                    src.append('      sb[%d * %d + (j - %d)] = acc[%d];' % (tt, NFP, s_lo_idx, tt))
+            src.append('    }')
         src.append('    ib_sg_sync(SG, sg, sgmask);')
         src.append('    if (W > 1) {  // slice 0 table += the other slices tables')
         src.append('      for (int x = r; x < %d; x += SG) {' % (NE * NF))
