@@ -819,6 +819,7 @@ def run_eri(args, rank, world, local):
     flops, _ = alg_flops(batch)
     flops_kept, _ = alg_flops(batch.subset(kept_idx)) if n_kept else (0.0, None)
     peak64 = eri.fma_peak(True)
+    peak32 = eri.fma_peak(False)  # the FP32 tier's pipe: its rate over FP64's bounds what FP32 VRR can gain
     achieved = flops / (ms64 * 1e-3)
     roofline = {'bound': 'fp64', 'achieved': achieved / 1e12, 'peak': peak64 / 1e12, 'unit': 'TFLOP/s',
                 'frac': achieved / peak64 if peak64 else None, 'traffic': None,
@@ -910,6 +911,8 @@ def run_eri(args, rank, world, local):
                           'note': 'fp32_below chosen by the sweep (fastest within 1e-10), then measured again '
                                   'on its own; the same screening as fp64_screened'},
                 'mixed_over_fp64': value / rate(ms_s),
+                'fma_peaks_tflops': {'fp64': peak64 / 1e12, 'fp32': peak32 / 1e12, 'fp32_over_fp64': peak32 / peak64,
+                                     'source': 'intception_b200_fma_peak, this run (independent FMA chains)'},
                 'screening_gain': rate(ms_s) / rate(ms64),
                 'kept_fraction': n_kept / batch.nq,
                 'cuda_graph': {'ms_per_step': ms_graph, 'max_abs_err_vs_fp64': err_graph},
