@@ -205,6 +205,62 @@ __device__ __forceinline__ void ib_boys(double T, const double* __restrict__ tab
   }
 }
 
+// FP32 Boys for the FP32 tier's setup: the same scheme, the table values
+// rounded to float, the arithmetic in float (T and the grid offset in FP64).
+// Relative error of every F_m <= IB_F32_SETUP_ROUNDINGS x 2^-24 (7 Taylor
+// roundings and the table's, 3 per recursion step, 2 ulp of expf).
+template <int L>
+__device__ __forceinline__ void ib_boys_f32(double T, const double* __restrict__ tab, double* F) {
+  float f32[L + 1];
+  if (T < IB_BOYS_TMAX) {
+    const int i = __double2int_rn(T * (double)IB_BOYS_H_INV);
+    const float dx = (float)((double)i * (1.0 / IB_BOYS_H_INV) - T);
+    const double* r = tab + i * IB_BOYS_NCOL + L;
+    float f = (float)__ldg(r + 6) * (1.0f / 720.0f);
+    f = fmaf(f, dx, (float)__ldg(r + 5) * (1.0f / 120.0f));
+    f = fmaf(f, dx, (float)__ldg(r + 4) * (1.0f / 24.0f));
+    f = fmaf(f, dx, (float)__ldg(r + 3) * (1.0f / 6.0f));
+    f = fmaf(f, dx, (float)__ldg(r + 2) * 0.5f);
+    f = fmaf(f, dx, (float)__ldg(r + 1));
+    f = fmaf(f, dx, (float)__ldg(r));
+    f32[L] = f;
+    if (L > 0) {
+      const float e = expf((float)-T), t2 = (float)(T + T);
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) f32[m] = fmaf(t2, f32[m + 1], e) * (1.0f / (2 * m + 1));
+    }
+  } else {
+    const float oT = 1.0f / (float)T;
+    f32[0] = sqrtf(0.78539816339744830962f * oT);
+    if (L > 0) {
+      const float he = 0.5f * expf((float)-T);
+#pragma unroll
+      for (int m = 0; m < L; ++m) f32[m + 1] = fmaf((float)m + 0.5f, f32[m], -he) * oT;
+    }
+  }
+#pragma unroll
+  for (int m = 0; m <= L; ++m) F[m] = (double)f32[m];
+}
+// Extra roundings of unit 2^-24 in the FP32 setup's scaled Boys values (Boys in
+// float <= 7 + 1 + 3 L + 2 for L <= 16, the float prefactor exponentials and
+// square root 5), counted into the FP32 tier's error bound.
+#define IB_F32_SETUP_ROUNDINGS 72
+
+// 1/x: a float reciprocal refined by one FP64 Newton step (relative error
+// ~2^-46, far below the FP32 tier's rounding unit), for the FP32 setup.
+__device__ __forceinline__ double ib_rcp_refined(double x) {
+  double r = (double)(1.0f / (float)x);
+  return r * fma(-x, r, 2.0);
+}
+
+// Pair prefactor for the FP32 setup: expf where its result stays a normal
+// float (the argument above -80), the FP64 exp below, so that the prefactor is
+// zero exactly where the FP64 one is and primitive quartets are culled alike.
+__device__ __forceinline__ double ib_pair_factor_f32(double xa, double ca, double xb, double cb, double oz, double r2) {
+  const double arg = -xa * xb * oz * r2;
+  return ca * cb * (arg > -80.0 ? (double)expf((float)arg) : exp(arg));
+}
+
 // Runtime-L variant reading the global table directly (one thread, no staging).
 __device__ inline void ib_boys_rt(double T, int L, const double* __restrict__ tab, double* F) {
   if (T < IB_BOYS_TMAX) {
@@ -235,16 +291,19 @@ __device__ inline void ib_boys_rt(double T, int L, const double* __restrict__ ta
 // |s0| g^S h^C with g^2 >= aS g + bS (base chain: aS = |X|+|W|, bS =
 // S (1+r)/2x) and h^2 >= (aC + tC/g) h + bC (chain side with the transfer
 // term tC = S/2(zeta+eta)); each value passes through at most 4(S+C)+2
-// roundings of unit 2^-24.
+// roundings of unit 2^-24, plus `extra` for inputs that carry rounding errors
+// of their own.  g and h are found in float (a few ulp each); the factor
+// 1.0001 covers their rounding through the powers (S + C <= 16).
 __device__ __forceinline__ double ib_fp32_err(double s0, double aS, double bS, int S, double aC, double bC,
-                                              double tC, int C) {
-  const double g = fmax(0.5 * (aS + sqrt(aS * aS + 4.0 * bS)), 1.0);
-  const double a2 = aC + tC / g;
-  const double h = fmax(0.5 * (a2 + sqrt(a2 * a2 + 4.0 * bC)), 1.0);
-  double v = fabs(s0);
-  for (int i = 0; i < S; ++i) v *= g;
-  for (int i = 0; i < C; ++i) v *= h;
-  return (4.0 * (S + C) + 2.0) * 5.9604644775390625e-08 * v;
+                                              double tC, int C, int extra = 0) {
+  const float as = (float)aS, bs = (float)bS;
+  const float g = fmaxf(0.5f * (as + sqrtf(as * as + 4.0f * bs)), 1.0f);
+  const float a2 = (float)aC + (float)tC / g;
+  const float h = fmaxf(0.5f * (a2 + sqrtf(a2 * a2 + 4.0f * (float)bC)), 1.0f);
+  float gh = 1.0001f;
+  for (int i = 0; i < S; ++i) gh *= g;
+  for (int i = 0; i < C; ++i) gh *= h;
+  return (4.0 * (S + C) + 2.0 + extra) * 5.9604644775390625e-08 * fabs(s0) * (double)gh;
 }
 
 __device__ __forceinline__ double ib_amax3(double x, double y, double z) { return fmax(fabs(x), fmax(fabs(y), fabs(z))); }
@@ -295,12 +354,15 @@ __device__ __forceinline__ double ib_pair_factor(double xa, double ca, double xb
   return ca * cb * exp(-xa * xb * oz * r2);
 }
 
+// Bra pair of primitives ia, ib.  F32SETUP (the FP32 tier): the reciprocal by
+// ib_rcp_refined and the prefactor by ib_pair_factor_f32.
+template <bool F32SETUP = false>
 __device__ __forceinline__ void ib_bra_pair(const IbLaunch& a, const IbQuartet& g, int ia, int ib, IbBraPair& bp) {
   const double xa = __ldg(a.prim_exp + g.ptr[0] + ia), ca = __ldg(a.prim_coef + g.ptr[0] + ia);
   const double xb = __ldg(a.prim_exp + g.ptr[1] + ib), cb = __ldg(a.prim_coef + g.ptr[1] + ib);
   bp.zeta = xa + xb;
-  bp.oz = 1.0 / bp.zeta;
-  bp.K = ib_pair_factor(xa, ca, xb, cb, bp.oz, g.RAB2);
+  bp.oz = F32SETUP ? ib_rcp_refined(bp.zeta) : 1.0 / bp.zeta;
+  bp.K = F32SETUP ? ib_pair_factor_f32(xa, ca, xb, cb, bp.oz, g.RAB2) : ib_pair_factor(xa, ca, xb, cb, bp.oz, g.RAB2);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     bp.P[d] = (xa * g.A[d] + xb * g.B[d]) * bp.oz;
@@ -514,10 +576,14 @@ __device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuart
                                                 IbPrimQuartet<R>& pq) {
   const double xc = __ldg(a.prim_exp + g.ptr[2] + ic), cc = __ldg(a.prim_coef + g.ptr[2] + ic);
   const double xd = __ldg(a.prim_exp + g.ptr[3] + id), cd = __ldg(a.prim_coef + g.ptr[3] + id);
-  const double eta = xc + xd, oe = 1.0 / eta;
-  const double Kcd = ib_pair_factor(xc, cc, xd, cd, oe, g.RCD2);
+  // the FP32 tier (R = float) computes the reciprocals, exponentials, square
+  // root and Boys values in float (reciprocals refined in FP64); its error
+  // bound counts IB_F32_SETUP_ROUNDINGS more roundings for the scaled F_m
+  constexpr bool F32 = sizeof(R) == 4;
+  const double eta = xc + xd, oe = F32 ? ib_rcp_refined(eta) : 1.0 / eta;
+  const double Kcd = F32 ? ib_pair_factor_f32(xc, cc, xd, cd, oe, g.RCD2) : ib_pair_factor(xc, cc, xd, cd, oe, g.RCD2);
   if (bp.K * Kcd == 0.0) return false;
-  const double ozpe = 1.0 / (bp.zeta + eta);
+  const double ozpe = F32 ? ib_rcp_refined(bp.zeta + eta) : 1.0 / (bp.zeta + eta);
   const double rho = bp.zeta * eta * ozpe;
   double Q[3], PQ[3];
 #pragma unroll
@@ -526,8 +592,11 @@ __device__ __forceinline__ bool ib_prim_quartet(const IbLaunch& a, const IbQuart
     PQ[d] = bp.P[d] - Q[d];
   }
   const double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
-  ib_boys<L>(rho * RPQ2, boys_tab, F);
-  const double pref = ib_two_pi52() * bp.oz * oe * sqrt(ozpe) * bp.K * Kcd;
+  if (F32)
+    ib_boys_f32<L>(rho * RPQ2, boys_tab, F);
+  else
+    ib_boys<L>(rho * RPQ2, boys_tab, F);
+  const double pref = ib_two_pi52() * bp.oz * oe * (F32 ? (double)sqrtf((float)ozpe) : sqrt(ozpe)) * bp.K * Kcd;
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;
 #pragma unroll

@@ -344,7 +344,7 @@ class Emitter:
         src.append('    for (int ia = 0; ia < g.k[0]; ++ia)')
         src.append('    for (int ib = 0; ib < g.k[1]; ++ib) {')
         src.append('      IbBraPair bp;')
-        src.append('      ib_bra_pair(a, g, ia, ib, bp);')
+        src.append('      ib_bra_pair<sizeof(R) == 4>(a, g, ia, ib, bp);')
         src.append('      if (bp.K == 0.0) continue;')
         src.append('      for (int ic = 0; ic < g.k[2]; ++ic)')
         src.append('      for (int id = 0; id < g.k[3]; ++id) {')

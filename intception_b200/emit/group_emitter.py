@@ -508,7 +508,7 @@ class GroupEmitter:
             aC = 'ib_amax3(pq.PA[0], pq.PA[1], pq.PA[2]) + ib_amax3(pq.WP[0], pq.WP[1], pq.WP[2])'
             bC = '%d.0 * (1.0 + (double)pq.roz) * (double)pq.o2z' % C
         tC = '%d.0 * (double)pq.o2zpe' % S
-        return 'ib_fp32_err(F[0], %s, %s, %d, %s, %s, %s, %d)' % (aS, bS, S, aC, bC, tC, C)
+        return 'ib_fp32_err(F[0], %s, %s, %d, %s, %s, %s, %d, IB_F32_SETUP_ROUNDINGS)' % (aS, bS, S, aC, bC, tC, C)
 
     def amp_expr(self):
         """Growth of an accumulator error through the HRRs and transforms."""
@@ -710,7 +710,7 @@ class GroupEmitter:
             src.append('        const int ab = ab0 + lst[qa], cd = cd0 + lst[64 + qc];')
             src.append('        if (ab != ab_last) {')
             src.append('          const int ia = (int)(((float)ab + 0.5f) * rkb), ib = ab - ia * kb_;')
-            src.append('          ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('          ib_bra_pair<sizeof(R) == 4>(a, g, ia, ib, bp);')
             src.append('          ab_last = ab;')
             src.append('        }')
             src.append('        const int ic = (int)(((float)cd + 0.5f) * rkd), id = cd - ic * kd_;')
@@ -747,7 +747,7 @@ class GroupEmitter:
             src.append('            double F[%d];' % (L + 1))
             src.append('            bool live = !(pre && ib_quartet_negligible(lst, qa, qc, a.prim_tol));')
             src.append('            if (live) {')
-            src.append('              ib_bra_pair(a, g, ia, ib, bp);')
+            src.append('              ib_bra_pair<sizeof(R) == 4>(a, g, ia, ib, bp);')
             src.append('              live = ib_prim_quartet<R, %d>(a, g, bp, ic, id, a.boys_tab, F, pq);' % L)
             src.append('            }')
             src.append('            if (live) {')
