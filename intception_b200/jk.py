@@ -66,6 +66,10 @@ class JKSystem:
         self.world = int(world if world is not None else (torch.distributed.get_world_size(group) if dist_on else 1))
         self.group = group
         self.reduce = bool(reduce) and self.world > 1  # False: return this rank's partial sums
+        # split of the device time between the ERI batches and the digestion
+        # kernels (CUDA events around each; read with kernel_split())
+        self.profile = False
+        self._marks = []
         l = np.asarray(shell_l, np.int32)
         k = np.asarray(shell_k, np.int32)
         e = np.asarray(prim_exp, np.float64)
@@ -202,13 +206,34 @@ class JKSystem:
         ej, ek = self._sum_over_ranks(e).tolist()
         return ej, ek
 
+    def _mark(self):
+        """A CUDA event on the current stream when profiling, else None."""
+        if not self.profile:
+            return None
+        ev = self.torch.cuda.Event(enable_timing=True)
+        ev.record()
+        return ev
+
+    def kernel_split(self):
+        """(ms in ERI batches, ms in digestion kernels) since the last call,
+        summed over the events recorded while self.profile was set."""
+        self.torch.cuda.synchronize()
+        t_eri = sum(a.elapsed_time(b) for a, b, _ in self._marks)
+        t_dig = sum(b.elapsed_time(c) for _, b, c in self._marks)
+        self._marks = []
+        return t_eri, t_dig
+
     def _energy_chunk(self, qt, e):
         """Adds the J/K energies of the unique quartets qt [n,4] to e[0:2]."""
+        m0 = self._mark()
         blocks, off = self._eri(qt, self.lmax)
+        m1 = self._mark()
         eri._check(_lib().intception_b200_jk_energy(
             qt.data_ptr(), off.data_ptr(), qt.shape[0], self.shell_l.data_ptr(), self.fofs.data_ptr(),
             self.P.data_ptr(), self.nbf_cart, blocks.data_ptr(), e.data_ptr(),
             C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)))
+        if m0 is not None:
+            self._marks.append((m0, m1, self._mark()))
 
     def gradient(self, xyz=None):
         """dE/dR [natom,3] of E = E_J + E_K at xyz (FP64)."""
@@ -239,11 +264,15 @@ class JKSystem:
                     continue
                 aux = qt[sel.long()].clone()
                 aux[:, pos] += self.ns if sign > 0 else 2 * self.ns
+                m0 = self._mark()
                 blocks, off = self._eri(aux.contiguous(), self.lmax + 1)
+                m1 = self._mark()
                 eri._check(lib.intception_b200_jk_force(
                     qt.data_ptr(), sel.data_ptr(), off.data_ptr(), sel.numel(), pos, sign,
                     self.shell_l.data_ptr(), self.fofs.data_ptr(), self.shell_atom.data_ptr(),
                     self.P.data_ptr(), self.nbf_cart, self.natom, blocks.data_ptr(), force.data_ptr(), stream))
+                if m0 is not None:
+                    self._marks.append((m0, m1, self._mark()))
 
 
 def _energy_function():
@@ -321,6 +350,13 @@ def main(argv=None):
     (ej, ek), te = timed(lambda: sys_.energy(xyz))
     nquart = sum(int(q.shape[0]) for q in sys_.quartet_chunks())
     g, tg = timed(lambda: sys_.gradient(xyz).cpu().numpy())
+    # the same two passes again with CUDA events around every ERI batch and digestion launch
+    sys_.profile = True
+    sys_.energy(xyz)
+    split_e = sys_.kernel_split()
+    sys_.gradient(xyz)
+    split_g = sys_.kernel_split()
+    sys_.profile = False
     rng = np.random.default_rng(a.seed + 100)
     checks = []
     for _ in range(a.fd_components):
@@ -334,6 +370,10 @@ def main(argv=None):
     out = {'atoms': a.atoms, 'nbf_sph': int(sum(2 * int(l) + 1 for l in sys_.shell_l[:sys_.ns].tolist())),
            'shells': sys_.ns, 'unique_quartets_after_screening': nquart, 'screen': a.screen,
            'E_J': ej, 'E_K': ek, 'energy_s': te, 'gradient_s': tg,
+           'energy_split_ms': {'eri': split_e[0], 'digestion': split_e[1],
+                               'digestion_share': split_e[1] / max(split_e[0] + split_e[1], 1e-9)},
+           'gradient_split_ms': {'eri': split_g[0], 'digestion': split_g[1],
+                                 'digestion_share': split_g[1] / max(split_g[0] + split_g[1], 1e-9)},
            'max_abs_fd_diff': max(c['abs_diff'] for c in checks) if checks else None,
            'translational_residual': float(np.abs(g.sum(axis=0)).max()), 'fd_checks': checks}
     print(json.dumps(out))
