@@ -78,6 +78,66 @@ __device__ __forceinline__ void ib_compact_first(const int* __restrict__ shell_k
   }
 }
 
+// Conditioning of a pair's horizontal recurrence.  The vertical recurrence
+// builds the pair on shell 0 (exponents x0[k0]) and the HRR moves l1 levels to
+// shell 1 (x1[k1], R apart): it combines intermediates of size
+// ~(sig + |PA| + R)^l1 into a result of size ~(sig + |PB|)^l1 (sig = zeta^-1/2,
+// P the product centre, A shell 0's centre, B shell 1's), so rounding errors
+// grow by up to kappa = max over the primitive pairs of
+// ((sig + |PA| + R) / (sig + |PB|))^l1.  Large when shell 0 is diffuse and
+// shell 1 tight and far: P then sits near B, far from A.  Plain loads, so
+// the host (drop-ins) and the device share it.
+__host__ __device__ inline double ib_hrr_kappa(int l1, int k0, int k1, const double* x0, const double* x1, double R) {
+  double kmax = 1.0;
+  for (int i = 0; i < k0; ++i)
+    for (int j = 0; j < k1; ++j) {
+      const double z = x0[i] + x1[j], sig = 1.0 / sqrt(z);
+      const double r = (sig + x1[j] / z * R + R) / (sig + x0[i] / z * R);
+      double k = 1.0;
+      for (int n = 0; n < l1; ++n) k *= r;
+      kmax = k > kmax ? k : kmax;
+    }
+  return kmax;
+}
+
+// A pair built on its higher-l shell (l0 > l1 >= 1) whose HRR kappa exceeds
+// IB_KAPPA_ROUTE, where building on the other shell lowers it by at least
+// IB_KAPPA_GAIN, is evaluated the other way round by the generic kernel (any
+// shell order); the unrolled class kernels only build on the higher-l shell.
+#define IB_KAPPA_ROUTE 1.0e4
+#define IB_KAPPA_GAIN 100.0
+__host__ __device__ inline bool ib_pair_reverse(int l0, int l1, int k0, int k1, const double* x0, const double* x1,
+                                                double R) {
+  if (!(l0 > l1 && l1 >= 1)) return false;
+  const double kc = ib_hrr_kappa(l1, k0, k1, x0, x1, R);
+  if (!(kc > IB_KAPPA_ROUTE)) return false;
+  return ib_hrr_kappa(l0, k1, k0, x1, x0, R) * IB_KAPPA_GAIN < kc;
+}
+
+// The generic kernel's shell order for a canonical quartet (s, l, st permuted
+// alike): pairs that ib_pair_reverse picks are swapped.  Returns whether any was.
+__device__ __forceinline__ bool ib_orient_generic(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                                  const double* __restrict__ prim_exp,
+                                                  const double* __restrict__ shell_xyz, int* s, int* l, int* st) {
+  bool any = false;
+  for (int i = 0; i < 4; i += 2) {
+    if (!(l[i] > l[i + 1] && l[i + 1] >= 1)) continue;
+    double R2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double u = shell_xyz[3 * s[i] + d] - shell_xyz[3 * s[i + 1] + d];
+      R2 += u * u;
+    }
+    if (ib_pair_reverse(l[i], l[i + 1], shell_k[s[i]], shell_k[s[i + 1]], prim_exp + shell_ptr[s[i]],
+                        prim_exp + shell_ptr[s[i + 1]], sqrt(R2))) {
+      int t = s[i]; s[i] = s[i + 1]; s[i + 1] = t;
+      t = l[i]; l[i] = l[i + 1]; l[i + 1] = t;
+      t = st[i]; st[i] = st[i + 1]; st[i + 1] = t;
+      any = true;
+    }
+  }
+  return any;
+}
+
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain
 // path, 5 bits per step (direction 0..2, or 3 for an identity step that pads
 // shorter paths at the front; then the exponent before the step); misc: the

@@ -89,14 +89,17 @@ __device__ __forceinline__ int na_pair(int la, int lb) { return la * (la + 1) / 
 
 // One descriptor per quartet, in the caller's order, with the canonical shell
 // permutation (la >= lb, lc >= ld, bra pair >= ket pair; within a pair of
-// equal l the more compact shell first, as the batch path orders them) and the
+// equal l the more compact shell first, and a pair whose horizontal
+// recurrence is ill-conditioned built on its lower-l shell, as the batch path
+// orders its generic quartets) and the
 // output strides that undo it; the generic range covers all of them.  A
 // quartet with an l outside [0, lmax] sets IB_ERR_ARG and is marked
 // (st[0] = 0): the generic kernel then writes the (ss|ss) value of its shells
 // into the first element of its block, as the batch path does.
 __global__ void ib_noalloc_items_kernel(const int* __restrict__ quartets, const int* __restrict__ shell_l,
                                         const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
-                                        const double* __restrict__ prim_exp, const long long* __restrict__ out_off,
+                                        const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz,
+                                        const long long* __restrict__ out_off,
                                         int nq, int spherical, int lmax, IbItem* __restrict__ items,
                                         int* __restrict__ ranges, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
@@ -130,7 +133,10 @@ __global__ void ib_noalloc_items_kernel(const int* __restrict__ quartets, const 
         t = st[k]; st[k] = st[k + 2]; st[k + 2] = t;
       }
     }
-    if (!bad) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);
+    if (!bad) {
+      ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);
+      ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);  // as the batch path's generic quartets
+    }
     IbItem it;
     for (int i = 0; i < 4; ++i) {
       it.s[i] = s[i];
@@ -148,10 +154,10 @@ __global__ void ib_noalloc_items_kernel(const int* __restrict__ quartets, const 
 
 long long noalloc_slice(int lmax) {
   long long best = 0;
-  for (int a = 0; a <= lmax; ++a)
-    for (int b = 0; b <= a; ++b)
+  for (int a = 0; a <= lmax; ++a)  // every shell order (ib_orient_generic may build a pair on either shell)
+    for (int b = 0; b <= lmax; ++b)
       for (int c = 0; c <= lmax; ++c)
-        for (int d = 0; d <= c; ++d) best = std::max(best, ib_generic_dims(a, b, c, d).total);
+        for (int d = 0; d <= lmax; ++d) best = std::max(best, ib_generic_dims(a, b, c, d).total);
   return (best + 31) / 32 * 32;
 }
 
@@ -184,7 +190,8 @@ extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* ba
     return ib_runtime_set_status(IB_ERR_CUDA, "eri_batch_noalloc: clearing the status word failed");
   const int tb = 256, nb = std::min((nq + tb - 1) / tb, 4 * d->nsm);
   ib_noalloc_items_kernel<<<nb, tb, 0, s>>>(quartets, basis->shell_l, basis->shell_k, basis->shell_ptr,
-                                            basis->prim_exp, out_off, nq, spherical ? 1 : 0, basis->lmax, d->items,
+                                            basis->prim_exp, basis->shell_xyz, out_off, nq, spherical ? 1 : 0,
+                                            basis->lmax, d->items,
                                             d->ranges, d->status);
   IbLaunch a;
   memset(&a, 0, sizeof(a));

@@ -163,9 +163,11 @@ __device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
 }
 
 __global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
-                            const int* __restrict__ shell_k, int nq, int lmax, const double* __restrict__ bounds,
-                            double skip_below, double thr, int mixed, const int* __restrict__ kind,
-                            unsigned* __restrict__ keys, int* __restrict__ vals, int* status) {
+                            const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                            const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz, int nq,
+                            int lmax, const double* __restrict__ bounds, double skip_below, double thr, int mixed,
+                            const int* __restrict__ kind, unsigned* __restrict__ keys, int* __restrict__ vals,
+                            int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], st[4] = {0, 0, 0, 0};
     bool bad = false;
@@ -185,8 +187,13 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int work = min(15, 31 - __clz(max(nprim, 1)));  // floor(log2) of the primitive quartet count
     const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
     const int k = kind[cid];
-    const int gen = (!skip && k == 0) ? 1 : 0;
-    const int fp32 = (!skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
+    // a class kernel builds every pair on its higher-l shell; a pair whose
+    // horizontal recurrence would lose too many digits that way goes to the
+    // generic kernel, which builds it on the other shell (ib_orient_generic)
+    int st2[4] = {0, 0, 0, 0}, s2[4] = {s[0], s[1], s[2], s[3]}, l2[4] = {l[0], l[1], l[2], l[3]};
+    const bool route = !skip && !bad && k != 0 && ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s2, l2, st2);
+    const int gen = (!skip && (k == 0 || route)) ? 1 : 0;
+    const int fp32 = (!gen && !skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
     // primitive quartet counts (powers of two) descending inside a class: the
     // longest quartets start first
     keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | (unsigned(cid) << 4) |
@@ -198,7 +205,8 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
 __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __restrict__ order, int nq,
                                const int* __restrict__ quartets, const int* __restrict__ shell_l,
                                const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
-                               const double* __restrict__ prim_exp, const long long* __restrict__ out_off,
+                               const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz,
+                               const long long* __restrict__ out_off,
                                int spherical, IbItem* __restrict__ items, int* __restrict__ ranges) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
     const int q = order[p];
@@ -213,6 +221,7 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     const unsigned key = keys[p];
     const int slot = (int)(key >> 4);  // skip*2048 + generic*1024 + fp32*512 + cid
     if (!(slot >> 11)) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);  // evaluated quartets only
+    if (((slot >> 10) & 3) == 1) ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
     IbItem it;
     for (int i = 0; i < 4; ++i) {
       it.s[i] = s[i];
@@ -484,10 +493,10 @@ IbLaunch base_launch(Context* c) {
 // Scratch doubles per block of the generic kernel, for shells up to lmax.
 long long generic_slice(int lmax) {
   long long best = 0;
-  for (int a = 0; a <= lmax; ++a)
-    for (int b = 0; b <= a; ++b)
+  for (int a = 0; a <= lmax; ++a)  // every shell order: the generic kernel may build a pair on either shell
+    for (int b = 0; b <= lmax; ++b)
       for (int cc = 0; cc <= lmax; ++cc)
-        for (int d = 0; d <= cc; ++d) {
+        for (int d = 0; d <= lmax; ++d) {
           IbGenericDims g = ib_generic_dims(a, b, cc, d);
           best = std::max(best, g.total);
         }
@@ -550,7 +559,10 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       }
     }
   }
-  if (lmax > ib_lmax_emitted && fp64_present) {
+  // the generic kernel serves the classes without an unrolled kernel and, for
+  // lmax >= 2, the quartets classify routes to it (ib_orient_generic); an
+  // empty range returns at once
+  if ((lmax > ib_lmax_emitted || lmax >= 2) && fp64_present) {
     const long long slice = generic_slice(lmax);
     long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
     nblk = std::max<long long>(nblk, 1);
@@ -674,6 +686,20 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     if (lperm[i] == lperm[i + 1] && min_exp(sperm[i]) < min_exp(sperm[i + 1])) swp(i, i + 1);
   const int pb = pair_index_h(lperm[0], lperm[1]), pk = pair_index_h(lperm[2], lperm[3]);
   const int cid = pb * (pb + 1) / 2 + pk;
+  // pairs whose horizontal recurrence is ill-conditioned when built on the
+  // higher-l shell are built on the other one, by the generic kernel (as the
+  // batch entries route them)
+  bool route = false;
+  for (int i = 0; i < 4; i += 2) {
+    const DropShell& s0 = sh[sperm[i]];
+    const DropShell& s1 = sh[sperm[i + 1]];
+    double R2 = 0.0;
+    for (int d = 0; d < 3; ++d) R2 += (s0.cen[d] - s1.cen[d]) * (s0.cen[d] - s1.cen[d]);
+    if (ib_pair_reverse(lperm[i], lperm[i + 1], s0.nprim, s1.nprim, s0.x, s1.x, std::sqrt(R2))) {
+      swp(i, i + 1);
+      route = true;
+    }
+  }
   int b = 0;
   for (int ka = 0; ka < sh[0].ncont; ++ka)
     for (int kb = 0; kb < sh[1].ncont; ++kb)
@@ -689,7 +715,7 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
           hit[b] = it;
         }
   std::memset(hrg, 0, kNRanges * sizeof(int));
-  const bool emitted = c->table[cid].launch != nullptr;
+  const bool emitted = c->table[cid].launch != nullptr && !route;
   if (emitted) {
     hrg[2 * cid] = 0;
     hrg[2 * cid + 1] = nblk;
@@ -898,7 +924,8 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
   const int grid = std::min((nq + 255) / 256, c->nsm * 16);
   const bool use_bounds = bounds != nullptr && (precision == IB_PREC_MIXED || skip_below > 0.0);
-  ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, nq, basis->lmax,
+  ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, basis->shell_ptr, basis->prim_exp,
+                                   basis->shell_xyz, nq, basis->lmax,
                                    use_bounds ? bounds : nullptr, skip_below, fp32_below,
                                    precision == IB_PREC_MIXED ? 1 : 0, c->kind.as<int>(), c->keys.as<unsigned>(),
                                    c->vals.as<int>(), c->status.as<int>());
@@ -907,7 +934,7 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   IB_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp_bytes, c->keys.as<unsigned>(), c->keys2.as<unsigned>(),
                                           c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
   ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
-                                      basis->shell_k, basis->shell_ptr, basis->prim_exp, out_off,
+                                      basis->shell_k, basis->shell_ptr, basis->prim_exp, basis->shell_xyz, out_off,
                                       spherical ? 1 : 0, c->items.as<IbItem>(), c->ranges.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());

