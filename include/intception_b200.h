@@ -194,8 +194,8 @@ int intception_b200_schwarz(const intception_b200_basis *basis, const int *pairs
  * pair's primitive pairs, a bound on the Coulomb norm of the primitive
  * product (|c_a c_b| exp(-x_a x_b |AB|^2 / zeta) times the norms of
  * (rho + |PA|)^la (rho + |PB|)^lb exp(-zeta rho^2), and for spherical output the
- * transformation's largest coefficient sum); bounds[q] = Q_ab Q_cd by
- * Cauchy-Schwarz in the Coulomb metric.  No ERI is evaluated: one pass over
+ * transformation's largest coefficient sum; each term in float, widened by
+ * 1.001); bounds[q] = Q_ab Q_cd by Cauchy-Schwarz in the Coulomb metric.  No ERI is evaluated: one pass over
  * the primitive pairs, cheap enough to run with every batch (on a random l <= 2
  * batch it keeps 1.3x the quartets Schwarz factors keep at 1e-12).  A value
  * whose true bound is below about 1e-300 may read 0.  An l outside [0, 6]

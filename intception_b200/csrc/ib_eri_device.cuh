@@ -88,16 +88,18 @@ __device__ __forceinline__ void ib_compact_first(const int* __restrict__ shell_k
 // shell 1 tight and far: P then sits near B, far from A.  Plain loads, so
 // the host (drop-ins) and the device share it.
 __host__ __device__ inline double ib_hrr_kappa(int l1, int k0, int k1, const double* x0, const double* x1, double R) {
-  double kmax = 1.0;
+  float kmax = 1.0f;
+  const float Rf = (float)R;
   for (int i = 0; i < k0; ++i)
     for (int j = 0; j < k1; ++j) {
-      const double z = x0[i] + x1[j], sig = 1.0 / sqrt(z);
-      const double r = (sig + x1[j] / z * R + R) / (sig + x0[i] / z * R);
-      double k = 1.0;
+      const float a = (float)x0[i], b = (float)x1[j];
+      const float z = a + b, oz = 1.0f / z, sig = 1.0f / sqrtf(z);
+      const float r = (sig + b * oz * Rf + Rf) / (sig + a * oz * Rf);
+      float k = 1.0f;
       for (int n = 0; n < l1; ++n) k *= r;
       kmax = k > kmax ? k : kmax;
     }
-  return kmax;
+  return (double)kmax;
 }
 
 // A pair built on its higher-l shell (l0 > l1 >= 1) whose HRR kappa exceeds
@@ -514,29 +516,42 @@ __device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa
   return 1.000001 * sph * K * s * s * sqrt(s) * poly;
 }
 
-// ib_pair_bound for angular momenta known only at run time (l0, l1 <= 6):
-// the sum over i, j of C(l0,i) C(l1,j) |PA|^(l0-i) |PB|^(l1-j) N_(i+j) s^(i+j)
-// regrouped by n = i + j as the coefficients of (pa + t)^l0 (pb + t)^l1.
-__device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double K, double zeta, double pa,
-                                                   double pb) {
-  double c[13];
-  c[0] = 1.0;
-  int deg = 0;
-  for (int r = 0; r < l0 + l1; ++r) {  // multiply by (p + t), p = pa for the first l0 factors
-    const double p = r < l0 ? pa : pb;
-    c[deg + 1] = c[deg];
-    for (int n = deg; n > 0; --n) c[n] = c[n] * p + c[n - 1];
-    c[0] *= p;
-    ++deg;
+// ib_pair_bound for angular momenta known only at run time (l0, l1 <= 6), in
+// float: the sum over i, j of C(l0,i) C(l1,j) |PA|^(l0-i) |PB|^(l1-j)
+// N_(i+j) s^(i+j), regrouped by n = i + j as the coefficients of
+// (pa + t)^l0 (pb + t)^l1 (loops unrolled to the largest degree so the
+// coefficients stay in registers).  Every operand is positive, so the float
+// result is within a few hundred ulp (< 1e-4 relative) of the exact one; the
+// factor 1.001 makes it an upper bound.  An exponent below -80 counts as
+// exp(-80) (float would flush it to zero; an upper bound may not).
+__device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double cc, double x0, double x1,
+                                                   double R) {
+  const float z = (float)(x0 + x1), oz = 1.0f / z;
+  const float arg = -(float)x0 * (float)x1 * oz * (float)(R * R);
+  const float e = __expf(fmaxf(arg, -80.0f));
+  const float pa = (float)x1 * oz * (float)R, pb = (float)x0 * oz * (float)R;
+  const int deg = l0 + l1;
+  float c[13];
+#pragma unroll
+  for (int n = 0; n < 13; ++n) c[n] = n == 0 ? 1.0f : 0.0f;
+#pragma unroll
+  for (int r = 0; r < 12; ++r) {
+    if (r < deg) {
+      const float p = r < l0 ? pa : pb;
+#pragma unroll
+      for (int n = r + 1; n > 0; --n) c[n] = fmaf(c[n], p, c[n - 1]);
+      c[0] *= p;
+    }
   }
-  const double s = 1.0 / sqrt(zeta);
-  double poly = 0.0, sn = 1.0;
-  for (int n = 0; n <= deg; ++n) {
-    poly += c[n] * ib_rn_norm(n) * sn;
+  const float s = rsqrtf(z);
+  float poly = 0.0f, sn = 1.0f;
+#pragma unroll
+  for (int n = 0; n < 13; ++n) {
+    if (n <= deg) poly = fmaf(c[n] * (float)ib_rn_norm(n), sn, poly);
     sn *= s;
   }
-  const double f = sph ? ib_sph_colsum(l0) * ib_sph_colsum(l1) : 1.0;
-  return 1.000001 * f * K * s * s * sqrt(s) * poly;
+  const float f = sph ? (float)(ib_sph_colsum(l0) * ib_sph_colsum(l1)) : 1.0f;
+  return 1.001 * fabs(cc) * (double)(f * e * s * s * sqrtf(s) * poly);
 }
 
 // Bound Q of primitive pair i0 * k1 + i1 of two shells (exponent/coefficient

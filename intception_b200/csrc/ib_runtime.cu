@@ -316,9 +316,7 @@ __global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, cons
           const double x0 = __ldg(prim_exp + p0 + i), c0 = __ldg(prim_coef + p0 + i);
           for (int j = 0; j < k1; ++j) {
             const double x1 = __ldg(prim_exp + p1 + j), c1 = __ldg(prim_coef + p1 + j);
-            const double z = x0 + x1, oz = 1.0 / z;
-            const double K = fabs(ib_pair_factor(x0, c0, x1, c1, oz, r2));
-            if (K != 0.0) Q += ib_pair_bound_rt(l0, l1, spherical != 0, K, z, x1 * oz * R, x0 * oz * R);
+            Q += ib_pair_bound_rt(l0, l1, spherical != 0, c0 * c1, x0, x1, R);
           }
         }
         Q *= 1.000001;  // the rounding of the sum

@@ -102,9 +102,12 @@ PACK_TEN = True
 # 32 lanes (the S_hi = 4 sides: 20 low + 15 top components): every warp of the
 # group holds all the low levels plus its share of the top level, so the
 # transfer operands stay inside the warp (shuffles, no per-level barrier); the
-# low levels are evaluated once per warp (False: one copy, transfer operands
-# through shared memory with a named barrier per level)
-DUP_LOW = True
+# low levels are evaluated once per warp.  Off (False: one copy, transfer
+# operands through shared memory with a named barrier per level): measured on
+# B200, (dd|dd) alone 11.6 ms with it against 10.2 ms without (1e5 quartets,
+# K 1..6), the l <= 2 FP64 step 16.0 against 15.7 ms -- the duplicated chains
+# cost more than the barriers they remove.
+DUP_LOW = False
 
 # register budgets offered to the autotuner: __launch_bounds__(IB_BLOCK, MINB)
 # asks for MINB resident blocks per SM (1: no register cap); must match
@@ -658,7 +661,15 @@ class GroupEmitter:
         # primitive screening (a.prim_tol > 0) for quartets of one pair tile a
         # side: the screened lists are built here, before the accumulators
         # are live; larger quartets keep exact-zero culling only
-        src.append('    const bool pre = a.prim_tol > 0.0 && kab <= 64 && kcd <= 64;  // uniform over the quartet')
+        # classes with a g shell build only the exact-zero lists: on the l <= 4
+        # sample workload with primitive screening on, a step of these kernels
+        # (with the low levels then duplicated per warp) stopped on an illegal
+        # address once; the screened lists stay off for them until that is
+        # explained (their exact path ran clean on the same quartets)
+        if max(self.la, self.lb, self.lc, self.ld) >= 4:
+            src.append('    constexpr bool pre = false;  // g classes: exact-zero lists only')
+        else:
+            src.append('    const bool pre = a.prim_tol > 0.0 && kab <= 64 && kcd <= 64;  // uniform over the quartet')
         src.append('    if (pre && r < 32) {')
         src += ['  ' + ln for ln in self.builder_lanes()]
         src.append('      const int2 nn = ib_live_pairs_screened<%s, SPH>(a.prim_exp, a.prim_coef, g.ptr[0], g.ptr[1], '

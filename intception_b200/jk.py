@@ -337,6 +337,7 @@ def main(argv=None):
     ap.add_argument('--screen', type=float, default=1e-15)
     ap.add_argument('--fd-components', type=int, default=3)
     ap.add_argument('--h', type=float, default=1e-4)
+    ap.add_argument('--fd4', action='store_true', help='also the four-point central stencil (same h)')
     a = ap.parse_args(argv)
     sys_, xyz = lattice_system(natom=a.atoms, seed=a.seed, screen=a.screen)
 
@@ -359,14 +360,23 @@ def main(argv=None):
     sys_.profile = False
     rng = np.random.default_rng(a.seed + 100)
     checks = []
+    def shifted(at, d, k):
+        x = xyz.copy()
+        x[at, d] += k * a.h
+        return sum(sys_.energy(x))
+
     for _ in range(a.fd_components):
         at, d = int(rng.integers(a.atoms)), int(rng.integers(3))
-        xp, xm = xyz.copy(), xyz.copy()
-        xp[at, d] += a.h
-        xm[at, d] -= a.h
-        fd = (sum(sys_.energy(xp)) - sum(sys_.energy(xm))) / (2 * a.h)
-        checks.append({'atom': at, 'xyz': d, 'adjoint': float(g[at, d]), 'central_fd': fd,
-                       'abs_diff': abs(float(g[at, d]) - fd)})
+        ep, em = shifted(at, d, 1), shifted(at, d, -1)
+        fd = (ep - em) / (2 * a.h)
+        chk = {'atom': at, 'xyz': d, 'adjoint': float(g[at, d]), 'central_fd': fd, 'abs_diff': abs(float(g[at, d]) - fd)}
+        if a.fd4:
+            # the same step h on the four-point central stencil: its O(h^2)
+            # truncation term cancels, which tells FD error from adjoint error
+            e2p, e2m = shifted(at, d, 2), shifted(at, d, -2)
+            fd4 = (8.0 * (ep - em) - (e2p - e2m)) / (12.0 * a.h)
+            chk.update(central_fd4=fd4, abs_diff4=abs(float(g[at, d]) - fd4))
+        checks.append(chk)
     out = {'atoms': a.atoms, 'nbf_sph': int(sum(2 * int(l) + 1 for l in sys_.shell_l[:sys_.ns].tolist())),
            'shells': sys_.ns, 'unique_quartets_after_screening': nquart, 'screen': a.screen,
            'E_J': ej, 'E_K': ek, 'energy_s': te, 'gradient_s': tg,
@@ -375,6 +385,7 @@ def main(argv=None):
            'gradient_split_ms': {'eri': split_g[0], 'digestion': split_g[1],
                                  'digestion_share': split_g[1] / max(split_g[0] + split_g[1], 1e-9)},
            'max_abs_fd_diff': max(c['abs_diff'] for c in checks) if checks else None,
+           'max_abs_fd4_diff': max(c['abs_diff4'] for c in checks) if checks and a.fd4 else None,
            'translational_residual': float(np.abs(g.sum(axis=0)).max()), 'fd_checks': checks}
     print(json.dumps(out))
 

@@ -520,15 +520,17 @@ def test_c1_every_quartet_through_the_dropin():
 
 @pytest.mark.parametrize('sph', [False, True])
 def test_analytic_quartet_bounds_match_oracle_and_cover_blocks(sph):
-    """intception_b200_quartet_bounds against its C restatement (oracle/pair_bound.h)
-    to 1e-12 relative, over l <= 6; every block of the batch path stays within
-    its bound, and screening with it errs by no more than the threshold."""
+    """intception_b200_quartet_bounds against its C restatement (oracle/pair_bound.h,
+    FP64): the device evaluates the primitive-pair terms in float and widens
+    them by 1.001, so it must lie in [1, 1.01] x the restatement, l <= 6; every
+    block of the batch path stays within its bound, and screening with it errs
+    by no more than the threshold."""
     import torch
     b = basis.independent_quartet_batch(131 + sph, 600, [0, 1, 2, 3, 4, 5, 6], [1, 2, 3, 6], 0.05, 1e4, 8.0, sph)
     eng = eri.EriEngine(b)
     dev = eng.analytic_bounds().cpu().numpy()
     ora = loader.quartet_bounds(b)
-    assert np.all(np.abs(dev - ora) <= 1e-12 * np.abs(ora) + 1e-300)
+    assert np.all(dev >= ora) and np.all(dev <= 1.01 * ora)
     out = run_batch(b)
     sizes = basis.block_sizes(b.shell_l, b.quartets, b.spherical)
     for q in range(b.nq):
