@@ -104,15 +104,37 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
 // or l-1 (sign < 0).  aux_off[k] locates the auxiliary block of quartet
 // qidx[k] of the unique quartet list.  Forces accumulate in shared memory per
 // atom and are flushed once per block.
+//
+// One warp per quartet.  When every shell has l <= JK_STAGE_L, the six density
+// blocks the quartet's weights read (P over the shell pairs ab, cd, ac, bd, ad,
+// bc) are first copied to the warp's slice of shared memory with coalesced
+// row loads, and every weight then reads shared memory: an element of the
+// auxiliary block needs up to 3 weights of 6 density values each, which as
+// global gathers dominated the kernel.
+#define JK_STAGE_L 3
+#define JK_STAGE_N 10  // ncart(JK_STAGE_L)
+#define JK_WARPS 8
+
+__device__ __forceinline__ void jk_stage(const double* __restrict__ P, int nbf, int r0, int nr, int c0, int nc,
+                                         double* __restrict__ dst, int lane) {
+  for (int e = lane; e < nr * nc; e += 32) {
+    const int i = e / nc, j = e - i * nc;
+    dst[i * JK_STAGE_N + j] = __ldg(P + (size_t)(r0 + i) * nbf + c0 + j);
+  }
+}
+
 __global__ void ib_jk_force_kernel(const int* __restrict__ quartets, const int* __restrict__ qidx,
                                    const long long* __restrict__ aux_off, int naux, int pos, int sign,
                                    const int* __restrict__ shell_l, const int* __restrict__ fofs,
                                    const int* __restrict__ shell_atom, const double* __restrict__ P, int nbf,
                                    int natom, const double* __restrict__ blocks, double* __restrict__ force) {
   extern __shared__ double fs[];
+  // [3 natom] force sums, then per warp 6 staged density blocks of JK_STAGE_N^2
+  double* stage = fs + ((3 * natom + 1) & ~1);
   for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x) fs[i] = 0.0;
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* __restrict__ st = stage + (size_t)wib * 6 * JK_STAGE_N * JK_STAGE_N;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
   for (int k = warp; k < naux; k += nwarp) {
     const int q = qidx[k];
@@ -129,6 +151,19 @@ __global__ void ib_jk_force_kernel(const int* __restrict__ quartets, const int* 
     const double deg = jk_deg(s);
     const double* blk = blocks + aux_off[k];
     const int tot = na[0] * na[1] * na[2] * na[3];
+    // staged blocks: 0 ab, 1 cd, 2 ac, 3 bd, 4 ad, 5 bc (rows of the first shell)
+    const bool staged = max(max(l[0], l[1]), max(l[2], l[3])) <= JK_STAGE_L;
+    const int SS = JK_STAGE_N * JK_STAGE_N;
+    if (staged) {
+      __syncwarp();
+      jk_stage(P, nbf, f[0], n[0], f[1], n[1], st + 0 * SS, lane);
+      jk_stage(P, nbf, f[2], n[2], f[3], n[3], st + 1 * SS, lane);
+      jk_stage(P, nbf, f[0], n[0], f[2], n[2], st + 2 * SS, lane);
+      jk_stage(P, nbf, f[1], n[1], f[3], n[3], st + 3 * SS, lane);
+      jk_stage(P, nbf, f[0], n[0], f[3], n[3], st + 4 * SS, lane);
+      jk_stage(P, nbf, f[1], n[1], f[2], n[2], st + 5 * SS, lane);
+      __syncwarp();
+    }
     double g[3] = {0.0, 0.0, 0.0};
     for (int e = lane; e < tot; e += 32) {
       int idx[4];
@@ -152,9 +187,18 @@ __global__ void ib_jk_force_kernel(const int* __restrict__ quartets, const int* 
           o[d] += 1;
           coef = -(double)o[d];
         }
-        int fi[4] = {f[0] + idx[0], f[1] + idx[1], f[2] + idx[2], f[3] + idx[3]};
-        fi[pos] = f[pos] + jk_index(o[0], o[1], o[2]);
-        g[d] += coef * v * jk_weight(P, nbf, fi[0], fi[1], fi[2], fi[3]);
+        int li[4] = {idx[0], idx[1], idx[2], idx[3]};  // component indices within each shell
+        li[pos] = jk_index(o[0], o[1], o[2]);
+        double w;
+        if (staged) {
+          const int N = JK_STAGE_N;
+          w = 0.5 * st[0 * SS + li[0] * N + li[1]] * st[1 * SS + li[2] * N + li[3]] -
+              0.125 * (st[2 * SS + li[0] * N + li[2]] * st[3 * SS + li[1] * N + li[3]] +
+                       st[4 * SS + li[0] * N + li[3]] * st[5 * SS + li[1] * N + li[2]]);
+        } else {
+          w = jk_weight(P, nbf, f[0] + li[0], f[1] + li[1], f[2] + li[2], f[3] + li[3]);
+        }
+        g[d] += coef * v * w;
       }
     }
     for (int d = 0; d < 3; ++d) g[d] = warp_sum(g[d]);
@@ -201,11 +245,12 @@ extern "C" int intception_b200_jk_force(const int* quartets, const int* qidx, co
   int dev = 0, nsm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return IB_ERR_NODEVICE;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = sizeof(double) * 3 * (size_t)natom;
+  const size_t smem =
+      sizeof(double) * (((3 * (size_t)natom + 1) & ~(size_t)1) + (size_t)JK_WARPS * 6 * JK_STAGE_N * JK_STAGE_N);
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(ib_jk_force_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return IB_ERR_CUDA;
-  const int threads = 256, wpb = threads / 32;
+  const int threads = 32 * JK_WARPS, wpb = JK_WARPS;
   int blocks_n = (naux + wpb - 1) / wpb;
   if (blocks_n > nsm * 8) blocks_n = nsm * 8;
   ib_jk_force_kernel<<<blocks_n, threads, smem, static_cast<cudaStream_t>(stream)>>>(
