@@ -522,13 +522,13 @@ __device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa
 // (pa + t)^l0 (pb + t)^l1 (loops unrolled to the largest degree so the
 // coefficients stay in registers).  Every operand is positive, so the float
 // result is within a few hundred ulp (< 1e-4 relative) of the exact one; the
-// factor 1.001 makes it an upper bound.  An exponent below -80 counts as
-// exp(-80) (float would flush it to zero; an upper bound may not).
+// factor 1.001 makes it an upper bound.  The Gaussian factor exp(-x0 x1 R^2 /
+// zeta) stays in FP64 below exp(-80), where float would flush it to zero.
 __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double cc, double x0, double x1,
                                                    double R) {
   const float z = (float)(x0 + x1), oz = 1.0f / z;
-  const float arg = -(float)x0 * (float)x1 * oz * (float)(R * R);
-  const float e = __expf(fmaxf(arg, -80.0f));
+  const double argd = -x0 * x1 / (x0 + x1) * (R * R);
+  const double e = argd > -80.0 ? (double)__expf((float)argd) : exp(argd);
   const float pa = (float)x1 * oz * (float)R, pb = (float)x0 * oz * (float)R;
   const int deg = l0 + l1;
   float c[13];
@@ -551,7 +551,7 @@ __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, dou
     sn *= s;
   }
   const float f = sph ? (float)(ib_sph_colsum(l0) * ib_sph_colsum(l1)) : 1.0f;
-  return 1.001 * fabs(cc) * (double)(f * e * s * s * sqrtf(s) * poly);
+  return 1.001 * fabs(cc) * e * (double)(f * s * s * sqrtf(s) * poly);
 }
 
 // Bound Q of primitive pair i0 * k1 + i1 of two shells (exponent/coefficient

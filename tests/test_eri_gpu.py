@@ -530,7 +530,8 @@ def test_analytic_quartet_bounds_match_oracle_and_cover_blocks(sph):
     eng = eri.EriEngine(b)
     dev = eng.analytic_bounds().cpu().numpy()
     ora = loader.quartet_bounds(b)
-    assert np.all(dev >= ora) and np.all(dev <= 1.01 * ora)
+    assert np.all(dev >= ora)
+    assert np.all(dev <= 1.01 * ora)
     out = run_batch(b)
     sizes = basis.block_sizes(b.shell_l, b.quartets, b.spherical)
     for q in range(b.nq):
