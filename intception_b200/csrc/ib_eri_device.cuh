@@ -21,7 +21,10 @@
 
 #define IB_LMAX 6
 #define IB_NPAIR ((IB_LMAX + 1) * (IB_LMAX + 2) / 2)
-#define IB_NCLASS (IB_NPAIR * (IB_NPAIR + 1) / 2)
+// pair ids: la >= lb canonical (0 .. IB_NPAIR-1), and the reversed pair (2,3)
+// -- the d shell built on, the f shell reached by the HRR -- as IB_NPAIR
+#define IB_NPAIR_EXT (IB_NPAIR + 1)
+#define IB_NCLASS (IB_NPAIR_EXT * (IB_NPAIR_EXT + 1) / 2)
 #define IB_BOYS_TAYLOR 7
 
 struct IbItem {
@@ -138,6 +141,53 @@ __device__ __forceinline__ bool ib_orient_generic(const int* __restrict__ shell_
     }
   }
   return any;
+}
+
+// Pair id of an ordered pair: la >= lb canonical; (2,3) the reversed pair.
+__host__ __device__ inline int ib_pair_ext(int la, int lb) {
+  return la >= lb ? la * (la + 1) / 2 + lb : IB_NPAIR;
+}
+
+// Reversal for the class kernels of a canonical quartet (s, l, st permuted
+// alike).  0: no pair needs it (ib_pair_reverse); 1: every pair that does is an
+// (f d) pair and all four l <= 3, so the quartet is reordered here for the
+// (d f| class kernels (the pair reversed, then the pair with the larger
+// ib_pair_ext id first); 2: the generic kernel is needed (left unchanged).
+__device__ __forceinline__ int ib_reverse_for_classes(const int* __restrict__ shell_k,
+                                                      const int* __restrict__ shell_ptr,
+                                                      const double* __restrict__ prim_exp,
+                                                      const double* __restrict__ shell_xyz, int* s, int* l, int* st) {
+  bool rev[2] = {false, false};
+  for (int i = 0; i < 4; i += 2) {
+    if (!(l[i] > l[i + 1] && l[i + 1] >= 1)) continue;
+    double R2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double u = shell_xyz[3 * s[i] + d] - shell_xyz[3 * s[i + 1] + d];
+      R2 += u * u;
+    }
+    rev[i / 2] = ib_pair_reverse(l[i], l[i + 1], shell_k[s[i]], shell_k[s[i + 1]], prim_exp + shell_ptr[s[i]],
+                                 prim_exp + shell_ptr[s[i + 1]], sqrt(R2));
+  }
+  if (!rev[0] && !rev[1]) return 0;
+  const int lm = max(max(l[0], l[1]), max(l[2], l[3]));
+  for (int h = 0; h < 2; ++h)
+    if (rev[h] && !(l[2 * h] == 3 && l[2 * h + 1] == 2)) return 2;
+  if (lm > 3) return 2;
+  for (int h = 0; h < 2; ++h) {
+    if (!rev[h]) continue;
+    const int i = 2 * h;
+    int t = s[i]; s[i] = s[i + 1]; s[i + 1] = t;
+    t = l[i]; l[i] = l[i + 1]; l[i + 1] = t;
+    t = st[i]; st[i] = st[i + 1]; st[i + 1] = t;
+  }
+  if (ib_pair_ext(l[0], l[1]) < ib_pair_ext(l[2], l[3])) {
+    for (int k = 0; k < 2; ++k) {
+      int t = s[k]; s[k] = s[k + 2]; s[k + 2] = t;
+      t = l[k]; l[k] = l[k + 2]; l[k + 2] = t;
+      t = st[k]; st[k] = st[k + 2]; st[k + 2] = t;
+    }
+  }
+  return 1;
 }
 
 // Per-lane constants of a lane-group kernel.  steps: the lane's base-chain

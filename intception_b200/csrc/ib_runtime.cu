@@ -181,18 +181,18 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
       for (int i = 0; i < 4; ++i) l[i] = 0;
     }
     ib_canon(s, l, st);
-    const int pb = ib_pair_d(l[0], l[1]), pk = ib_pair_d(l[2], l[3]);
+    const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
+    // a class kernel builds every pair on its higher-l shell; a pair whose
+    // horizontal recurrence would lose too many digits that way is built on
+    // the other shell: by the (d f| class kernels for an (f d) pair of an
+    // l <= 3 quartet, else by the generic kernel (ib_reverse_for_classes)
+    const int rv = (!skip && !bad) ? ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st) : 0;
+    const int pb = ib_pair_ext(l[0], l[1]), pk = ib_pair_ext(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
     const int nprim = shell_k[s[0]] * shell_k[s[1]] * shell_k[s[2]] * shell_k[s[3]];
     const int work = min(15, 31 - __clz(max(nprim, 1)));  // floor(log2) of the primitive quartet count
-    const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
     const int k = kind[cid];
-    // a class kernel builds every pair on its higher-l shell; a pair whose
-    // horizontal recurrence would lose too many digits that way goes to the
-    // generic kernel, which builds it on the other shell (ib_orient_generic)
-    int st2[4] = {0, 0, 0, 0}, s2[4] = {s[0], s[1], s[2], s[3]}, l2[4] = {l[0], l[1], l[2], l[3]};
-    const bool route = !skip && !bad && k != 0 && ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s2, l2, st2);
-    const int gen = (!skip && (k == 0 || route)) ? 1 : 0;
+    const int gen = (!skip && (k == 0 || rv == 2)) ? 1 : 0;
     const int fp32 = (!gen && !skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
     // primitive quartet counts (powers of two) descending inside a class: the
     // longest quartets start first
@@ -220,6 +220,9 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     ib_canon(s, l, st);
     const unsigned key = keys[p];
     const int slot = (int)(key >> 4);  // skip*2048 + generic*1024 + fp32*512 + cid
+    // the (d f| classes: the reordering classify chose (the same decision)
+    if (((slot >> 10) & 3) == 0 && (slot & 511) >= IB_NPAIR * (IB_NPAIR + 1) / 2)
+      ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
     if (!(slot >> 11)) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);  // evaluated quartets only
     if (((slot >> 10) & 3) == 1) ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
     IbItem it;
@@ -501,16 +504,18 @@ long long generic_slice(int lmax) {
   return (best + 31) / 32 * 32;
 }
 
-// Largest l of canonical class cid (pair index pb = la(la+1)/2 + lb, pb >= pk).
+// Largest l of class cid (pair ids pb >= pk, ib_pair_ext; IB_NPAIR is (2,3)).
 int class_lmax(int cid) {
   int pb = 0;
   while ((pb + 1) * (pb + 2) / 2 <= cid) ++pb;
-  int la = 0;
-  while ((la + 1) * (la + 2) / 2 <= pb) ++la;
   const int pk = cid - pb * (pb + 1) / 2;
-  int lc = 0;
-  while ((lc + 1) * (lc + 2) / 2 <= pk) ++lc;
-  return std::max(la, lc);
+  auto pair_lmax = [](int p) {
+    if (p == IB_NPAIR) return 3;
+    int la = 0;
+    while ((la + 1) * (la + 2) / 2 <= p) ++la;
+    return la;
+  };
+  return std::max(pair_lmax(pb), pair_lmax(pk));
 }
 
 // Launch the emitted kernels for the given variants and the generic kernel;
@@ -687,17 +692,31 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
   // pairs whose horizontal recurrence is ill-conditioned when built on the
   // higher-l shell are built on the other one, by the generic kernel (as the
   // batch entries route them)
-  bool route = false;
+  bool rev[2] = {false, false};
   for (int i = 0; i < 4; i += 2) {
     const DropShell& s0 = sh[sperm[i]];
     const DropShell& s1 = sh[sperm[i + 1]];
     double R2 = 0.0;
     for (int d = 0; d < 3; ++d) R2 += (s0.cen[d] - s1.cen[d]) * (s0.cen[d] - s1.cen[d]);
-    if (ib_pair_reverse(lperm[i], lperm[i + 1], s0.nprim, s1.nprim, s0.x, s1.x, std::sqrt(R2))) {
-      swp(i, i + 1);
-      route = true;
-    }
+    rev[i / 2] = ib_pair_reverse(lperm[i], lperm[i + 1], s0.nprim, s1.nprim, s0.x, s1.x, std::sqrt(R2));
   }
+  // (f d) pairs of an l <= 3 quartet: the (d f| class kernels; any other: generic
+  bool route = false, to_class = rev[0] || rev[1];
+  for (int h = 0; h < 2; ++h)
+    if (rev[h] && !(lperm[2 * h] == 3 && lperm[2 * h + 1] == 2)) to_class = false;
+  if (std::max(std::max(lperm[0], lperm[1]), std::max(lperm[2], lperm[3])) > 3) to_class = false;
+  for (int h = 0; h < 2; ++h)
+    if (rev[h]) swp(2 * h, 2 * h + 1);
+  if (to_class) {
+    if (ib_pair_ext(lperm[0], lperm[1]) < ib_pair_ext(lperm[2], lperm[3])) {
+      swp(0, 2);
+      swp(1, 3);
+    }
+  } else if (rev[0] || rev[1]) {
+    route = true;
+  }
+  const int pbx = ib_pair_ext(lperm[0], lperm[1]), pkx = ib_pair_ext(lperm[2], lperm[3]);
+  const int cidx = to_class ? pbx * (pbx + 1) / 2 + pkx : cid;
   int b = 0;
   for (int ka = 0; ka < sh[0].ncont; ++ka)
     for (int kb = 0; kb < sh[1].ncont; ++kb)
@@ -713,10 +732,10 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
           hit[b] = it;
         }
   std::memset(hrg, 0, kNRanges * sizeof(int));
-  const bool emitted = c->table[cid].launch != nullptr && !route;
+  const bool emitted = c->table[cidx].launch != nullptr && !route;
   if (emitted) {
-    hrg[2 * cid] = 0;
-    hrg[2 * cid + 1] = nblk;
+    hrg[2 * cidx] = 0;
+    hrg[2 * cidx + 1] = nblk;
   } else {
     hrg[kSlotGeneric] = 0;
     hrg[kSlotGeneric + 1] = nblk;
@@ -741,11 +760,11 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
   a.out = c->d_cart.as<double>();
   IB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
   if (emitted) {
-    const int vt = 4 * c->minb_idx[cid][0];
-    const int grid = std::max(1, std::min(c->nsm * c->occ[cid][vt], (nblk + IB_BLOCK - 1) / IB_BLOCK));
+    const int vt = 4 * c->minb_idx[cidx][0];
+    const int grid = std::max(1, std::min(c->nsm * c->occ[cidx][vt], (nblk + IB_BLOCK - 1) / IB_BLOCK));
     a.counter = c->counters.as<int>() + kNCounters;  // never used by a batch that may still run
     IB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
-    c->table[cid].launch(vt, grid, s, a);
+    c->table[cidx].launch(vt, grid, s, a);
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
     long long nb = std::min<long long>({(long long)nblk, 2LL * c->nsm,

@@ -41,7 +41,14 @@ THREAD_CLASSES = set()
 
 DIRS = 'xyz'
 NPAIR_TOTAL = 7 * 8 // 2                       # shell pairs with l <= 6 (IB_NPAIR)
-NCLASS_TOTAL = NPAIR_TOTAL * (NPAIR_TOTAL + 1) // 2  # canonical classes (IB_NCLASS)
+# pair ids: la >= lb canonical (0..27), and (2,3) -- a d shell built on before
+# its f partner -- as pair 28 (IB_NPAIR_EXT): the one reversed pair with class
+# kernels, for pairs whose horizontal recurrence is ill-conditioned the
+# canonical way round (the runtime routes other reversed pairs to the generic
+# kernel)
+REV_PAIRS = {(2, 3): NPAIR_TOTAL}
+NPAIR_EXT = NPAIR_TOTAL + len(REV_PAIRS)
+NCLASS_TOTAL = NPAIR_EXT * (NPAIR_EXT + 1) // 2  # class ids (IB_NCLASS)
 
 
 def comps(l):
@@ -60,7 +67,9 @@ def comps_range(lo, hi):
 
 
 def pair_index(la, lb):
-    return la * (la + 1) // 2 + lb
+    if la >= lb:
+        return la * (la + 1) // 2 + lb
+    return REV_PAIRS[(la, lb)]
 
 
 def class_id(la, lb, lc, ld):
@@ -435,6 +444,11 @@ def emitted_classes():
     out = [(c, True) for c in canonical_classes(LMAX_EMIT)]
     for c in canonical_classes(4):
         if max(c) >= 3 and group_fits(c):
+            out.append((c, False))
+    # the reversed (d f| pair against every pair up to f (bra: its pair id is the largest)
+    for kp in [(a, b) for a in range(4) for b in range(a + 1)] + [(2, 3)]:
+        c = (2, 3) + kp
+        if group_fits(c):
             out.append((c, False))
     out.sort(key=lambda x: class_id(*x[0]))
     return out

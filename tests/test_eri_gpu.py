@@ -588,3 +588,76 @@ def test_ill_conditioned_pairs_built_on_the_compact_shell(sph):
         blk = refs[offs[i]:offs[i] + np.prod(n)].reshape(n[3], n[2], n[0], n[1]).transpose(0, 1, 3, 2).ravel()
         worst = max(worst, float(np.abs(out[off[i]:off[i] + np.prod(n)] - blk).max()))
     assert worst <= tolerance(refs), worst
+
+
+@pytest.mark.parametrize('sph', [False, True])
+def test_df_class_kernels_for_ill_conditioned_fd_pairs(sph):
+    """(f d) pairs of a diffuse f and a tight d shell 2-4 bohr apart, in the
+    bra, the ket or both, against partners up to f: the (d f| class kernels
+    (the d shell built on) must match, at the flat bar, the oracle evaluated
+    with every such pair swapped (its stable order), block transposed back."""
+    rng = np.random.default_rng(311 + sph)
+    ls, xs, cs, cens, ks, quartets, swaps = [], [], [], [], [], [], []
+
+    def shell(l, lo, hi, cen):
+        k = int(rng.integers(1, 3))
+        e = np.exp(rng.uniform(np.log(lo), np.log(hi), k))
+        ls.append(l)
+        ks.append(k)
+        xs.append(e)
+        cs.append(basis.normalize_shell(l, e, rng.uniform(0.1, 1.0, k)))
+        cens.append(cen)
+        return len(ls) - 1
+
+    def fd_pair():
+        A = rng.uniform(0, 1, 3)
+        u = rng.normal(size=3)
+        return shell(3, 0.08, 0.3, A), shell(2, 2e3, 5e4, A + rng.uniform(2.0, 4.0) * u / np.linalg.norm(u))
+
+    for rep in range(4):
+        for kind in ('bra', 'ket', 'both'):
+            for lp in [(0, 0), (1, 0), (2, 1), (3, 3), (3, 1)]:
+                if kind == 'both':
+                    a, b = fd_pair()
+                    c, d = fd_pair()
+                    quartets.append([a, b, c, d])
+                    swaps.append((True, True))
+                else:
+                    a, b = fd_pair()
+                    C = rng.uniform(0, 3, 3)
+                    c = shell(lp[0], 0.3, 20.0, C)
+                    d = shell(lp[1], 0.3, 20.0, C + 0.7)
+                    quartets.append([a, b, c, d] if kind == 'bra' else [c, d, a, b])
+                    swaps.append((kind == 'bra', kind == 'ket'))
+    l_ = np.array(ls, np.int32)
+    k_ = np.array(ks, np.int32)
+    p_ = np.concatenate([[0], np.cumsum(k_)[:-1]]).astype(np.int32)
+    q = np.array(quartets, np.int32)
+    def mk(qq):
+        off, total = basis.packed_offsets(l_, qq, sph)
+        return basis.ShellBatch(l_, k_, p_, np.array(cens), np.concatenate(xs), np.concatenate(cs), qq, off, sph,
+                                total)
+
+    b = mk(q)
+    out = run_batch(b)
+    qs = q.copy()
+    for i, (sb, sk) in enumerate(swaps):
+        if sb:
+            qs[i, [0, 1]] = qs[i, [1, 0]]
+        if sk:
+            qs[i, [2, 3]] = qs[i, [3, 2]]
+    bs = mk(qs)
+    refs = loader.oracle_batch(bs, basis.sph_matrices(6))
+    worst = 0.0
+    for i in range(b.nq):
+        n = [2 * l_[s] + 1 if sph else (l_[s] + 1) * (l_[s] + 2) // 2 for s in q[i]]
+        ns = [n[1], n[0], n[2], n[3]] if swaps[i][0] else list(n)
+        if swaps[i][1]:
+            ns[2], ns[3] = ns[3], ns[2]
+        blk = refs[bs.out_off[i]:bs.out_off[i] + np.prod(n)].reshape(ns[3], ns[2], ns[1], ns[0])
+        if swaps[i][0]:
+            blk = blk.transpose(0, 1, 3, 2)
+        if swaps[i][1]:
+            blk = blk.transpose(1, 0, 2, 3)
+        worst = max(worst, float(np.abs(out[b.out_off[i]:b.out_off[i] + np.prod(n)] - blk.ravel()).max()))
+    assert worst <= tolerance(refs), worst
