@@ -80,9 +80,11 @@ def parse():
     ap.add_argument('--npairs', type=int, default=4_000_000)
     ap.add_argument('--nq-lattice', type=int, default=2_000_000)
     ap.add_argument('--nq-c5', type=int, default=50_000)
-    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim'],
+    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim', 'class'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time; fp64_cart '
-                         'is the FP64 step with Cartesian output (no spherical transform)')
+                         'is the FP64 step with Cartesian output (no spherical transform); class runs one class '
+                         '(--cls) alone, FP64 then its FP32 kernel with every quartet in the FP32 tier')
+    ap.add_argument('--cls', default='2222', help='--only class: the class as four digits la lb lc ld')
     return ap.parse_args()
 
 
@@ -274,6 +276,19 @@ def reference_error(batch, outs, nsample=20000, seed=123):
     sizes = basis.block_sizes(batch.shell_l, batch.quartets[idx], batch.spherical)
     gather = np.concatenate([np.arange(o, o + n) for o, n in zip(batch.out_off[idx], sizes)])
     res = {name: float(np.abs(out[gather] - ref).max()) for name, out in outs.items()}
+    # the quartets with the largest differences (first path), for diagnosis
+    name0 = next(iter(outs))
+    diff = np.abs(outs[name0][gather] - ref)
+    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    perq = np.maximum.reduceat(diff, starts) if len(starts) else np.zeros(0)
+    worst = []
+    for w in np.argsort(-perq)[:5]:
+        qq = batch.quartets[idx[w]]
+        exps = [batch.prim_exp[batch.shell_ptr[s_]:batch.shell_ptr[s_] + batch.shell_k[s_]] for s_ in qq]
+        worst.append({'l': [int(batch.shell_l[s_]) for s_ in qq], 'k': [int(batch.shell_k[s_]) for s_ in qq],
+                      'exp_range': [[float(e.min()), float(e.max())] for e in exps],
+                      'err': float(perq[w]), 'max_abs': float(np.abs(ref[starts[w]:starts[w] + sizes[w]]).max())})
+    res['worst_quartets_' + name0] = worst
     res['sample'] = '%d seeded random quartets of this rank\'s batch vs the %s C99, unscreened' % (len(idx), kind)
     res['max_abs_reference'] = float(np.abs(ref).max())
     return res
@@ -725,10 +740,45 @@ def run_only(args, eng, out):
                       'kernels_per_step': eri.EriEngine.last_launch_count() + (1 if screened else 0)}), flush=True)
 
 
+def run_one_class(args):
+    """One class alone (--cls), --nq quartets with the headline distribution:
+    W warm-up + K timed steps of the FP64 kernel, then of the class's FP32
+    kernel with every quartet in the FP32 tier and every result kept (what the
+    FP32 kernel costs, for profilers)."""
+    import torch
+    from intception_b200 import eri
+    from intception_b200.autotune import class_batch
+    cls = tuple(int(ch) for ch in args.cls)
+    b = class_batch(cls, args.nq, seed=1000, spherical=True)
+    eng = eri.EriEngine(b)
+    out = torch.empty(b.out_size, dtype=torch.float64, device='cuda')
+    ones = torch.ones(b.nq, dtype=torch.float64, device='cuda')
+    eri.set_class_fp32(True, cls)
+    res = {'only': 'class', 'cls': args.cls, 'nq': b.nq}
+    for name, prec in (('fp64', eri.PREC_FP64), ('fp32', eri.PREC_MIXED)):
+        kw = dict(bounds=ones, skip_below=0.0, fp32_below=2.0, mixed_tol=1e300) if prec == eri.PREC_MIXED else {}
+        for _ in range(args.warmup):
+            eng.compute(out=out, precision=prec, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            eng.compute(out=out, precision=prec, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        assert eng.device_status() == 0
+        res[name + '_ms'] = e0.elapsed_time(e1) / args.steps
+    eri.set_class_fp32(None, cls)
+    print(json.dumps(res), flush=True)
+
+
 def run_eri(args, rank, world, local):
     """The headline workload: one C2 batch, split over the ranks."""
     import torch
     from intception_b200 import basis, eri, shard
+    if args.only == 'class':
+        run_one_class(args)
+        return
     full = basis.config_mixed_l2(nq=args.nq, seed=1, spherical=args.only != 'fp64_cart')
     batch = full if world == 1 else shard.shard_for_rank(full, rank, world)[0]
     eng = eri.EriEngine(batch)

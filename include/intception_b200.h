@@ -198,8 +198,8 @@ int intception_b200_schwarz(const intception_b200_basis *basis, const int *pairs
  * 1.001); bounds[q] = Q_ab Q_cd by Cauchy-Schwarz in the Coulomb metric.  No ERI is evaluated: one pass over
  * the primitive pairs, cheap enough to run with every batch (on a random l <= 2
  * batch it keeps 1.3x the quartets Schwarz factors keep at 1e-12).  A value
- * whose true bound is below about 1e-300 may read 0.  An l outside [0, 6]
- * gives +inf.  New: the reference has no screening. */
+ * whose true bound is below about 1e-300 may read 0.  A pair with an l above
+ * basis->lmax (or outside [0, 6]) gives +inf.  New: the reference has no screening. */
 int intception_b200_quartet_bounds(const intception_b200_basis *basis, const int *quartets, int nq, int spherical,
                                    double *bounds, void *stream);
 

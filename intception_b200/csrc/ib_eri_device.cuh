@@ -574,6 +574,7 @@ __device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa
 // result is within a few hundred ulp (< 1e-4 relative) of the exact one; the
 // factor 1.001 makes it an upper bound.  The Gaussian factor exp(-x0 x1 R^2 /
 // zeta) stays in FP64 below exp(-80), where float would flush it to zero.
+template <int MAXDEG>
 __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double cc, double x0, double x1,
                                                    double R) {
   const float z = (float)(x0 + x1), oz = 1.0f / z;
@@ -581,11 +582,11 @@ __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, dou
   const double e = argd > -80.0 ? (double)__expf((float)argd) : exp(argd);
   const float pa = (float)x1 * oz * (float)R, pb = (float)x0 * oz * (float)R;
   const int deg = l0 + l1;
-  float c[13];
+  float c[MAXDEG + 1];  // MAXDEG >= l0 + l1: the batch's 2 lmax, so the unrolled loops stay short
 #pragma unroll
-  for (int n = 0; n < 13; ++n) c[n] = n == 0 ? 1.0f : 0.0f;
+  for (int n = 0; n <= MAXDEG; ++n) c[n] = n == 0 ? 1.0f : 0.0f;
 #pragma unroll
-  for (int r = 0; r < 12; ++r) {
+  for (int r = 0; r < MAXDEG; ++r) {
     if (r < deg) {
       const float p = r < l0 ? pa : pb;
 #pragma unroll
@@ -596,7 +597,7 @@ __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, dou
   const float s = rsqrtf(z);
   float poly = 0.0f, sn = 1.0f;
 #pragma unroll
-  for (int n = 0; n < 13; ++n) {
+  for (int n = 0; n <= MAXDEG; ++n) {
     if (n <= deg) poly = fmaf(c[n] * (float)ib_rn_norm(n), sn, poly);
     sn *= s;
   }

@@ -162,6 +162,15 @@ __device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
   }
 }
 
+// ib_reverse_for_classes out of line: classify runs it for every evaluated
+// quartet but it rarely does anything, and inlined its registers would lower
+// the occupancy of the whole (gather-latency-bound) kernel.
+__device__ __noinline__ int ib_reverse_noinline(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
+                                                const double* __restrict__ prim_exp,
+                                                const double* __restrict__ shell_xyz, int* s, int* l, int* st) {
+  return ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
+}
+
 __global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
                             const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                             const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz, int nq,
@@ -186,7 +195,7 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     // horizontal recurrence would lose too many digits that way is built on
     // the other shell: by the (d f| class kernels for an (f d) pair of an
     // l <= 3 quartet, else by the generic kernel (ib_reverse_for_classes)
-    const int rv = (!skip && !bad) ? ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st) : 0;
+    const int rv = (!skip && !bad) ? ib_reverse_noinline(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st) : 0;
     const int pb = ib_pair_ext(l[0], l[1]), pk = ib_pair_ext(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
     const int nprim = shell_k[s[0]] * shell_k[s[1]] * shell_k[s[2]] * shell_k[s[3]];
@@ -292,6 +301,7 @@ __global__ void ib_zero_screened(const unsigned* __restrict__ keys, int nq, cons
 // inequality over the contraction), then bounds[q] = Q_ab Q_cd >= |(ab|cd)| of
 // every element (Cauchy-Schwarz in the Coulomb metric).  An l outside [0, 6]
 // gives +inf (never screened; the batch reports it).
+template <int MAXDEG>
 __global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, const int* __restrict__ shell_l,
                                   const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                                   const double* __restrict__ shell_xyz, const double* __restrict__ prim_exp,
@@ -304,7 +314,7 @@ __global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, cons
     if (q < nq) {
       const int s0 = __ldg(quartets + 4 * q + 2 * side), s1 = __ldg(quartets + 4 * q + 2 * side + 1);
       const int l0 = __ldg(shell_l + s0), l1 = __ldg(shell_l + s1);
-      if (l0 < 0 || l0 > IB_LMAX || l1 < 0 || l1 > IB_LMAX) {
+      if (l0 < 0 || l1 < 0 || l0 > IB_LMAX || l1 > IB_LMAX || l0 + l1 > MAXDEG) {  // l above lmax: never screened
         Q = __longlong_as_double(0x7ff0000000000000LL);
       } else {
         const int k0 = __ldg(shell_k + s0), k1 = __ldg(shell_k + s1);
@@ -319,7 +329,7 @@ __global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, cons
           const double x0 = __ldg(prim_exp + p0 + i), c0 = __ldg(prim_coef + p0 + i);
           for (int j = 0; j < k1; ++j) {
             const double x1 = __ldg(prim_exp + p1 + j), c1 = __ldg(prim_coef + p1 + j);
-            Q += ib_pair_bound_rt(l0, l1, spherical != 0, c0 * c1, x0, x1, R);
+            Q += ib_pair_bound_rt<MAXDEG>(l0, l1, spherical != 0, c0 * c1, x0, x1, R);
           }
         }
         Q *= 1.000001;  // the rounding of the sum
@@ -1168,9 +1178,21 @@ int intception_b200_quartet_bounds(const intception_b200_basis* basis, const int
   resolve_stream(c, stream, &s);
   const long long threads = 2LL * ((nq + 15) / 16) * 16;
   const int grid = (int)std::min<long long>((threads + 255) / 256, (long long)c->nsm * 16);
-  ib_quartet_bounds<<<grid, 256, 0, s>>>(quartets, nq, basis->shell_l, basis->shell_k, basis->shell_ptr,
-                                         basis->shell_xyz, basis->prim_exp, basis->prim_coef, spherical ? 1 : 0,
-                                         bounds);
+  if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "quartet_bounds: basis lmax out of range");
+#define IB_QB(D)                                                                                                 \
+  ib_quartet_bounds<D><<<grid, 256, 0, s>>>(quartets, nq, basis->shell_l, basis->shell_k, basis->shell_ptr,      \
+                                            basis->shell_xyz, basis->prim_exp, basis->prim_coef, spherical ? 1 : 0, \
+                                            bounds)
+  switch (basis->lmax) {  // the polynomial degree is at most 2 lmax
+    case 0: IB_QB(0); break;
+    case 1: IB_QB(2); break;
+    case 2: IB_QB(4); break;
+    case 3: IB_QB(6); break;
+    case 4: IB_QB(8); break;
+    case 5: IB_QB(10); break;
+    default: IB_QB(12); break;
+  }
+#undef IB_QB
   IB_CUDA(cudaGetLastError());
   return set_status(IB_OK, "");
 }
