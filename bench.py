@@ -57,6 +57,7 @@ SKIP_BELOW = 1e-12      # screening: blocks whose bound is smaller are written a
 FP32_BELOW = 1e-4       # mixed path: FP32 VRR attempted below this bound ...
 MIXED_TOL = 5e-11       # ... and kept only where its rounding-error bound is below this; else FP64
 PRIM_TOL = 1e-18        # screened paths: primitive quartets with Q_ab Q_cd below this skipped
+HRR_TOL = 1e-13         # class kernels: HRR rounding-error estimate above this -> generic kernel (library default)
 FP32_SWEEP = (0.0, 1e-10, 1e-8, 1e-6, 1e-4)  # candidate FP32-tier bounds (0 = tier off), tuned per run
 FP32_CHOSEN = [0.0]
 ERR_BAR = 1e-10
@@ -425,12 +426,19 @@ def run_c5(args, rank, world, local):
     clk = ClockSampler(local).__enter__()
     eri.set_prim_tol(0.0)
     ms64 = timed(lambda: eng.compute(out=out))
+    redo64 = eri.last_hrr_redo()
     ref = out.clone()
     host = {'fp64_exact': ref.cpu().numpy()}
+    # once, untimed: the class kernels' results without the HRR check (no redo)
+    eri.set_hrr_tol(0.0)
+    eng.compute(out=out)
+    host['fp64_no_hrr_check'] = out.cpu().numpy()
+    eri.set_hrr_tol(HRR_TOL)
     eri.set_prim_tol(PRIM_TOL)
     mss = timed(lambda: screened_step(eri.PREC_FP64))
     errs = max_over_ranks(float((out - ref).abs().max().item()), world)
     msm = timed(lambda: screened_step(eri.PREC_MIXED))
+    redom = eri.last_hrr_redo()
     errm = max_over_ranks(float((out - ref).abs().max().item()), world)
     host['mixed'] = out.cpu().numpy()
     launches = eri.EriEngine.last_launch_count() + 1
@@ -466,11 +474,12 @@ def run_c5(args, rank, world, local):
                        'l2': 'outputs %.0f MB per step; no flush' % (batch.out_size * 8 / 1e6)},
             'max_abs_err_vs_fp64': errm, 'max_abs_err_vs_reference': ref_err,
             'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'every sampled quartet, FP64',
-                     'ns_per_live_primitive_quartet': ms64 * 1e6 / nprim},
+                     'ns_per_live_primitive_quartet': ms64 * 1e6 / nprim, 'hrr_redo': redo64},
             'fp64_screened': {'ms_per_step': mss, 'value': nq / (mss * 1e-3), 'max_abs_err_vs_fp64': errs,
                               'note': 'the mixed path\'s screening, FP64 throughout'},
-            'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm},
+            'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm, 'hrr_redo': redom},
             'cuda_graph': {'ms_per_step': msg, 'max_abs_err_vs_fp64': errg},
+            'hrr_tol': HRR_TOL,
             'mixed_over_fp64': mss / msm, 'live_primitive_quartets': nprim,
             'estimated_5e7_quartets_s': 5e7 / (nq / (msm * 1e-3)),
             'cpu_baseline': cpu, 'gpu_launches': launches * args.steps, 'clocks': clk.summary()}), flush=True)
@@ -527,6 +536,7 @@ def run_lattice(args, rank, world, local):
     errm = max_over_ranks(float((out - ref).abs().max().item()), world)
     host['mixed'] = out.cpu().numpy()
     rej = eng.fp32_rejected()
+    redo_m = eri.last_hrr_redo()
     nfp32 = int((bounds < FP32_BELOW).sum().item())
     # the fastest path within 1e-10 of exact FP64, then measured again on its own
     cands = [(ms64, 0.0, 'fp64'), (msp, errp, 'fp64 + primitive screening'), (msm, errm, 'precision tiers')]
@@ -564,7 +574,7 @@ def run_lattice(args, rank, world, local):
             'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'exact, no screening'},
             'fp64_prim': {'ms_per_step': msp, 'max_abs_err_vs_fp64': errp},
             'mixed': {'ms_per_step': msm, 'max_abs_err_vs_fp64': errm, 'fp32_attempted': nfp32,
-                      'fp32_rejected': rej},
+                      'fp32_rejected': rej, 'hrr_redo': redo_m},
             'estimated_full_lattice_s': total / (nq / (ms * 1e-3)),
             'cpu_baseline': cpu, 'gpu_launches': launches * args.steps, 'clocks': clk.summary()}), flush=True)
 
@@ -820,6 +830,7 @@ def run_eri(args, rank, world, local):
     eri.set_prim_tol(0.0)
     ms64 = timed(lambda: eng.compute(out=out))
     launches64 = eri.EriEngine.last_launch_count()
+    redo64 = eri.last_hrr_redo()
     ref64 = out.clone()
     host_fp64 = out.cpu().numpy() if rank == 0 else None
     # ---- screened FP64: analytic bounds in the step, zeros below SKIP_BELOW, primitive screening
@@ -851,6 +862,7 @@ def run_eri(args, rank, world, local):
     launches = eri.EriEngine.last_launch_count() + 1  # + the bounds kernel
     err_m = err_vs(ref64)
     rej = eng.fp32_rejected() if fb > 0 else 0
+    redo_m = eri.last_hrr_redo()
     host_mixed = out.cpu().numpy() if rank == 0 else None
     value = rate(msm)
     # ---- the headline configuration replayed from a CUDA graph (bounds kernel
@@ -954,10 +966,11 @@ def run_eri(args, rank, world, local):
                 'max_abs_err_vs_fp64': err_m,
                 'max_abs_err_vs_reference': ref_err,
                 'fp64_exact': {'value': rate(ms64), 'ms_per_step': ms64, 'kernels_per_step': launches64,
-                               'note': 'every quartet evaluated in FP64, no screening'},
+                               'hrr_redo': redo64, 'note': 'every quartet evaluated in FP64, no screening'},
                 'fp64_screened': fp64_s,
                 'mixed': {'value': value, 'ms_per_step': msm, 'fp32_below': fb, 'fp32_tier_active': fb > 0,
-                          'fp32_rejected': rej, 'mixed_tol': MIXED_TOL, 'fp32_sweep': sweep,
+                          'fp32_rejected': rej, 'hrr_redo': redo_m, 'hrr_tol': HRR_TOL, 'mixed_tol': MIXED_TOL,
+                          'fp32_sweep': sweep,
                           'note': 'fp32_below chosen by the sweep (fastest within 1e-10), then measured again '
                                   'on its own; the same screening as fp64_screened'},
                 'mixed_over_fp64': value / rate(ms_s),

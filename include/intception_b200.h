@@ -206,9 +206,16 @@ int intception_b200_quartet_bounds(const intception_b200_basis *basis, const int
 /* Number of library kernels the last intception_b200_eri_batch launched. */
 int intception_b200_last_launch_count(void);
 
-/* Waits for the device and returns how many quartets of the last IB_PREC_MIXED
- * batch had their FP32 result rejected by the error bound and recomputed in FP64. */
+/* Waits for the device and returns how many quartets of the last batch had
+ * their FP32 result rejected by the error bound and recomputed in FP64 (0
+ * unless that batch was IB_PREC_MIXED). */
 int intception_b200_last_fp32_rejections(void);
+
+/* Waits for the device and returns how many quartets of the last batch (or
+ * drop-in call) the unrolled class kernels handed to the generic kernel
+ * because their HRR rounding-error estimate exceeded the tolerance
+ * (intception_b200_set_hrr_tol).  New: the reference has no counterpart. */
+int intception_b200_last_hrr_redo(void);
 
 /* Tuning: at most cap lane groups (a power of two; 0 = no cap) share one
  * contracted quartet in the kernel of canonical class cid (cid < 0: every
@@ -227,6 +234,21 @@ int intception_b200_set_slice_cap(int cid, int cap);
  * tol outside [0, 1e-6] returns IB_ERR_ARG.  The drop-in functions never
  * screen.  New: the reference evaluates every primitive quartet. */
 int intception_b200_set_prim_tol(double tol);
+
+/* HRR conditioning check of the unrolled class kernels (batch entries and
+ * drop-ins).  A pair whose contraction mixes tight and diffuse exponents on
+ * both shells has no orientation in which all its primitive pairs keep the
+ * horizontal recurrence well conditioned; after contraction each class kernel
+ * estimates its HRR rounding error as 32 x 2^-53 x the largest contracted
+ * [e0|f0] element times its HRR coefficient bound C(lb,k) |AB|^(lb-k)
+ * C(ld,j) |CD|^(ld-j) (k, j its levels above la, lc) and, when that exceeds
+ * tol, the quartet is recomputed by the generic kernel, which builds every
+ * primitive pair on the shell that conditions its HRR.  Default 1e-13
+ * (outputs then agree with an exact evaluation to about 1e-13 on such
+ * quartets); 0 switches the check off; tol outside [0, 1e-6] returns
+ * IB_ERR_ARG.  New: the reference builds the ket by vertical recurrences on
+ * both shells and has no such check. */
+int intception_b200_set_hrr_tol(double tol);
 
 /* Tuning: register budget of the kernel of canonical class cid for variant v4
  * (0 FP64 Cartesian, 1 FP64 spherical, 2 FP32 Cartesian, 3 FP32 spherical):

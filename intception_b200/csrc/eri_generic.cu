@@ -1,11 +1,22 @@
 // eri_generic.cu -- one thread block per contracted quartet, any l <= IB_LMAX.
 //
 // Used for the classes that have no unrolled kernel (some l > the emitted
-// maximum).  Same schedule as the emitted kernels (HGP: bra VRR, ket VRR with
-// the electron-transfer term, contraction, bra HRR, ket HRR, spherical
-// transform), but every stage is a loop over the elements of one recurrence
-// level, spread over the block's threads, with the levels in global scratch
-// (one slice per resident block).  FP64 throughout.
+// maximum), for quartets whose pairs are best built on their lower-l shell,
+// and for the quartets the class kernels put on the redo list (HRR rounding
+// estimate over the tolerance).  Same schedule as the emitted kernels (HGP:
+// bra VRR, ket VRR with the electron-transfer term, contraction, bra HRR, ket
+// HRR, spherical transform), but every stage is a loop over the elements of
+// one recurrence level, spread over the block's threads, with the levels in
+// global scratch (one slice per resident block).  FP64 throughout.
+//
+// Each primitive pair is built on the shell that conditions its HRR
+// (ib_gen_orient): a contraction that mixes tight and diffuse exponents on
+// both shells of a pair has no single good orientation (whichever shell the
+// recurrences build on, some primitive pairs put the product centre far from
+// it and the HRR then cancels many digits), so the quartet is evaluated in up
+// to four passes, one per (bra orientation, ket orientation) that some
+// primitive quartet uses, each over those primitive quartets only; the first
+// pass stores the block and the others add to it.
 //
 // Scratch slice layout (doubles), sizes from ib_generic_dims():
 //   acc  [ne * nf]                 contracted [e0|f0], e in [la,la+lb], f in [lc,lc+ld]
@@ -30,13 +41,31 @@ __device__ __forceinline__ void ib_comp_of(int cum, int& x, int& y, int& z) {
   x = l - s;
 }
 
+// Orientation of one primitive pair (exponents x0 on the pair's first shell,
+// l0, and x1 on its second, l1, R apart): 0 builds it on the first shell and
+// moves l1 quanta to the second by the HRR, 1 the other way round; the one
+// with the smaller growth bound ((sig + |PA| + R) / (sig + |PB|))^l_moved
+// (ib_hrr_kappa's per-pair term; ties: 0).  Every thread evaluates it alike.
+__device__ __forceinline__ int ib_gen_orient(int l0, int l1, double x0, double x1, float R) {
+  if (l1 == 0) return 0;
+  if (l0 == 0) return 1;
+  const float a = (float)x0, b = (float)x1, z = a + b, oz = 1.0f / z, sig = rsqrtf(z);
+  const float pa = b * oz * R, pb = a * oz * R;
+  const float g0 = (float)l1 * __logf((sig + pa + R) / (sig + pb));
+  const float g1 = (float)l0 * __logf((sig + pb + R) / (sig + pa));
+  return g1 < g0 ? 1 : 0;
+}
+
 struct IbGenShared {
   IbGenericDims d;
-  double A[3], B[3], C[3], D[3], AB[3], CD[3];
+  double A[3], B[3], C[3], D[3], AB[3], CD[3];  // this pass's shell order
   double PA[3], WP[3], QC[3], WQ[3];
   double o2z, roz, o2e, roe, o2zpe;
   double F[4 * IB_LMAX + 1];
-  int k[4], ptr[4], st[4];
+  int k[4], ptr[4], st[4];     // this pass's shell order
+  int s0[4], l0[4], st0[4];    // the item's shell order
+  int use[2];                  // per pair: bit o set when some primitive pair has orientation o
+  float R[2];                  // |AB|, |CD| of the item
   long long off;
 };
 
@@ -45,24 +74,57 @@ struct IbGenShared {
 __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
                                                                double* __restrict__ scratch, long long slice) {
   __shared__ IbGenShared sh;
-  const int beg = a.ranges[range_slot], end = a.ranges[range_slot + 1];
+  // range_slot < 0: the redo list (a.redo[0] items at a.redo + 1)
+  const bool redo = range_slot < 0;
+  const int beg = redo ? 0 : a.ranges[range_slot], end = redo ? a.redo[0] : a.ranges[range_slot + 1];
   double* __restrict__ w = scratch + (size_t)blockIdx.x * (size_t)slice;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int p = beg + blockIdx.x; p < end; p += gridDim.x) {
+  for (int pi = beg + blockIdx.x; pi < end; pi += gridDim.x) {
+    const int p = redo ? a.redo[1 + pi] : pi;
     if (tid == 0) {
       const IbItem it = a.items[p];
       const bool bad = it.st[0] == 0;  // an l out of range: evaluated as (ss|ss), the status already says so
+      for (int i = 0; i < 4; ++i) {
+        sh.s0[i] = it.s[i];
+        sh.l0[i] = bad ? 0 : a.shell_l[it.s[i]];
+        sh.st0[i] = it.st[i];
+      }
+      sh.off = it.off;
+      for (int h = 0; h < 2; ++h) {
+        const int s0 = it.s[2 * h], s1 = it.s[2 * h + 1];
+        double R2 = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          const double u = a.shell_xyz[3 * s0 + c] - a.shell_xyz[3 * s1 + c];
+          R2 += u * u;
+        }
+        sh.R[h] = (float)sqrt(R2);
+        const int k0 = a.shell_k[s0], k1 = a.shell_k[s1], p0 = a.shell_ptr[s0], p1 = a.shell_ptr[s1];
+        int use = 0;
+        for (int i = 0; i < k0 && use != 3; ++i)
+          for (int j = 0; j < k1 && use != 3; ++j)
+            use |= 1 << ib_gen_orient(sh.l0[2 * h], sh.l0[2 * h + 1], a.prim_exp[p0 + i], a.prim_exp[p1 + j], sh.R[h]);
+        sh.use[h] = use;
+      }
+    }
+    __syncthreads();
+    bool first = true;
+    for (int pass = 0; pass < 4; ++pass) {
+    const int ob = pass >> 1, ok = pass & 1;
+    if (!((sh.use[0] >> ob) & 1) || !((sh.use[1] >> ok) & 1)) continue;  // uniform: shared
+    const bool split_b = sh.use[0] == 3, split_k = sh.use[1] == 3;
+    __syncthreads();  // the previous pass is done with sh
+    if (tid == 0) {
+      const int ord[4] = {ob, 1 - ob, 2 + ok, 3 - ok};
       int l[4];
       for (int i = 0; i < 4; ++i) {
-        const int s = it.s[i];
-        l[i] = bad ? 0 : a.shell_l[s];
+        const int s = sh.s0[ord[i]];
+        l[i] = sh.l0[ord[i]];
         sh.k[i] = a.shell_k[s];
         sh.ptr[i] = a.shell_ptr[s];
-        sh.st[i] = it.st[i];
+        sh.st[i] = sh.st0[ord[i]];
         double* R = i == 0 ? sh.A : (i == 1 ? sh.B : (i == 2 ? sh.C : sh.D));
         for (int c = 0; c < 3; ++c) R[c] = a.shell_xyz[3 * s + c];
       }
-      sh.off = it.off;
       for (int c = 0; c < 3; ++c) {
         sh.AB[c] = sh.A[c] - sh.B[c];
         sh.CD[c] = sh.C[c] - sh.D[c];
@@ -73,8 +135,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
     const IbGenericDims d = sh.d;
     if ((long long)d.total > slice) {
       if (tid == 0) atomicExch(a.status, 3);  // scratch slice too small for this class
-      __syncthreads();
-      continue;
+      break;
     }
     double* acc = w + d.o_acc;
     double* bra = w + d.o_bra;
@@ -84,6 +145,20 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
     const double RCD2 = sh.CD[0] * sh.CD[0] + sh.CD[1] * sh.CD[1] + sh.CD[2] * sh.CD[2];
     const int nprim = sh.k[0] * sh.k[1] * sh.k[2] * sh.k[3];
     for (int pq = 0; pq < nprim; ++pq) {
+      {  // every thread decides alike: skip primitive quartets of other passes and exact zeros
+        int r = pq;
+        const int id = r % sh.k[3]; r /= sh.k[3];
+        const int ic = r % sh.k[2]; r /= sh.k[2];
+        const int ib = r % sh.k[1]; r /= sh.k[1];
+        const int ia = r;
+        const double xa = a.prim_exp[sh.ptr[0] + ia], xb = a.prim_exp[sh.ptr[1] + ib];
+        const double xc = a.prim_exp[sh.ptr[2] + ic], xd = a.prim_exp[sh.ptr[3] + id];
+        // the prefactor's Gaussian exactly as below: zero means the primitive quartet adds exact zeros
+        if (exp(-xa * xb * (1.0 / (xa + xb)) * RAB2 - xc * xd * (1.0 / (xc + xd)) * RCD2) == 0.0) continue;
+        // exponents in the item's order of each pair
+        if (split_b && ib_gen_orient(sh.l0[0], sh.l0[1], ob ? xb : xa, ob ? xa : xb, sh.R[0]) != ob) continue;
+        if (split_k && ib_gen_orient(sh.l0[2], sh.l0[3], ok ? xd : xc, ok ? xc : xd, sh.R[1]) != ok) continue;
+      }
       __syncthreads();
       if (tid == 0) {
         int r = pq;
@@ -280,9 +355,14 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
       const int i3 = idx % dims[3], r3 = idx / dims[3];
       const int i2 = r3 % dims[2], r2 = r3 / dims[2];
       const int i1 = r2 % dims[1], i0 = r2 / dims[1];
-      o[(long long)i0 * sh.st[0] + (long long)i1 * sh.st[1] + (long long)i2 * sh.st[2] + (long long)i3 * sh.st[3]] =
-          src[idx];
+      double* dst = o + (long long)i0 * sh.st[0] + (long long)i1 * sh.st[1] + (long long)i2 * sh.st[2] +
+                    (long long)i3 * sh.st[3];
+      // each element once per pass; an earlier pass's stores are visible after its closing barrier
+      *dst = first ? src[idx] : *dst + src[idx];
     }
+    first = false;
+    __syncthreads();
+    }  // pass
     __syncthreads();
   }
 }

@@ -47,14 +47,34 @@ struct IbLaunch {
   const double* sph;       // library Cartesian->spherical matrices, packed per l
   double* out;
   int* status;             // device error word (0 = ok)
-  int* flags;              // per sorted item: 1 = FP32 result rejected, recompute in FP64
-  int recheck;             // FP64 kernels: evaluate only flagged items
+  int* flags;              // per sorted item: bit 0 = FP32 result rejected (recompute in FP64),
+                           // bit 1 = on the redo list
+  int* redo;               // [0]: count, [1..]: sorted items the generic kernel recomputes (HRR check)
+  double hrr_tol;          // class kernels: largest accepted HRR rounding-error estimate (0: no check)
+  int recheck;             // FP64 kernels: evaluate only items with flag bit 0
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
   int max_slices;          // class kernels: cap on lane groups sharing one quartet (0: lane groups per block)
   int slice_boost;         // class kernels: choose slices as if the grid had this many times its lane groups (>= 1)
   int* counter;            // class kernels: next quartet of the range (zero before the launch; one per launch)
   double prim_tol;         // class kernels: skip primitive quartets whose bound is below this (0: exact zeros only)
 };
+
+// Rounding-error estimate of a class kernel's horizontal recurrences.  The
+// HRRs map the contracted [e0|f0] table linearly onto the block; an element at
+// levels (la + k, lc + j) enters every output with a coefficient of at most
+// C(lb,k) |AB|^(lb-k) C(ld,j) |CD|^(ld-j), and its rounding error (from the
+// vertical recurrences, the contraction and the HRR steps) with it.  The
+// kernels take the largest |element| x coefficient over the table and
+// multiply by IB_HRR_ERR_COEF.  Measured against binary128 evaluations of the
+// same scheme (l <= 4, K <= 8, exponents in [0.02, 1e5]; 162 quartets with an
+// error above 1e-16), the error stayed below 21.7 x 2^-53 x that maximum, so
+// with 32 units a quartet that passes a tolerance t is within about 0.7 t.
+#define IB_HRR_ERR_COEF (32.0 * 1.1102230246251565e-16)
+
+// Puts sorted item p on the generic kernel's redo list once (flag bit 1).
+__device__ __forceinline__ void ib_redo_push(const IbLaunch& a, int p) {
+  if (!(atomicOr(a.flags + p, 2) & 2)) a.redo[1 + atomicAdd(a.redo, 1)] = p;
+}
 
 // Smallest primitive exponent of shell s.
 __device__ __forceinline__ double ib_min_exp(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,

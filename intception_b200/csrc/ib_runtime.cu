@@ -116,13 +116,18 @@ struct Context {
   // FP64 step -5 %) and 8 is slower again.
   int slice_boost = 4;
   double prim_tol = 0.0;  // batch entries: primitive-quartet screening tolerance (0: exact zeros only)
+  // class kernels: quartets whose HRR rounding-error estimate (IB_HRR_ERR_COEF
+  // x the largest weighted contracted element) exceeds this are recomputed by
+  // the generic kernel (0: no check)
+  double hrr_tol = 1e-13;
   cudaStream_t side[kNSideMax] = {};
   cudaEvent_t fork = nullptr, join[kNSideMax] = {};
   DevBuf boys_tab, sph, keys, vals, keys2, vals2, items, ranges, status, cub_tmp, scratch;
   DevBuf counters;  // per class kernel launch of a batch: the next quartet (FP64, FP32, FP64 recheck passes)
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
-  DevBuf flags;                                             // FP32 rejections of the last mixed batch
-  int flags_nq = 0;                                         // its quartet count (flags beyond it are stale)
+  DevBuf flags;    // per sorted item of the last batch: FP32 rejection (bit 0), on the redo list (bit 1)
+  int flags_nq = 0;  // its quartet count (flags beyond it are stale)
+  DevBuf redo;     // the last batch's redo list: count, then sorted items
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
   int kind_h[IB_NCLASS] = {};  // host copy of kind: 2 where the class has FP32 kernels and the FP32 tier uses them
   DevBuf d_stage, d_cart, d_res;
@@ -528,6 +533,18 @@ int class_lmax(int cid) {
   return std::max(pair_lmax(pb), pair_lmax(pk));
 }
 
+// The generic kernel over the redo list of a (on stream s, after the class
+// kernels that fill it).
+cudaError_t redo_launch(Context* c, cudaStream_t s, const IbLaunch& a, bool sph, int lmax) {
+  const long long slice = generic_slice(lmax);
+  long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
+  nblk = std::max<long long>(nblk, 1);
+  cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
+  if (e != cudaSuccess) return e;
+  ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, s>>>(a, -1, sph ? 1 : 0, c->scratch.as<double>(), slice);
+  return cudaGetLastError();
+}
+
 // Launch the emitted kernels for the given variants and the generic kernel;
 // items/ranges already on the device.  Returns the number of kernels launched.
 int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
@@ -588,6 +605,12 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   for (int i = 0; i < c->nside; ++i) {
     IB_CUDA(cudaEventRecord(c->join[i], c->side[i]));
     IB_CUDA(cudaStreamWaitEvent(s, c->join[i], 0));
+  }
+  // after every class kernel: the quartets they put on the redo list (an
+  // empty list returns at once)
+  if (a.redo && a.hrr_tol > 0.0) {
+    IB_CUDA(redo_launch(c, s, a, sph, lmax));
+    ++k;
   }
   *nlaunch += k;
   return IB_OK;
@@ -774,7 +797,17 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     const int grid = std::max(1, std::min(c->nsm * c->occ[cidx][vt], (nblk + IB_BLOCK - 1) / IB_BLOCK));
     a.counter = c->counters.as<int>() + kNCounters;  // never used by a batch that may still run
     IB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
+    IB_CUDA(c->flags.ensure((size_t)nblk * sizeof(int)));
+    IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nblk * sizeof(int), s));
+    IB_CUDA(c->redo.ensure((size_t)(nblk + 1) * sizeof(int)));
+    IB_CUDA(cudaMemsetAsync(c->redo.p, 0, sizeof(int), s));
+    c->flags_nq = nblk;
+    a.flags = c->flags.as<int>();
+    a.redo = c->redo.as<int>();
+    a.hrr_tol = c->hrr_tol;
     c->table[cidx].launch(vt, grid, s, a);
+    if (a.hrr_tol > 0.0)
+      IB_CUDA(redo_launch(c, s, a, false, std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l))));
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
     long long nb = std::min<long long>({(long long)nblk, 2LL * c->nsm,
@@ -976,13 +1009,15 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   a.prim_coef = basis->prim_coef;
   a.out = out;
   a.prim_tol = screen_prims ? c->prim_tol : 0.0;
-  if (precision == IB_PREC_MIXED) {
-    IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
-    IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
-    c->flags_nq = nq;
-    a.flags = c->flags.as<int>();
-    a.mixed_tol = mixed_tol;
-  }
+  IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
+  IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
+  IB_CUDA(c->redo.ensure((size_t)(nq + 1) * sizeof(int)));
+  IB_CUDA(cudaMemsetAsync(c->redo.p, 0, sizeof(int), s));
+  c->flags_nq = nq;
+  a.flags = c->flags.as<int>();
+  a.redo = c->redo.as<int>();
+  a.hrr_tol = c->hrr_tol;
+  if (precision == IB_PREC_MIXED) a.mixed_tol = mixed_tol;
   const ZeroFill zf = {c->keys.as<unsigned>(), nq, quartets, basis->shell_l, out_off};
   return dispatch(c, s, a, true, precision == IB_PREC_MIXED, spherical != 0, basis->lmax, nl,
                   use_bounds && skip_below > 0.0 ? &zf : nullptr);
@@ -1267,20 +1302,45 @@ int intception_b200_eri_graph_destroy(void* handle) {
   return set_status(IB_OK, "");
 }
 
-// Number of quartets of the last mixed batch whose FP32 result was rejected
-// and recomputed in FP64 (synchronous).
+// Number of quartets of the last batch whose FP32 result was rejected and
+// recomputed in FP64 (0 unless it was a mixed batch; synchronous).
 int intception_b200_last_fp32_rejections(void) {
   Context* c = nullptr;
   if (get_context(&c)) return -1;
   if (!c->flags.p || c->flags_nq <= 0) return 0;
   IB_CUDA(cudaDeviceSynchronize());
-  // only the last mixed batch's flags: the buffer keeps stale entries past them
+  // only the last batch's flags: the buffer keeps stale entries past them
   const size_t n = std::min((size_t)c->flags_nq, c->flags.cap / sizeof(int));
   std::vector<int> h(n);
   IB_CUDA(cudaMemcpy(h.data(), c->flags.p, n * sizeof(int), cudaMemcpyDeviceToHost));
   int k = 0;
-  for (int v : h) k += v != 0;
+  for (int v : h) k += v & 1;
   return k;
+}
+
+// Number of quartets of the last batch (or drop-in call) that the class
+// kernels put on the redo list (HRR rounding-error estimate over the
+// tolerance) and the generic kernel recomputed (synchronous).
+int intception_b200_last_hrr_redo(void) {
+  Context* c = nullptr;
+  if (get_context(&c)) return -1;
+  if (!c->redo.p) return 0;
+  IB_CUDA(cudaDeviceSynchronize());
+  int h = 0;
+  IB_CUDA(cudaMemcpy(&h, c->redo.p, sizeof(int), cudaMemcpyDeviceToHost));
+  return h;
+}
+
+// Tolerance of the class kernels' HRR rounding-error estimate, in the output's
+// units (0 switches the check off).
+int intception_b200_set_hrr_tol(double tol) {
+  Context* c = nullptr;
+  int st = get_context(&c);
+  if (st) return st;
+  if (!(tol >= 0.0) || tol > 1e-6) return set_status(IB_ERR_ARG, "set_hrr_tol: tolerance outside [0, 1e-6]");
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->hrr_tol = tol;
+  return set_status(IB_OK, "");
 }
 
 // Cap on the lane groups that share one quartet in the class kernels, per

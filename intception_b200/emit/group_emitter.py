@@ -527,6 +527,47 @@ class GroupEmitter:
             parts.append('(1.0 + ib_amax3(g.CD[0], g.CD[1], g.CD[2]))')
         return ' * '.join(parts + ['(SPH ? %.17g : 1.0)' % sph])
 
+    def hrr_check(self, NE, NF, NFP):
+        """HRR rounding-error check on the contracted table sb0 ([e][f], rows
+        of levels la..la+lb, columns lc..lc+ld, pitch NFP): the element at
+        levels (la+k, lc+j) enters the outputs with coefficients of at most
+        C(lb,k) |AB|^(lb-k) C(ld,j) |CD|^(ld-j); the largest |element| x
+        weight, times IB_HRR_ERR_COEF, estimates the error."""
+        def weights(l0, l1, r):
+            # level boundaries of the rows (cumulative counts) and the weight of each level
+            bounds, n = [], 0
+            for k in range(l1 + 1):
+                n += (l0 + k + 1) * (l0 + k + 2) // 2
+                bounds.append(n)
+            w = []
+            for k in range(l1 + 1):
+                c = 1
+                for t in range(k):
+                    c = c * (l1 - t) // (t + 1)
+                w.append(' * '.join(['%d.0' % c] + [r] * (l1 - k)))
+            return bounds, w
+
+        def select(var, bounds, w):
+            e = w[-1]
+            for k in range(len(w) - 2, -1, -1):
+                e = '(%s < %d ? %s : %s)' % (var, bounds[k], w[k], e)
+            return e
+        bb, wb = weights(self.la, self.lb, 'rab')
+        bd, wd = weights(self.lc, self.ld, 'rcd')
+        out = ['    if (a.hrr_tol > 0.0) {',
+               '      const double rab = sqrt(g.AB[0] * g.AB[0] + g.AB[1] * g.AB[1] + g.AB[2] * g.AB[2]);',
+               '      const double rcd = sqrt(g.CD[0] * g.CD[0] + g.CD[1] * g.CD[1] + g.CD[2] * g.CD[2]);',
+               '      (void)rab; (void)rcd;',
+               '      double hm = 0.0;',
+               '      for (int x = r; x < %d; x += SG) {' % (NE * NF),
+               '        const int row = x / %d, col = x - row * %d;' % (NF, NF),
+               '        hm = fmax(hm, fabs(sb0[row * %d + col]) * %s * %s);' % (NFP, select('row', bb, wb),
+                                                                          select('col', bd, wd)),
+               '      }',
+               '      if (hm * IB_HRR_ERR_COEF > a.hrr_tol) ib_redo_push(a, p);',
+               '    }']
+        return out
+
     # -------------------------------------------------------------- kernel
     def kernel(self, fp32=True):
         """CUDA source of the class kernel and its launcher; fp32=False
@@ -653,7 +694,7 @@ class GroupEmitter:
         lane0 = '0' if self.wide else 'lane - r'
         grab = 'ib_grab(a.counter, beg, r, SG, sg, sgmask, %s, lcnt + 2)' % lane0
         src.append('  for (int p = %s; p < end; p = %s) {' % (grab, grab))
-        src.append('    if (sizeof(R) == 8 && a.recheck && !a.flags[p]) continue;  // uniform over the quartet\'s lanes')
+        src.append('    if (sizeof(R) == 8 && a.recheck && !(a.flags[p] & 1)) continue;  // uniform over the quartet\'s lanes')
         src.append('    IbQuartet g;')
         src.append('    ib_load_quartet(a, p, g);')
         src.append('    const int kb_ = g.k[1], kd_ = g.k[3];')
@@ -919,6 +960,13 @@ class GroupEmitter:
         src.append('      }')
         src.append('      ib_sg_sync(SG, sg, sgmask);')
         src.append('    }')
+        if self.lb or self.ld:
+            # the contracted table is complete: estimate the HRRs' rounding
+            # error from its largest element; a quartet over the tolerance is
+            # recomputed by the generic kernel, which builds each primitive
+            # pair on the shell that conditions its HRR (this kernel's result
+            # is written all the same and overwritten then)
+            src += self.hrr_check(NE, NF, NFP)
         src.append('    const double ABx = g.AB[0], ABy = g.AB[1], ABz = g.AB[2];')
         src.append('    const double CDx = g.CD[0], CDy = g.CD[1], CDz = g.CD[2];')
         src.append('    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;')

@@ -114,6 +114,10 @@ def load():
     lib.intception_b200_set_slice_cap.restype = C.c_int
     lib.intception_b200_set_prim_tol.argtypes = [C.c_double]
     lib.intception_b200_set_prim_tol.restype = C.c_int
+    lib.intception_b200_set_hrr_tol.argtypes = [C.c_double]
+    lib.intception_b200_set_hrr_tol.restype = C.c_int
+    lib.intception_b200_last_hrr_redo.argtypes = []
+    lib.intception_b200_last_hrr_redo.restype = C.c_int
     lib.intception_b200_set_class_minb.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.intception_b200_set_class_minb.restype = C.c_int
     lib.intception_b200_set_class_fp32.argtypes = [C.c_int, C.c_int]
@@ -166,6 +170,20 @@ def set_prim_tol(tol):
     skipped, so an element moves by at most Ka Kb Kc Kd * tol; 0 (default)
     skips only exact-zero prefactors.  The drop-ins never screen."""
     _check(load().intception_b200_set_prim_tol(float(tol)))
+
+
+def set_hrr_tol(tol):
+    """Tolerance of the class kernels' HRR rounding-error estimate (output
+    units; default 1e-13, 0 = no check): quartets over it are recomputed by
+    the generic kernel with every primitive pair built on the shell that
+    conditions its HRR."""
+    _check(load().intception_b200_set_hrr_tol(float(tol)))
+
+
+def last_hrr_redo():
+    """Quartets of the last batch the generic kernel recomputed for the HRR
+    check (waits for the device)."""
+    return load().intception_b200_last_hrr_redo()
 
 
 def set_class_minb(cls, variant, minb):

@@ -34,6 +34,26 @@
 #include "boys_tables.h"
 #include "pair_bound.h"
 
+/* Arithmetic of the recurrences, contraction, HRR and transform: double (the
+ * default, the restatement proper), or with -DORACLE_QUAD binary128 with an
+ * accurate binary128 Boys function (oracle/_gen/liberi_oracle_quad.so): an
+ * exact evaluation of the same integrals for quartets on which every double
+ * scheme loses digits (contractions that mix tight and diffuse exponents). */
+#ifdef ORACLE_QUAD
+#include <quadmath.h>
+typedef __float128 oreal;
+#define OR_EXP expq
+#define OR_SQRT sqrtq
+#define OR_POW powq
+#define OR_PI M_PIq
+#else
+typedef double oreal;
+#define OR_EXP exp
+#define OR_SQRT sqrt
+#define OR_POW pow
+#define OR_PI 3.14159265358979323846
+#endif
+
 #define OR_LMAX 8
 
 static const double oracle_oof[7] = {1.0, 1.0, 1.0 / 2.0, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
@@ -176,20 +196,48 @@ int oracle_eri_work_array_size(int la, int lb, int lc, int ld, int na_prim, int 
   return mem1;
 }
 
+/* F_0..F_nmax(x) in the recurrences' arithmetic: the reference's Boys function
+ * for double; for binary128 the series below x = 60 (positive terms, downward
+ * recursion) and erf-based F_0 with upward recursion from there. */
+#ifdef ORACLE_QUAD
+static void oracle_boys_real(oreal *f, int nmax, oreal x) {
+  oreal ex = expq(-x);
+  if (x < 60) {
+    oreal term = 1 / (oreal)(2 * nmax + 1), sum = term;
+    for (int k = 1; k < 100000; ++k) {
+      term *= 2 * x / (oreal)(2 * nmax + 2 * k + 1);
+      oreal next = sum + term;
+      if (next == sum) break;
+      sum = next;
+    }
+    f[nmax] = ex * sum;
+    for (int m = nmax - 1; m >= 0; --m) f[m] = (2 * x * f[m + 1] + ex) / (oreal)(2 * m + 1);
+  } else {
+    oreal g = 0.5Q * sqrtq(M_PIq / x) * erfq(sqrtq(x));
+    for (int m = 0; m <= nmax; ++m) {
+      f[m] = g;
+      g = ((oreal)m + 0.5Q) / x * g - 0.5Q * ex / x;
+    }
+  }
+}
+#else
+static void oracle_boys_real(oreal *f, int nmax, oreal x) { oracle_boys(f, 1, 0, nmax, x); }
+#endif
+
 /* One primitive quartet: V[m][a][c][d] over cumulative component indices, with
  * a <= la+lb, c <= lc, d <= ld and m + |a| + |c| + |d| <= L.  Recurrences are the
  * input script's vrra / vrrc / vrrd (Obara-Saika with the auxiliary index m). */
 typedef struct {
   int L, na, nc, nd; /* cumulative counts */
-  double *v;
+  oreal *v;
 } vtab;
 #define V(t, m, a, c, d) ((t)->v[(((size_t)(m) * (t)->na + (a)) * (t)->nc + (c)) * (t)->nd + (d)])
 
 static int first_dir(const int *e) { return e[0] > 0 ? 0 : (e[1] > 0 ? 1 : 2); }
 
-static void prim_vrr(vtab *t, int lab, int lc, int ld, const double *base, const double PA[3],
-                     const double WP[3], const double QC[3], const double QD[3], const double WQ[3],
-                     double o2z, double roz, double o2e, double roe, double o2zpe) {
+static void prim_vrr(vtab *t, int lab, int lc, int ld, const oreal *base, const oreal PA[3],
+                     const oreal WP[3], const oreal QC[3], const oreal QD[3], const oreal WQ[3],
+                     oreal o2z, oreal roz, oreal o2e, oreal roe, oreal o2zpe) {
   int L = t->L;
   for (int m = 0; m <= L; ++m) V(t, m, 0, 0, 0) = base[m];
   /* vrra: [a+1i| = PA_i [a| + WP_i [a|^(m+1) + a_i/(2zeta) ([a-1i| - rho/zeta [a-1i|^(m+1)) */
@@ -208,7 +256,7 @@ static void prim_vrr(vtab *t, int lab, int lc, int ld, const double *base, const
       a2 = cidx(e2[0], e2[1], e2[2]);
     }
     for (int m = 0; m + la_ <= L; ++m) {
-      double v = PA[i] * V(t, m, a1, 0, 0) + WP[i] * V(t, m + 1, a1, 0, 0);
+      oreal v = PA[i] * V(t, m, a1, 0, 0) + WP[i] * V(t, m + 1, a1, 0, 0);
       if (a2 >= 0) v += o2z * n2 * (V(t, m, a2, 0, 0) - roz * V(t, m + 1, a2, 0, 0));
       V(t, m, ia, 0, 0) = v;
     }
@@ -239,7 +287,7 @@ static void prim_vrr(vtab *t, int lab, int lc, int ld, const double *base, const
         a1 = cidx(em[0], em[1], em[2]);
       }
       for (int m = 0; m + le + lf <= L; ++m) {
-        double v = QC[i] * V(t, m, ia, c1, 0) + WQ[i] * V(t, m + 1, ia, c1, 0);
+        oreal v = QC[i] * V(t, m, ia, c1, 0) + WQ[i] * V(t, m + 1, ia, c1, 0);
         if (c2 >= 0) v += o2e * n2 * (V(t, m, ia, c2, 0) - roe * V(t, m + 1, ia, c2, 0));
         if (a1 >= 0) v += o2zpe * na_i * V(t, m + 1, a1, c1, 0);
         V(t, m, ia, ic, 0) = v;
@@ -281,7 +329,7 @@ static void prim_vrr(vtab *t, int lab, int lc, int ld, const double *base, const
           c1 = cidx(fm[0], fm[1], fm[2]);
         }
         for (int m = 0; m + le + lf + lg <= L; ++m) {
-          double v = QD[i] * V(t, m, ia, ic, d1) + WQ[i] * V(t, m + 1, ia, ic, d1);
+          oreal v = QD[i] * V(t, m, ia, ic, d1) + WQ[i] * V(t, m + 1, ia, ic, d1);
           if (d2 >= 0) v += o2e * n2 * (V(t, m, ia, ic, d2) - roe * V(t, m + 1, ia, ic, d2));
           if (c1 >= 0) v += o2e * nc_i * (V(t, m, ia, c1, d1) - roe * V(t, m + 1, ia, c1, d1));
           if (a1 >= 0) v += o2zpe * na_i * V(t, m + 1, a1, ic, d1);
@@ -304,7 +352,7 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
                             int nd_cont, int iskipd_cont, const double *cd, const double *Td,
                             double *out) {
   init_comp_tab();
-  const double two_pi52 = 2.0 * pow(3.14159265358979323846, 2.5);
+  const oreal two_pi52 = 2.0 * OR_POW(OR_PI, 2.5);
   int lab = la + lb, L = la + lb + lc + ld;
   int ne = ncum(lab) - ncum(la - 1); /* a range [la, la+lb] */
   int e0 = ncum(la - 1);
@@ -313,52 +361,52 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
   int ncont = na_cont * nb_cont * nc_cont * nd_cont;
   /* contracted [e0|cd]: index ((((ka*nbk+kb)*nck+kc)*ndk+kd)*ne + e)*ncc + c)*ncd + d */
   size_t nblk = (size_t)ne * ncc * ncd;
-  double *acc = calloc(nblk * ncont, sizeof(double));
+  oreal *acc = calloc(nblk * ncont, sizeof(oreal));
   vtab t;
   t.L = L;
   t.na = ncum(lab);
   t.nc = ncum(lc);
   t.nd = ncum(ld);
-  t.v = calloc((size_t)(L + 1) * t.na * t.nc * t.nd, sizeof(double));
-  double F[4 * OR_LMAX + 1];
-  double AB[3], CD[3];
+  t.v = calloc((size_t)(L + 1) * t.na * t.nc * t.nd, sizeof(oreal));
+  oreal F[4 * OR_LMAX + 1];
+  oreal AB[3], CD[3];
   for (int i = 0; i < 3; ++i) {
-    AB[i] = cA[i] - cB[i];
-    CD[i] = cC[i] - cD[i];
+    AB[i] = (oreal)cA[i] - cB[i];
+    CD[i] = (oreal)cC[i] - cD[i];
   }
-  double RAB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
-  double RCD2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+  oreal RAB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+  oreal RCD2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
   for (int pc = 0; pc < nc_prim; ++pc)
     for (int pd = 0; pd < nd_prim; ++pd) {
-      double eta = xc[pc] + xd[pd], oeta = 1.0 / eta;
-      double Q[3], QC[3], QD[3];
+      oreal eta = (oreal)xc[pc] + xd[pd], oeta = 1.0 / eta;
+      oreal Q[3], QC[3], QD[3];
       for (int i = 0; i < 3; ++i) {
-        Q[i] = (xc[pc] * cC[i] + xd[pd] * cD[i]) * oeta;
+        Q[i] = ((oreal)xc[pc] * cC[i] + (oreal)xd[pd] * cD[i]) * oeta;
         QC[i] = Q[i] - cC[i];
         QD[i] = Q[i] - cD[i];
       }
-      double xi_cd = xc[pc] * xd[pd] * oeta;
+      oreal xi_cd = (oreal)xc[pc] * xd[pd] * oeta;
       for (int pb = 0; pb < nb_prim; ++pb)
         for (int pa = 0; pa < na_prim; ++pa) {
-          double zeta = xa[pa] + xb[pb], ozeta = 1.0 / zeta;
-          double P[3], PA[3], W[3], WP[3], WQ[3], PQ[3];
+          oreal zeta = (oreal)xa[pa] + xb[pb], ozeta = 1.0 / zeta;
+          oreal P[3], PA[3], W[3], WP[3], WQ[3], PQ[3];
           for (int i = 0; i < 3; ++i) {
-            P[i] = (xa[pa] * cA[i] + xb[pb] * cB[i]) * ozeta;
+            P[i] = ((oreal)xa[pa] * cA[i] + (oreal)xb[pb] * cB[i]) * ozeta;
             PA[i] = P[i] - cA[i];
           }
-          double xi_ab = xa[pa] * xb[pb] * ozeta;
-          double ozpe = 1.0 / (zeta + eta);
-          double rho = zeta * eta * ozpe;
+          oreal xi_ab = (oreal)xa[pa] * xb[pb] * ozeta;
+          oreal ozpe = 1.0 / (zeta + eta);
+          oreal rho = zeta * eta * ozpe;
           for (int i = 0; i < 3; ++i) {
             PQ[i] = P[i] - Q[i];
             W[i] = (zeta * P[i] + eta * Q[i]) * ozpe;
             WP[i] = W[i] - P[i];
             WQ[i] = W[i] - Q[i];
           }
-          double RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+          oreal RPQ2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
           /* base: 2 pi^{5/2} / (zeta eta sqrt(zeta+eta)) exp(-xi_ab RAB2 - xi_cd RCD2) F_m(rho RPQ2) */
-          oracle_boys(F, 1, 0, L, rho * RPQ2);
-          double pref = two_pi52 * ozeta * oeta * sqrt(ozpe) * exp(-xi_ab * RAB2 - xi_cd * RCD2);
+          oracle_boys_real(F, L, rho * RPQ2);
+          oreal pref = two_pi52 * ozeta * oeta * OR_SQRT(ozpe) * OR_EXP(-xi_ab * RAB2 - xi_cd * RCD2);
           for (int m = 0; m <= L; ++m) F[m] *= pref;
           prim_vrr(&t, lab, lc, ld, F, PA, WP, QC, QD, WQ, 0.5 * ozeta, rho * ozeta, 0.5 * oeta, rho * oeta,
                    0.5 * ozpe);
@@ -366,9 +414,9 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
             for (int kb = 0; kb < nb_cont; ++kb)
               for (int kc = 0; kc < nc_cont; ++kc)
                 for (int kd = 0; kd < nd_cont; ++kd) {
-                  double w = ca[pa + ka * na_prim] * cb[pb + kb * nb_prim] * cc[pc + kc * nc_prim] *
+                  oreal w = (oreal)ca[pa + ka * na_prim] * cb[pb + kb * nb_prim] * cc[pc + kc * nc_prim] *
                              cd[pd + kd * nd_prim];
-                  double *blk = acc + ((((size_t)ka * nb_cont + kb) * nc_cont + kc) * nd_cont + kd) * nblk;
+                  oreal *blk = acc + ((((size_t)ka * nb_cont + kb) * nc_cont + kc) * nd_cont + kd) * nblk;
                   for (int e = 0; e < ne; ++e)
                     for (int c = 0; c < ncc; ++c)
                       for (int d = 0; d < ncd; ++d)
@@ -382,18 +430,18 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
    * direction = x if b_x>0, else y if b_y>0, else z. */
   int nca = nc_l(la), ncb = nc_l(lb);
   size_t nout_cart = (size_t)nca * ncb * ncc * ncd;
-  double *cart = malloc(sizeof(double) * nout_cart * ncont); /* index (((a*ncb+b)*ncc+c)*ncd+d) */
+  oreal *cart = malloc(sizeof(oreal) * nout_cart * ncont); /* index (((a*ncb+b)*ncc+c)*ncd+d) */
   for (int k = 0; k < ncont; ++k) {
-    const double *blk = acc + (size_t)k * nblk;
+    const oreal *blk = acc + (size_t)k * nblk;
     /* layer j holds (e, b) for |b| = j, e in [la, la+lb-j] (cumulative index offset e0) */
-    double *prev = malloc(sizeof(double) * nblk);
-    memcpy(prev, blk, sizeof(double) * nblk);
+    oreal *prev = malloc(sizeof(oreal) * nblk);
+    memcpy(prev, blk, sizeof(oreal) * nblk);
     int prev_ne = ne;
     for (int j = 1; j <= lb; ++j) {
       int cur_ne = ncum(lab - j) - ncum(la - 1);
       int nbj = nc_l(j), nbp = nc_l(j - 1);
       size_t cur_sz = (size_t)cur_ne * nbj * ncc * ncd;
-      double *cur = malloc(sizeof(double) * cur_sz);
+      oreal *cur = malloc(sizeof(oreal) * cur_sz);
       for (int ib = 0; ib < nbj; ++ib) {
         const int *bb = comp_tab[ncum(j - 1) + ib];
         int i = first_dir(bb);
@@ -417,7 +465,7 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
     }
     (void)prev_ne;
     /* prev now holds (a, b) with a in level la only (cur_ne == nca) */
-    memcpy(cart + (size_t)k * nout_cart, prev, sizeof(double) * nout_cart);
+    memcpy(cart + (size_t)k * nout_cart, prev, sizeof(oreal) * nout_cart);
     free(prev);
   }
   free(acc);
@@ -430,23 +478,23 @@ static void oracle_eri_cont(const double *xa, const double *cA, int la, int na, 
       for (int kc = 0; kc < nc_cont; ++kc)
         for (int kd = 0; kd < nd_cont; ++kd) {
           int k = ((ka * nb_cont + kb) * nc_cont + kc) * nd_cont + kd;
-          const double *X = cart + (size_t)k * nout_cart;
+          const oreal *X = cart + (size_t)k * nout_cart;
           for (int sa = 0; sa < oa; ++sa)
             for (int sb = 0; sb < ob; ++sb)
               for (int sc = 0; sc < oc; ++sc)
                 for (int sd = 0; sd < od; ++sd) {
-                  double s = 0.0;
+                  oreal s = 0.0;
                   for (int a = 0; a < nca; ++a) {
-                    double wa = Ta ? Ta[a + sa * nca] : (a == sa);
+                    oreal wa = Ta ? Ta[a + sa * nca] : (a == sa);
                     if (wa == 0.0) continue;
                     for (int b = 0; b < ncb; ++b) {
-                      double wb = Tb ? Tb[b + sb * ncb] : (b == sb);
+                      oreal wb = Tb ? Tb[b + sb * ncb] : (b == sb);
                       if (wb == 0.0) continue;
                       for (int c = 0; c < ncc; ++c) {
-                        double wc = Tc ? Tc[c + sc * ncc] : (c == sc);
+                        oreal wc = Tc ? Tc[c + sc * ncc] : (c == sc);
                         if (wc == 0.0) continue;
                         for (int d = 0; d < ncd; ++d) {
-                          double wd = Td ? Td[d + sd * ncd] : (d == sd);
+                          oreal wd = Td ? Td[d + sd * ncd] : (d == sd);
                           if (wd == 0.0) continue;
                           s += wa * wb * wc * wd * X[(((size_t)a * ncb + b) * ncc + c) * ncd + d];
                         }

@@ -178,6 +178,31 @@ def oracle_batch(b, sphT=None, exact_boys=False):
     return out
 
 
+_oracle_quad = None
+
+
+def oracle_batch_quad(b, sphT=None):
+    """Evaluate a ShellBatch with the C restatement computed in binary128
+    (eri_oracle.c built with ORACLE_QUAD, accurate Boys function): exact to
+    double precision even where double-precision recurrences cancel digits.
+    Slow (software binary128): for a few quartets."""
+    global _oracle_quad
+    if _oracle_quad is None:
+        so = os.path.join(os.path.dirname(_ORACLE_SO), 'liberi_oracle_quad.so')
+        if not os.path.exists(so):
+            subprocess.run(['make', '-s', '-C', HERE], check=True)
+        lib = C.CDLL(so)
+        lib.oracle_eri_batch.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, C.POINTER(_dp), _lp, _dp]
+        lib.oracle_eri_batch.restype = None
+        _oracle_quad = lib
+    q, sl, sk, sp, xyz, e, c, off = _batch_args(b)
+    out = np.zeros(b.out_size)
+    tab, keep = _sph_table(sphT) if b.spherical else (None, None)
+    _oracle_quad.oracle_eri_batch(b.nq, _ptr(q, _ip), _ptr(sl, _ip), _ptr(sk, _ip), _ptr(sp, _ip), _ptr(xyz),
+                                  _ptr(e), _ptr(c), tab, _ptr(off, _lp), _ptr(out))
+    return out
+
+
 def quartet_bounds(b):
     """The library's analytic screening bound of every quartet (pair_bound.h),
     with the C restatement."""

@@ -3,7 +3,9 @@
 Run in a container that has the reference tree (it builds oracle/_ref first):
     python oracle/gen_ref.py && python tests/golden/make_golden.py
 (``make_golden.py twoidx`` writes only twoidx.npz, ``make_golden.py c1`` only
-c1_pppp_k3_cart_4096.npz.)
+c1_pppp_k3_cart_4096.npz, ``make_golden.py mixed`` only
+mixed_contraction_sph.npz, whose ``out`` is exact (binary128) and whose
+``ref_out`` is the reference's.)
 
 Every fixture stores seeded inputs (shell table, quartets, spherical matrices)
 and the outputs of intception_integral_eri_abcd_m_cont_{cart,sph}_main as
@@ -233,12 +235,95 @@ def c1():
     save_batch('c1_pppp_k3_cart_4096.npz', b, T, ref(b, T))
 
 
+def pair_kappa(b, s0, s1, l_moved, build_first):
+    """Growth bound of a pair's HRR (the library's ib_hrr_kappa restated):
+    max over primitive pairs of ((sig + |PA| + R) / (sig + |PB|))^l_moved,
+    A the shell the recurrences build on."""
+    e = lambda s: b.prim_exp[b.shell_ptr[s]:b.shell_ptr[s] + b.shell_k[s]]  # noqa: E731
+    x0, x1 = (e(s0), e(s1)) if build_first else (e(s1), e(s0))
+    R = float(np.linalg.norm(b.shell_xyz[s0] - b.shell_xyz[s1]))
+    a, c = x0[:, None], x1[None, :]
+    z = a + c
+    sig = 1.0 / np.sqrt(z)
+    return float((((sig + c / z * R + R) / (sig + a / z * R)) ** l_moved).max())
+
+
+def compact_batch(picks):
+    """One ShellBatch (spherical) holding only the shells of the given
+    (batch, quartet index) picks, four fresh shells per quartet."""
+    ls, ks, xyz, ex, co = [], [], [], [], []
+    for b, q in picks:
+        for s in b.quartets[q]:
+            ls.append(b.shell_l[s])
+            ks.append(b.shell_k[s])
+            xyz.append(b.shell_xyz[s])
+            ex.append(b.prim_exp[b.shell_ptr[s]:b.shell_ptr[s] + b.shell_k[s]])
+            co.append(b.prim_coef[b.shell_ptr[s]:b.shell_ptr[s] + b.shell_k[s]])
+    ls, ks = np.array(ls, np.int32), np.array(ks, np.int32)
+    ptr = np.concatenate([[0], np.cumsum(ks)[:-1]]).astype(np.int32)
+    quart = np.arange(len(ls), dtype=np.int32).reshape(-1, 4)
+    off, size = basis.packed_offsets(ls, quart, True)
+    return basis.ShellBatch(ls, ks, ptr, np.array(xyz), np.concatenate(ex), np.concatenate(co), quart, off, True,
+                            size)
+
+
+def mixed():
+    """mixed_contraction_sph.npz: quartets of the l <= 4, K <= 8 workload
+    (exponents log-uniform in [0.02, 1e5], centres in a 10-bohr cube) with a
+    pair whose HRR growth bound exceeds 1e6 in both shell orders -- their
+    contractions mix tight and diffuse exponents on both shells -- plus the
+    (fg|gg) quartet 13409 of the 50000-quartet draw with seed 4.  out holds
+    exact values (the C restatement in binary128, oracle_batch_quad); ref_out
+    the reference's emitted C99 on the same quartets, whose own double
+    recurrences lose digits on some of them."""
+    T = basis.sph_matrices(6)
+    b = basis.independent_quartet_batch(4, 20000, [0, 1, 2, 3, 4], [1, 2, 3, 4, 5, 6, 7, 8], 0.02, 1.0e5, 10.0, True)
+    bnd = loader.quartet_bounds(b)
+    pick, total = [], 0
+    for q in range(b.nq):
+        if bnd[q] < 1e-12:
+            continue
+        s = b.quartets[q]
+        l = b.shell_l[s]
+        if np.prod(b.shell_k[s]) > 1500:  # keeps the binary128 evaluation to seconds per quartet
+            continue
+        hard = False
+        for i in (0, 2):
+            if min(l[i], l[i + 1]) == 0:
+                continue
+            k0 = pair_kappa(b, s[i], s[i + 1], l[i + 1], True)
+            k1 = pair_kappa(b, s[i], s[i + 1], l[i], False)
+            hard = hard or min(k0, k1) > 1e6
+        n = int(np.prod(2 * l + 1))
+        if hard and total + n <= 60000:
+            pick.append(q)
+            total += n
+        if len(pick) == 40:
+            break
+    big = basis.independent_quartet_batch(4, 50000, [0, 1, 2, 3, 4], [1, 2, 3, 4, 5, 6, 7, 8], 0.02, 1.0e5, 10.0,
+                                          True)
+    mb = compact_batch([(b, q) for q in pick] + [(big, 13409)])
+    from multiprocessing import Pool
+    with Pool(os.cpu_count() or 1) as p:
+        parts = p.map(_quad_one, [(mb, q, T) for q in range(mb.nq)], chunksize=1)
+    exact = np.concatenate(parts)
+    save_batch('mixed_contraction_sph', mb, T, exact, ref_out=ref(mb, T))
+
+
+def _quad_one(args):
+    b, q, T = args
+    return loader.oracle_batch_quad(b.subset(np.array([q])), T)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['twoidx']:
         twoidx()
     elif sys.argv[1:] == ['c1']:
         c1()
+    elif sys.argv[1:] == ['mixed']:
+        mixed()
     else:
         main()
         twoidx()
         c1()
+        mixed()

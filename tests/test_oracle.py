@@ -102,3 +102,31 @@ def test_oracle_vs_reference_live():
         b = basis.independent_quartet_batch(123, 50, [0, 1, 2, 3], [1, 2, 3], 0.1, 60.0, 5.0, sph)
         ref = loader.ref_batch(b, T)
         assert np.abs(loader.oracle_batch(b, T) - ref).max() <= tolerance(ref)
+
+
+def test_quad_oracle_matches_golden_where_double_is_exact():
+    """The binary128 build of the restatement (oracle_batch_quad) against the
+    reference's golden values on well-conditioned (pp|pp) quartets, where
+    double recurrences keep every digit: the two builds compute the same
+    integrals."""
+    b, T, ref = load_batch('pppp_k3_cart')
+    sub = b.subset(np.arange(12))
+    sizes = basis.block_sizes(b.shell_l, sub.quartets, False)
+    gather = np.concatenate([np.arange(o, o + n) for o, n in zip(b.out_off[:12], sizes)])
+    out = loader.oracle_batch_quad(sub, T)
+    assert np.abs(out - ref[gather]).max() <= 1e-14 * max(1.0, float(np.abs(ref).max()))
+
+
+def test_mixed_contraction_fixture_exact_values():
+    """The fixture's exact values re-evaluated (its smallest quartets), and
+    the reference's own error on its quartets, which the fixture records."""
+    b, T, exact = load_batch('mixed_contraction_sph')
+    sizes = basis.block_sizes(b.shell_l, b.quartets, True)
+    cost = [int(np.prod(b.shell_k[s])) for s in b.quartets]
+    for q in np.argsort(cost)[:3]:
+        out = loader.oracle_batch_quad(b.subset(np.array([q])), T)
+        assert np.array_equal(out, exact[b.out_off[q]:b.out_off[q] + sizes[q]])
+    ref = np.load(GOLDEN + '/mixed_contraction_sph.npz')['ref_out']
+    # the reference's double recurrences (bra HRR in the caller's shell order)
+    # miss the exact values by more than the parity bar on some of these quartets
+    assert np.abs(ref - exact).max() > tolerance(exact)
