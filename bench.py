@@ -260,11 +260,14 @@ def cpu_reference(batch, seconds, step_index=0, skip_below=SKIP_BELOW):
     return n2 / dt2, kind, used, '%d random quartets of the workload (uniform sample); %s' % (n2, what)
 
 
-def reference_error(batch, outs, nsample=20000, seed=123):
+def reference_error(batch, outs, nsample=20000, seed=123, exact_worst=0):
     """Max |GPU - reference C99| over a seeded sample of the batch's quartets:
     outs maps a path name to that path's device output for the whole batch.
     The reference evaluates every sampled quartet (no screening), so a
-    screened path's figure includes its screening error."""
+    screened path's figure includes its screening error.  exact_worst > 0:
+    the quartets with the largest differences (up to that many, K product
+    <= 2000) are also evaluated exactly (the oracle in binary128), and each
+    side's error against those values is reported."""
     from intception_b200 import basis
     from oracle import loader
     rng = np.random.default_rng(seed)
@@ -286,9 +289,14 @@ def reference_error(batch, outs, nsample=20000, seed=123):
     for w in np.argsort(-perq)[:5]:
         qq = batch.quartets[idx[w]]
         exps = [batch.prim_exp[batch.shell_ptr[s_]:batch.shell_ptr[s_] + batch.shell_k[s_]] for s_ in qq]
-        worst.append({'l': [int(batch.shell_l[s_]) for s_ in qq], 'k': [int(batch.shell_k[s_]) for s_ in qq],
-                      'exp_range': [[float(e.min()), float(e.max())] for e in exps],
-                      'err': float(perq[w]), 'max_abs': float(np.abs(ref[starts[w]:starts[w] + sizes[w]]).max())})
+        ent = {'l': [int(batch.shell_l[s_]) for s_ in qq], 'k': [int(batch.shell_k[s_]) for s_ in qq],
+               'exp_range': [[float(e.min()), float(e.max())] for e in exps],
+               'err': float(perq[w]), 'max_abs': float(np.abs(ref[starts[w]:starts[w] + sizes[w]]).max())}
+        if len(worst) < exact_worst and np.prod(ent['k']) <= 2000 and perq[w] > 1e-13:
+            ex = loader.oracle_batch_quad(batch.subset(idx[w:w + 1]), basis.sph_matrices(6))
+            ent['gpu_vs_exact'] = float(np.abs(outs[name0][gather][starts[w]:starts[w] + sizes[w]] - ex).max())
+            ent['reference_vs_exact'] = float(np.abs(ref[starts[w]:starts[w] + sizes[w]] - ex).max())
+        worst.append(ent)
     res['worst_quartets_' + name0] = worst
     res['sample'] = '%d seeded random quartets of this rank\'s batch vs the %s C99, unscreened' % (len(idx), kind)
     res['max_abs_reference'] = float(np.abs(ref).max())
@@ -458,7 +466,7 @@ def run_c5(args, rank, world, local):
     nprim = float((live_pairs(batch, 0, 1) * live_pairs(batch, 2, 3)).sum())
     cpu, ref_err = None, None
     if rank == 0:
-        ref_err = reference_error(batch, host, nsample=2000)
+        ref_err = reference_error(batch, host, nsample=2000, exact_worst=3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference(batch, args.cpu_seconds, skip_below=0.0)
         cpu = {'value': v, 'unit': 'quartets/s', 'cores': cores, 'kind': kind, 'sample': sample}
