@@ -81,10 +81,12 @@ def parse():
     ap.add_argument('--npairs', type=int, default=4_000_000)
     ap.add_argument('--nq-lattice', type=int, default=2_000_000)
     ap.add_argument('--nq-c5', type=int, default=50_000)
-    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim', 'class'],
+    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim', 'class',
+                                                     'c5classes'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time; fp64_cart '
                          'is the FP64 step with Cartesian output (no spherical transform); class runs one class '
-                         '(--cls) alone, FP64 then its FP32 kernel with every quartet in the FP32 tier')
+                         '(--cls) alone, FP64 then its FP32 kernel with every quartet in the FP32 tier; c5classes '
+                         'times each class of --cls (comma-separated) on the l <= 4 shell distribution')
     ap.add_argument('--cls', default='2222', help='--only class: the class as four digits la lb lc ld')
     return ap.parse_args()
 
@@ -758,6 +760,59 @@ def run_only(args, eng, out):
                       'kernels_per_step': eri.EriEngine.last_launch_count() + (1 if screened else 0)}), flush=True)
 
 
+def run_c5_classes(args):
+    """Per-class cost on the l <= 4 workload's shell distribution (K uniform
+    in 1..8, exponents log-uniform in [0.02, 1e5], centres in a 10-bohr
+    cube, spherical): each class of --cls (comma-separated la lb lc ld
+    digits) alone, --nq quartets, FP64, the HRR check on; ns per live
+    primitive quartet (c_a c_b exp(-xi R^2) != 0 on both pairs)."""
+    import torch
+    from intception_b200 import basis, eri
+    from intception_b200.emit.eri_emitter import emitted_classes
+
+    def canon(c):
+        p0, p1 = sorted(c[:2], reverse=True), sorted(c[2:], reverse=True)
+        key = lambda p: p[0] * (p[0] + 1) // 2 + p[1]  # noqa: E731
+        return tuple(p0 + p1) if key(p0) >= key(p1) else tuple(p1 + p0)
+    emitted = {c for c, _ in emitted_classes()}
+    rows = []
+    for tag in args.cls.split(','):
+        cls = tuple(int(ch) for ch in tag)
+        rng = np.random.default_rng(2000 + int(tag))
+        ls = np.tile(np.asarray(cls, np.int32), args.nq)
+        ks = rng.integers(1, 9, 4 * args.nq).astype(np.int32)
+        l, k, ptr, xyz, e, c = basis.make_shells(rng, ls, ks, 0.02, 1.0e5, 10.0)
+        q = np.arange(4 * args.nq, dtype=np.int32).reshape(args.nq, 4)
+        off, total = basis.packed_offsets(l, q, True)
+        b = basis.ShellBatch(l, k, ptr, xyz, e, c, q, off, True, total)
+        eng = eri.EriEngine(b)
+        out = torch.empty(b.out_size, dtype=torch.float64, device='cuda')
+
+        def timed():
+            for _ in range(args.warmup):
+                eng.compute(out=out)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                eng.compute(out=out)
+            e1.record()
+            torch.cuda.synchronize()
+            assert eng.device_status() == 0
+            return e0.elapsed_time(e1) / args.steps
+        ms = timed()
+        redo = eri.last_hrr_redo()
+        eri.set_hrr_tol(0.0)  # the class's own kernel alone: no quartet handed to the generic kernel
+        ms0 = timed()
+        eri.set_hrr_tol(HRR_TOL)
+        live = float((live_pairs(b, 0, 1) * live_pairs(b, 2, 3)).sum())
+        rows.append({'cls': tag, 'nq': args.nq, 'ms': ms, 'live_primitive_quartets': live,
+                     'ns_per_live_primitive_quartet': ms * 1e6 / live, 'hrr_redo': redo,
+                     'ms_without_hrr_check': ms0, 'ns_per_live_primitive_quartet_without_hrr_check': ms0 * 1e6 / live,
+                     'kernel': 'unrolled' if canon(cls) in emitted else 'generic'})
+        print(json.dumps(rows[-1]), flush=True)
+
+
 def run_one_class(args):
     """One class alone (--cls), --nq quartets with the headline distribution:
     W warm-up + K timed steps of the FP64 kernel, then of the class's FP32
@@ -796,6 +851,9 @@ def run_eri(args, rank, world, local):
     from intception_b200 import basis, eri, shard
     if args.only == 'class':
         run_one_class(args)
+        return
+    if args.only == 'c5classes':
+        run_c5_classes(args)
         return
     full = basis.config_mixed_l2(nq=args.nq, seed=1, spherical=args.only != 'fp64_cart')
     batch = full if world == 1 else shard.shard_for_rank(full, rank, world)[0]

@@ -302,7 +302,9 @@ int intception_b200_noalloc_status(void *stream);
  * 8-fold permutation families; blocks/out_off are their Cartesian ERI blocks
  * (a fastest); fofs[s] is the first Cartesian function of shell s; P the
  * symmetric nbf x nbf Cartesian density.  Adds E_J = 1/2 sum P_ij P_kl (ij|kl)
- * to e_out[0] and E_K = -1/4 sum P_ik P_jl (ij|kl) to e_out[1]. */
+ * to e_out[0] and E_K = -1/4 sum P_ik P_jl (ij|kl) to e_out[1], summed in
+ * double-double in a fixed order (the same bits on every run; allocates its
+ * block partials stream-ordered with cudaMallocAsync). */
 int intception_b200_jk_energy(const int *quartets, const long long *out_off, int nq, const int *shell_l,
                               const int *fofs, const double *P, int nbf, const double *blocks, double *e_out,
                               void *stream);
@@ -317,6 +319,18 @@ int intception_b200_jk_energy(const int *quartets, const long long *out_off, int
 int intception_b200_jk_force(const int *quartets, const int *qidx, const long long *aux_off, int naux, int pos,
                              int sign, const int *shell_l, const int *fofs, const int *shell_atom, const double *P,
                              int nbf, int natom, const double *blocks, double *force, void *stream);
+
+/* The same gradient from all six auxiliary batches of nq quartets in one pass:
+ * batch b = 2 pos + (sign < 0) has its blocks at aux_blocks[b] +
+ * aux_off[b][q] for quartet q (aux_off[b][q] = -1: no block, an l = 0 shell
+ * at pos for sign -1).  The host arrays aux_off[6] and aux_blocks[6] hold
+ * device pointers.  Each original element's density weight is formed once
+ * and applied to its raised and lowered partners of every centre and
+ * direction; the result equals the six intception_b200_jk_force calls. */
+int intception_b200_jk_force_all(const int *quartets, int nq, const long long *const *aux_off,
+                                 const double *const *aux_blocks, const int *shell_l, const int *fofs,
+                                 const int *shell_atom, const double *P, int nbf, int natom, double *force,
+                                 void *stream);
 
 /* Batched two-index primitive integrals (no counterpart in the reference,
  * which emits one call per pair): pair i of n has exponents xa[i], xb[i],

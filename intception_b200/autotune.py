@@ -1,7 +1,9 @@
 """Autotuner for the class kernels (run on the GPU the library will serve).
 
-For every canonical class with l <= 2 it builds a batch of quartets of that
-class with the headline workload's distribution (K uniform in 1..6 per shell,
+For every canonical class with l <= 2 (``--classes f``: every emitted class
+whose largest l is 3, FP64 variants only, merged into the existing file) it
+builds a batch of quartets of that class with the headline workload's
+distribution (K uniform in 1..6 per shell,
 exponents log-uniform [0.05, 1e4], centres in a 30-bohr cube, coefficients
 normalised), times the batch with each register budget the library was
 compiled with (``__launch_bounds__(IB_BLOCK, minb)``, minb in 1, 3, 4, 5 resident
@@ -73,17 +75,20 @@ def tune(nq=40000, reps=5, classes=None, log=print):
     from . import eri
     from .emit.eri_emitter import canonical_classes
     torch.cuda.set_device(0)
+    from .emit.eri_emitter import emitted_classes
     classes = classes or canonical_classes(2)
+    has_fp32 = {c for c, f in emitted_classes() if f}
     result = {}
     for cls in classes:
         tag = '%d%d%d%d' % tuple(cls)
         ent = {'minb': [0, 0, 0, 0], 'ms': {}}
+        precs = (eri.PREC_FP64, eri.PREC_MIXED) if tuple(cls) in has_fp32 else (eri.PREC_FP64,)
         for sph in (False, True):
             b = class_batch(cls, nq, seed=1000 + eri.class_id(*cls), spherical=sph)
             eng = eri.EriEngine(b)
             eng._tune_bounds = torch.ones(b.nq, dtype=torch.float64, device='cuda')
             out = torch.empty(b.out_size, dtype=torch.float64, device='cuda')
-            for prec in (eri.PREC_FP64, eri.PREC_MIXED):
+            for prec in precs:
                 v4 = (2 if prec == eri.PREC_MIXED else 0) + (1 if sph else 0)
                 times = []
                 for mi, mb in enumerate(MINB_VALUES):
@@ -95,8 +100,12 @@ def tune(nq=40000, reps=5, classes=None, log=print):
                 ent['ms'][VARIANTS[v4]] = [round(t, 4) for t in times]
             del eng, out
         # the FP32 tier uses this class's FP32 kernel only where it beats FP64
-        ent['fp32'] = bool(min(ent['ms']['fp32_sph']) < FP32_GAIN * min(ent['ms']['fp64_sph']) and
-                           min(ent['ms']['fp32_cart']) < FP32_GAIN * min(ent['ms']['fp64_cart']))
+        if len(precs) == 2:
+            ent['fp32'] = bool(min(ent['ms']['fp32_sph']) < FP32_GAIN * min(ent['ms']['fp64_sph']) and
+                               min(ent['ms']['fp32_cart']) < FP32_GAIN * min(ent['ms']['fp64_cart']))
+        else:  # FP64 kernels only: the FP32 slots take the FP64 choice
+            ent['minb'][2], ent['minb'][3] = ent['minb'][0], ent['minb'][1]
+            ent['fp32'] = False
         result[tag] = ent
         log('%s %s fp32:%s' % (tag, ' '.join('%s:%s' % (VARIANTS[v], MINB_VALUES[ent['minb'][v]]) for v in range(4)),
                                ent['fp32']))
@@ -140,6 +149,9 @@ def main():
     ap.add_argument('--nq', type=int, default=40000)
     ap.add_argument('--reps', type=int, default=5)
     ap.add_argument('--out', default=os.path.join(PKG, 'tuning.json'))
+    ap.add_argument('--classes', default='l2', choices=['l2', 'f'],
+                    help='l2: every class with l <= 2 (writes --out); f: the emitted classes whose largest l is 3, '
+                         'FP64 only, merged into --out')
     ap.add_argument('--merge', nargs='+', default=None,
                     help='combine tuning files of builds with different chain orders into --out (no GPU)')
     a = ap.parse_args()
@@ -149,6 +161,23 @@ def main():
         return
     import torch
     t0 = time.time()
+    if a.classes == 'f':
+        from .emit.eri_emitter import emitted_classes
+        # canonical orders only: a (d f| pair is canonicalised to (f d| by the batch
+        # entry, so its reversed class kernels (ill-conditioned pairs) keep the default
+        fcls = [c for c, _ in emitted_classes() if max(c) == 3 and c[0] >= c[1] and c[2] >= c[3]]
+        res = tune(a.nq, a.reps, classes=fcls)
+        with open(a.out) as fh:
+            cur = json.load(fh)
+        for tag, ent in res.items():
+            ent.setdefault('order', cur['classes'].get(tag, {}).get('order', 'dfs'))
+            cur['classes'][tag] = ent
+        cur['meta']['f_classes'] = {'nq_per_class': a.nq, 'reps': a.reps, 'seconds': round(time.time() - t0, 1),
+                                    'variants': 'FP64 Cartesian and spherical'}
+        with open(a.out, 'w') as fh:
+            json.dump(cur, fh, indent=1)
+        print('merged', len(res), 'f classes into', a.out)
+        return
     res = tune(a.nq, a.reps)
     meta = {'device': torch.cuda.get_device_name(0), 'nq_per_class': a.nq, 'reps': a.reps,
             'minb_values': list(MINB_VALUES), 'variants': list(VARIANTS),

@@ -28,6 +28,18 @@
 
 namespace {
 
+// Cartesian exponents of every cumulative component index below ncum(12)
+// (every index the kernel decodes: levels up to 2 IB_LMAX), 5 bits each,
+// filled once per block: the level loops read them instead of decoding.
+#define IB_GEN_NCT 455
+static_assert(IB_GEN_NCT == (2 * IB_LMAX + 1) * (2 * IB_LMAX + 2) * (2 * IB_LMAX + 3) / 6, "component table size");
+__device__ __forceinline__ void ib_ct_get(const unsigned short* ct, int cum, int& x, int& y, int& z) {
+  const unsigned v = ct[cum];
+  x = v & 31;
+  y = (v >> 5) & 31;
+  z = v >> 10;
+}
+
 __device__ __forceinline__ void ib_comp_of(int cum, int& x, int& y, int& z) {
   // level l with ncum(l-1) <= cum < ncum(l), then the in-level index k
   int l = 0;
@@ -74,6 +86,13 @@ struct IbGenShared {
 __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
                                                                double* __restrict__ scratch, long long slice) {
   __shared__ IbGenShared sh;
+  __shared__ unsigned short ct[IB_GEN_NCT];
+  for (int t = threadIdx.x; t < IB_GEN_NCT; t += blockDim.x) {
+    int x, y, z;
+    ib_comp_of(t, x, y, z);
+    ct[t] = (unsigned short)(x | (y << 5) | (z << 10));
+  }
+  __syncthreads();
   // range_slot < 0: the redo list (a.redo[0] items at a.redo + 1)
   const bool redo = range_slot < 0;
   const int beg = redo ? 0 : a.ranges[range_slot], end = redo ? a.redo[0] : a.ranges[range_slot + 1];
@@ -206,7 +225,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
         for (int idx = tid; idx < nce * nm; idx += nt) {
           const int m = idx / nce, e = ib_ncum(le - 1) + idx % nce;
           int ex, ey, ez;
-          ib_comp_of(e, ex, ey, ez);
+          ib_ct_get(ct, e, ex, ey, ez);
           int ev[3] = {ex, ey, ez};
           const int i = ev[0] > 0 ? 0 : (ev[1] > 0 ? 1 : 2);
           ev[i] -= 1;
@@ -233,7 +252,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
           const int rest = (int)(idx / d.ncumE);
           const int fc = rest % ncf, m = rest / ncf;
           int fx, fy, fz;
-          ib_comp_of(ib_ncum(lf - 1) + fc, fx, fy, fz);
+          ib_ct_get(ct, ib_ncum(lf - 1) + fc, fx, fy, fz);
           int fv[3] = {fx, fy, fz};
           const int i = fv[0] > 0 ? 0 : (fv[1] > 0 ? 1 : 2);
           fv[i] -= 1;
@@ -254,7 +273,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
                  (s2[((size_t)m * nc2 + f2) * d.ncumE + e] - sh.roe * s2[((size_t)(m + 1) * nc2 + f2) * d.ncumE + e]);
           }
           int ex, ey, ez;
-          ib_comp_of(e, ex, ey, ez);
+          ib_ct_get(ct, e, ex, ey, ez);
           int ev[3] = {ex, ey, ez};
           if (ev[i] > 0) {
             const int ne_i = ev[i];
@@ -283,13 +302,13 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
         const int f = idx % d.nf, rest = idx / d.nf;
         const int b = rest % ncb, e = rest / ncb;
         int bx, by, bz;
-        ib_comp_of(ib_ncum(j - 1) + b, bx, by, bz);
+        ib_ct_get(ct, ib_ncum(j - 1) + b, bx, by, bz);
         int bv[3] = {bx, by, bz};
         const int i = bv[0] > 0 ? 0 : (bv[1] > 0 ? 1 : 2);
         bv[i] -= 1;
         const int bm = ib_cidx(bv[0], bv[1], bv[2]) - ib_ncum(j - 2);
         int ex, ey, ez;
-        ib_comp_of(d.e0 + e, ex, ey, ez);
+        ib_ct_get(ct, d.e0 + e, ex, ey, ez);
         int ev[3] = {ex, ey, ez};
         ev[i] += 1;
         const int ep = ib_cidx(ev[0], ev[1], ev[2]) - d.e0;
@@ -309,13 +328,13 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
         const int dd = idx % ndj, rest = idx / ndj;
         const int c = rest % nc_j, ab = rest / nc_j;
         int dx, dy, dz;
-        ib_comp_of(ib_ncum(j - 1) + dd, dx, dy, dz);
+        ib_ct_get(ct, ib_ncum(j - 1) + dd, dx, dy, dz);
         int dv[3] = {dx, dy, dz};
         const int i = dv[0] > 0 ? 0 : (dv[1] > 0 ? 1 : 2);
         dv[i] -= 1;
         const int dm = ib_cidx(dv[0], dv[1], dv[2]) - ib_ncum(j - 2);
         int cx, cy, cz;
-        ib_comp_of(d.f0 + c, cx, cy, cz);
+        ib_ct_get(ct, d.f0 + c, cx, cy, cz);
         int cv[3] = {cx, cy, cz};
         cv[i] += 1;
         const int cp = ib_cidx(cv[0], cv[1], cv[2]) - d.f0;

@@ -18,6 +18,7 @@ __host__ __device__ inline int ib_sph_offset(int l) {
 struct IbGenericDims {
   int la, lb, lc, ld, L, E, F;
   int ncumE, e0, ne, f0, nf;
+  long long klev;  // doubles of the largest ket level; the ket levels roll through 3 slots of this size
   long long o_acc, o_bra, o_ket, o_h0, o_h1, total;
 };
 
@@ -27,7 +28,9 @@ __host__ __device__ inline long long ib_koff_raw(int F, int ncumE, int lf) {
   return o;
 }
 
-__host__ __device__ inline long long ib_koff(const IbGenericDims& d, int lf) { return ib_koff_raw(d.F, d.ncumE, lf); }
+// Ket level lf (>= 1) is built from levels lf-1 and lf-2 only, and the
+// contracted table takes its elements as it is built, so three slots suffice.
+__host__ __device__ inline long long ib_koff(const IbGenericDims& d, int lf) { return (long long)(lf % 3) * d.klev; }
 
 __host__ __device__ inline IbGenericDims ib_generic_dims(int la, int lb, int lc, int ld) {
   IbGenericDims d;
@@ -52,10 +55,15 @@ __host__ __device__ inline IbGenericDims ib_generic_dims(int la, int lb, int lc,
     if (v > hmax) hmax = v;
   }
   // spherical stages never exceed the Cartesian block
+  d.klev = 0;
+  for (int lf = 1; lf <= d.F; ++lf) {
+    const long long v = (long long)(d.F - lf + 1) * ib_ncart(lf) * d.ncumE;
+    if (v > d.klev) d.klev = v;
+  }
   d.o_acc = 0;
   d.o_bra = d.o_acc + (long long)d.ne * d.nf;
   d.o_ket = d.o_bra + (long long)(d.L + 2) * d.ncumE;
-  d.o_h0 = d.o_ket + ib_koff_raw(d.F, d.ncumE, d.F + 1);
+  d.o_h0 = d.o_ket + 3 * d.klev;
   d.o_h1 = d.o_h0 + hmax;
   d.total = d.o_h1 + hmax;
   return d;

@@ -48,15 +48,34 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// One warp per quartet; e_out[0] += E_J part, e_out[1] += E_K part.
+// Compensated (double-double) sums: the energy of a large system is a sum of
+// ~1e8 quartet terms, and a plain sum in an order that changes with the
+// quartet list (atomics, a geometry's screening) moves it by ~1e-13
+// relative -- enough to swamp a central difference with h = 1e-4.
+struct JkDD {
+  double hi, lo;
+};
+__device__ __forceinline__ JkDD jk_dd_add(JkDD a, double b) {  // Knuth's TwoSum
+  const double s = a.hi + b, bb = s - a.hi, e = (a.hi - (s - bb)) + (b - bb);
+  return {s, a.lo + e};
+}
+__device__ __forceinline__ JkDD jk_dd_add(JkDD a, JkDD b) {
+  JkDD r = jk_dd_add(a, b.hi);
+  r.lo += b.lo;
+  return r;
+}
+
+// One warp per quartet.  Block k writes its (E_J, E_K) partial sums, each a
+// double-double, to part[4k .. 4k+3]; ib_jk_energy_finish adds the partials in
+// block order into e_out.  The result does not depend on scheduling.
 __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long long* __restrict__ out_off, int nq,
                                     const int* __restrict__ shell_l, const int* __restrict__ fofs,
                                     const double* __restrict__ P, int nbf, const double* __restrict__ blocks,
-                                    double* __restrict__ e_out) {
-  __shared__ double red[2][32];
+                                    double* __restrict__ part) {
+  __shared__ JkDD red[2][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
-  double ej = 0.0, ek = 0.0;
+  JkDD ej = {0.0, 0.0}, ek = {0.0, 0.0};
   for (int q = warp; q < nq; q += nwarp) {
     int s[4], n[4], f[4];
     for (int i = 0; i < 4; ++i) {
@@ -78,25 +97,39 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
       pk += (__ldg(P + (size_t)i * nbf + k) * __ldg(P + (size_t)j * nbf + l) +
              __ldg(P + (size_t)i * nbf + l) * __ldg(P + (size_t)j * nbf + k)) * v;
     }
-    ej += 0.5 * deg * pj;
-    ek -= 0.125 * deg * pk;
+    // the warp's quartet term, summed over its lanes in a fixed order, then added compensated
+    pj = warp_sum(pj);
+    pk = warp_sum(pk);
+    ej = jk_dd_add(ej, 0.5 * deg * pj);
+    ek = jk_dd_add(ek, -0.125 * deg * pk);
   }
-  ej = warp_sum(ej);
-  ek = warp_sum(ek);
   if (lane == 0) {
     red[0][wib] = ej;
     red[1][wib] = ek;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
+    JkDD a = {0.0, 0.0}, b = {0.0, 0.0};
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      a += red[0][w];
-      b += red[1][w];
+      a = jk_dd_add(a, red[0][w]);
+      b = jk_dd_add(b, red[1][w]);
     }
-    atomicAdd(e_out, a);
-    atomicAdd(e_out + 1, b);
+    part[4 * blockIdx.x + 0] = a.hi;
+    part[4 * blockIdx.x + 1] = a.lo;
+    part[4 * blockIdx.x + 2] = b.hi;
+    part[4 * blockIdx.x + 3] = b.lo;
   }
+}
+
+// One thread: e_out[0..1] += the partials of nb blocks, in block order.
+__global__ void ib_jk_energy_finish(const double* __restrict__ part, int nb, double* __restrict__ e_out) {
+  JkDD a = {0.0, 0.0}, b = {0.0, 0.0};
+  for (int k = 0; k < nb; ++k) {
+    a = jk_dd_add(a, JkDD{part[4 * k], part[4 * k + 1]});
+    b = jk_dd_add(b, JkDD{part[4 * k + 2], part[4 * k + 3]});
+  }
+  e_out[0] += a.hi + a.lo;
+  e_out[1] += b.hi + b.lo;
 }
 
 // Gradient contribution of one auxiliary batch: centre `pos` (0..2) of each
@@ -219,6 +252,118 @@ __global__ void ib_jk_force_kernel(const int* __restrict__ quartets, const int* 
     if (fs[i] != 0.0) atomicAdd(force + i, fs[i]);
 }
 
+// All six auxiliary batches of a quartet list at once.  aux.off[b][q] locates
+// quartet q's block in aux.blk[b] (b = 2 pos + (sign < 0); -1: the quartet has
+// no block there, an l = 0 shell at pos for sign < 0).  The loop runs over the
+// quartet's ORIGINAL elements o: its density weight W(o) is formed once, and
+// for each centre pos and direction x
+//   dE/dA_pos,x += deg W(o) [(o + 1x | raised at pos) - o_x (o - 1x | lowered at pos)],
+// the adjoint of the derivative rule above; centre D takes the opposite sum.
+struct JkAux {
+  const long long* off[6];
+  const double* blk[6];
+};
+
+__global__ void ib_jk_force_all_kernel(const int* __restrict__ quartets, int nq, const JkAux aux,
+                                       const int* __restrict__ shell_l, const int* __restrict__ fofs,
+                                       const int* __restrict__ shell_atom, const double* __restrict__ P, int nbf,
+                                       int natom, double* __restrict__ force) {
+  extern __shared__ double fs[];
+  double* stage = fs + ((3 * natom + 1) & ~1);
+  for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x) fs[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* __restrict__ st = stage + (size_t)wib * 6 * JK_STAGE_N * JK_STAGE_N;
+  const int SS = JK_STAGE_N * JK_STAGE_N;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int q = warp; q < nq; q += nwarp) {
+    int s[4], l[4], n[4], f[4];
+    for (int i = 0; i < 4; ++i) {
+      s[i] = quartets[4 * q + i];
+      l[i] = shell_l[s[i]];
+      f[i] = fofs[s[i]];
+      n[i] = ib_ncart(l[i]);
+    }
+    long long off[6];
+    for (int b = 0; b < 6; ++b) off[b] = __ldg(aux.off[b] + q);
+    const double deg = jk_deg(s);
+    const int tot = n[0] * n[1] * n[2] * n[3];
+    const bool staged = max(max(l[0], l[1]), max(l[2], l[3])) <= JK_STAGE_L && tot >= 128;
+    if (staged) {
+      __syncwarp();
+      jk_stage(P, nbf, f[0], n[0], f[1], n[1], st + 0 * SS, lane);
+      jk_stage(P, nbf, f[2], n[2], f[3], n[3], st + 1 * SS, lane);
+      jk_stage(P, nbf, f[0], n[0], f[2], n[2], st + 2 * SS, lane);
+      jk_stage(P, nbf, f[1], n[1], f[3], n[3], st + 3 * SS, lane);
+      jk_stage(P, nbf, f[0], n[0], f[3], n[3], st + 4 * SS, lane);
+      jk_stage(P, nbf, f[1], n[1], f[2], n[2], st + 5 * SS, lane);
+      __syncwarp();
+    }
+    double g[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // [pos][x]
+    for (int e = lane; e < tot; e += 32) {
+      int idx[4];
+      int r = e;
+      for (int i = 0; i < 4; ++i) {
+        idx[i] = r % n[i];
+        r /= n[i];
+      }
+      double w;
+      if (staged) {
+        const int N = JK_STAGE_N;
+        w = 0.5 * st[0 * SS + idx[0] * N + idx[1]] * st[1 * SS + idx[2] * N + idx[3]] -
+            0.125 * (st[2 * SS + idx[0] * N + idx[2]] * st[3 * SS + idx[1] * N + idx[3]] +
+                     st[4 * SS + idx[0] * N + idx[3]] * st[5 * SS + idx[1] * N + idx[2]]);
+      } else {
+        w = jk_weight(P, nbf, f[0] + idx[0], f[1] + idx[1], f[2] + idx[2], f[3] + idx[3]);
+      }
+      w *= deg;
+      for (int pos = 0; pos < 3; ++pos) {
+        int cx, cy, cz;
+        jk_comp(l[pos], idx[pos], cx, cy, cz);
+        const int c[3] = {cx, cy, cz};
+        // flat index of the block with component k at pos and extent m there
+        int lo = 0, stride = 1;  // contribution of the indices before pos, stride of pos
+        for (int i = 0; i < pos; ++i) {
+          lo += idx[i] * stride;
+          stride *= n[i];
+        }
+        int hi = 0, hs = 1;  // indices after pos, in units of the stride after pos
+        for (int i = pos + 1; i < 4; ++i) {
+          hi += idx[i] * hs;
+          hs *= n[i];
+        }
+        const int np1 = ib_ncart(l[pos] + 1), nm1 = ib_ncart(l[pos] - 1);
+        const double* bp = aux.blk[2 * pos] + off[2 * pos];
+        const double* bm = off[2 * pos + 1] >= 0 ? aux.blk[2 * pos + 1] + off[2 * pos + 1] : nullptr;
+        for (int x = 0; x < 3; ++x) {
+          int o[3] = {c[0], c[1], c[2]};
+          o[x] += 1;
+          double v = __ldg(bp + lo + stride * (jk_index(o[0], o[1], o[2]) + np1 * hi));
+          if (c[x] > 0 && bm) {
+            o[x] -= 2;
+            v -= (double)c[x] * __ldg(bm + lo + stride * (jk_index(o[0], o[1], o[2]) + nm1 * hi));
+          }
+          g[3 * pos + x] += w * v;
+        }
+      }
+    }
+    for (int k = 0; k < 9; ++k) g[k] = warp_sum(g[k]);
+    if (lane == 0) {
+      const int ad = shell_atom[s[3]];
+      for (int pos = 0; pos < 3; ++pos) {
+        const int ax = shell_atom[s[pos]];
+        for (int x = 0; x < 3; ++x) {
+          atomicAdd(&fs[3 * ax + x], g[3 * pos + x]);
+          atomicAdd(&fs[3 * ad + x], -g[3 * pos + x]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x)
+    if (fs[i] != 0.0) atomicAdd(force + i, fs[i]);
+}
+
 }  // namespace
 
 extern "C" int intception_b200_jk_energy(const int* quartets, const long long* out_off, int nq, const int* shell_l,
@@ -233,9 +378,15 @@ extern "C" int intception_b200_jk_energy(const int* quartets, const long long* o
   const int threads = 256, wpb = threads / 32;
   int blocks_n = (nq + wpb - 1) / wpb;
   if (blocks_n > nsm * 16) blocks_n = nsm * 16;
-  ib_jk_energy_kernel<<<blocks_n, threads, 0, static_cast<cudaStream_t>(stream)>>>(quartets, out_off, nq, shell_l,
-                                                                                  fofs, P, nbf, blocks, e_out);
-  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* part = nullptr;  // stream-ordered: freed after the finishing kernel has read it
+  if (cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * 4 * (size_t)blocks_n, s) != cudaSuccess)
+    return IB_ERR_CUDA;
+  ib_jk_energy_kernel<<<blocks_n, threads, 0, s>>>(quartets, out_off, nq, shell_l, fofs, P, nbf, blocks, part);
+  ib_jk_energy_finish<<<1, 1, 0, s>>>(part, blocks_n, e_out);
+  const cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(part, s);
+  return e == cudaSuccess ? IB_OK : IB_ERR_CUDA;
 }
 
 extern "C" int intception_b200_jk_force(const int* quartets, const int* qidx, const long long* aux_off, int naux,
@@ -259,5 +410,35 @@ extern "C" int intception_b200_jk_force(const int* quartets, const int* qidx, co
   if (blocks_n > nsm * 8) blocks_n = nsm * 8;
   ib_jk_force_kernel<<<blocks_n, threads, smem, static_cast<cudaStream_t>(stream)>>>(
       quartets, qidx, aux_off, naux, pos, sign, shell_l, fofs, shell_atom, P, nbf, natom, blocks, force);
+  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+}
+
+extern "C" int intception_b200_jk_force_all(const int* quartets, int nq, const long long* const* aux_off,
+                                            const double* const* aux_blocks, const int* shell_l, const int* fofs,
+                                            const int* shell_atom, const double* P, int nbf, int natom,
+                                            double* force, void* stream) {
+  if (nq < 0 || natom < 1 || natom > 4096) return IB_ERR_ARG;
+  if (nq == 0) return IB_OK;
+  if (!quartets || !aux_off || !aux_blocks || !shell_l || !fofs || !shell_atom || !P || !force) return IB_ERR_ARG;
+  JkAux aux;
+  for (int b = 0; b < 6; ++b) {
+    if (!aux_off[b] || !aux_blocks[b]) return IB_ERR_ARG;
+    aux.off[b] = aux_off[b];
+    aux.blk[b] = aux_blocks[b];
+  }
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return IB_ERR_NODEVICE;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem =
+      sizeof(double) * (((3 * (size_t)natom + 1) & ~(size_t)1) + (size_t)JK_WARPS * 6 * JK_STAGE_N * JK_STAGE_N);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(ib_jk_force_all_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return IB_ERR_CUDA;
+  const int threads = 32 * JK_WARPS, wpb = JK_WARPS;
+  int blocks_n = (nq + wpb - 1) / wpb;
+  if (blocks_n > nsm * 8) blocks_n = nsm * 8;
+  ib_jk_force_all_kernel<<<blocks_n, threads, smem, static_cast<cudaStream_t>(stream)>>>(
+      quartets, nq, aux, shell_l, fofs, shell_atom, P, nbf, natom, force);
   return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
 }

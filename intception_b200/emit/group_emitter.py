@@ -120,7 +120,7 @@ class GroupEmitter:
         self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
         self.L = la + lb + lc + ld
         # every register budget is instantiated for the l <= 2 classes
-        self.tuned = max(la, lb, lc, ld) <= 2 if tuned is None else tuned
+        self.tuned = (max(la, lb, lc, ld) <= 3 and la >= lb) if tuned is None else tuned
         self.E, self.F = la + lb, lc + ld
         self.orient = orientation(la, lb, lc, ld)
         assert self.orient is not None

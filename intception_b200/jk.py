@@ -41,6 +41,10 @@ def _lib():
                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                                  C.c_void_p, C.c_void_p, C.c_void_p]
         lib.intception_b200_jk_force.restype = C.c_int
+        lib.intception_b200_jk_force_all.argtypes = [C.c_void_p, C.c_int, C.c_void_p * 6, C.c_void_p * 6,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                     C.c_int, C.c_void_p, C.c_void_p]
+        lib.intception_b200_jk_force_all.restype = C.c_int
         lib._jk_ready = True
     return lib
 
@@ -70,6 +74,9 @@ class JKSystem:
         # kernels (CUDA events around each; read with kernel_split())
         self.profile = False
         self._marks = []
+        # gradient digestion: False = one pass over the six auxiliary batches of
+        # a chunk (their blocks held together); True = one launch per batch
+        self.per_batch_digestion = False
         l = np.asarray(shell_l, np.int32)
         k = np.asarray(shell_k, np.int32)
         e = np.asarray(prim_exp, np.float64)
@@ -248,12 +255,43 @@ class JKSystem:
         return self._sum_over_ranks(force).view(self.natom, 3)
 
     def _force_chunk(self, qt, force):
-        """Adds the adjoint gradient of the unique quartets qt [n,4] to force."""
+        """Adds the adjoint gradient of the unique quartets qt [n,4] to force:
+        the six auxiliary batches (each centre raised and lowered), then one
+        digestion pass over them (intception_b200_jk_force_all)."""
         torch = self.torch
         lib = _lib()
         stream = C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
         lorig = self.shell_l[:self.ns]
         n = qt.shape[0]
+        if not self.per_batch_digestion:
+            m0 = self._mark()
+            offs, blks = [], []
+            for pos in range(3):
+                for sign in (1, -1):
+                    if sign > 0:
+                        sel = None
+                        aux = qt.clone()
+                    else:
+                        sel = torch.nonzero(lorig[qt[:, pos].long()] >= 1).flatten()
+                        aux = qt[sel].clone()
+                    aux[:, pos] += self.ns if sign > 0 else 2 * self.ns
+                    blocks, off = self._eri(aux.contiguous(), self.lmax + 1)
+                    if sel is not None:
+                        full = torch.full((n,), -1, dtype=torch.int64, device=self.dev)
+                        full[sel] = off
+                        off = full
+                    offs.append(off)
+                    blks.append(blocks)
+            m1 = self._mark()
+            eri._check(lib.intception_b200_jk_force_all(
+                qt.data_ptr(), n, (C.c_void_p * 6)(*[o.data_ptr() for o in offs]),
+                (C.c_void_p * 6)(*[b.data_ptr() for b in blks]), self.shell_l.data_ptr(), self.fofs.data_ptr(),
+                self.shell_atom.data_ptr(), self.P.data_ptr(), self.nbf_cart, self.natom, force.data_ptr(),
+                stream))
+            if m0 is not None:
+                self._marks.append((m0, m1, self._mark()))
+            return
+        # one digestion launch per auxiliary batch (intception_b200_jk_force)
         for pos in range(3):
             for sign in (1, -1):
                 if sign > 0:

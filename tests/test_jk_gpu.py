@@ -95,3 +95,30 @@ def test_jk_shards_add_up_on_one_gpu():
     for k in range(2):
         assert abs(es[0][k] + es[1][k] - e1[k]) <= 1e-12 * max(1.0, abs(e1[k]))
     assert np.abs(gs[0] + gs[1] - g1).max() <= 1e-12 * max(1.0, np.abs(g1).max())
+
+
+def test_jk_one_pass_digestion_equals_per_batch_launches():
+    """The one-pass gradient digestion over the six auxiliary batches
+    (intception_b200_jk_force_all, the default) against one launch per batch
+    (intception_b200_jk_force), on a system with f shells so that the
+    staged-density path and the gathering path both run."""
+    sys_, xyz = jk.lattice_system(natom=4, seed=11, shells=((0, 3), (1, 2), (2, 2), (3, 1)), alpha=(0.2, 30.0),
+                                  nocc=6, screen=1e-16)
+    g_all = sys_.gradient(xyz).cpu().numpy()
+    sys_.per_batch_digestion = True
+    g_per = sys_.gradient(xyz).cpu().numpy()
+    assert np.abs(g_all - g_per).max() <= 1e-12 * max(1.0, np.abs(g_per).max())
+    assert np.abs(g_per).max() > 1e-4
+
+
+def test_jk_energy_independent_of_chunking():
+    """The energy sums are compensated and fixed-order: chunks of 97 quartets
+    and one chunk give the same energies to 1e-15 relative (plain sums in a
+    changing order move them by ~1e-13, which a central difference with
+    h = 1e-4 would turn into a 1e-7 gradient error)."""
+    sys_, xyz = small_system()
+    e1 = sys_.energy(xyz)
+    sys_.chunk = 97
+    e2 = sys_.energy(xyz)
+    for a, b in zip(e1, e2):
+        assert abs(a - b) <= 1e-15 * abs(a)
