@@ -97,11 +97,14 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
       pk += (__ldg(P + (size_t)i * nbf + k) * __ldg(P + (size_t)j * nbf + l) +
              __ldg(P + (size_t)i * nbf + l) * __ldg(P + (size_t)j * nbf + k)) * v;
     }
-    // the warp's quartet term, summed over its lanes in a fixed order, then added compensated
-    pj = warp_sum(pj);
-    pk = warp_sum(pk);
+    // each lane's share of the quartet term, added compensated to the lane's sums
     ej = jk_dd_add(ej, 0.5 * deg * pj);
     ek = jk_dd_add(ek, -0.125 * deg * pk);
+  }
+  // the lanes' double-double sums over the warp, in a fixed shuffle order
+  for (int o = 16; o > 0; o >>= 1) {
+    ej = jk_dd_add(ej, JkDD{__shfl_xor_sync(0xffffffffu, ej.hi, o), __shfl_xor_sync(0xffffffffu, ej.lo, o)});
+    ek = jk_dd_add(ek, JkDD{__shfl_xor_sync(0xffffffffu, ek.hi, o), __shfl_xor_sync(0xffffffffu, ek.lo, o)});
   }
   if (lane == 0) {
     red[0][wib] = ej;

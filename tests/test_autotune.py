@@ -35,6 +35,9 @@ def test_committed_tuning_covers_every_tuned_class():
     with open(path) as fh:
         tun = json.load(fh)['classes']
     tags = {'%d%d%d%d' % c for c in eri_emitter.canonical_classes(2)}
+    # and the emitted f classes in canonical order (autotune --classes f)
+    tags |= {'%d%d%d%d' % c for c, _ in eri_emitter.emitted_classes()
+             if max(c) == 3 and c[0] >= c[1] and c[2] >= c[3]}
     assert tags == set(tun)
     for ent in tun.values():
         assert len(ent['minb']) == 4 and all(0 <= m < len(autotune.MINB_VALUES) for m in ent['minb'])
