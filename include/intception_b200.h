@@ -303,8 +303,9 @@ int intception_b200_noalloc_status(void *stream);
  * (a fastest); fofs[s] is the first Cartesian function of shell s; P the
  * symmetric nbf x nbf Cartesian density.  Adds E_J = 1/2 sum P_ij P_kl (ij|kl)
  * to e_out[0] and E_K = -1/4 sum P_ik P_jl (ij|kl) to e_out[1], summed in
- * double-double in a fixed order (the same bits on every run; allocates its
- * block partials stream-ordered with cudaMallocAsync). */
+ * double-double in a fixed order (the same bits on every run).  Its block
+ * partials live in a file-scope device array: calls on one device must be
+ * ordered (one stream, or events between streams). */
 int intception_b200_jk_energy(const int *quartets, const long long *out_off, int nq, const int *shell_l,
                               const int *fofs, const double *P, int nbf, const double *blocks, double *e_out,
                               void *stream);

@@ -87,12 +87,26 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
                                                                double* __restrict__ scratch, long long slice) {
   __shared__ IbGenShared sh;
   __shared__ unsigned short ct[IB_GEN_NCT];
+  // em[i][e]: the index of e - 1_i (low 9 bits) and the exponent of e along i
+  // (above them; 0: no such component)
+  __shared__ unsigned short em[3 * IB_GEN_NCT];
   for (int t = threadIdx.x; t < IB_GEN_NCT; t += blockDim.x) {
     int x, y, z;
     ib_comp_of(t, x, y, z);
     ct[t] = (unsigned short)(x | (y << 5) | (z << 10));
+    const int c[3] = {x, y, z};
+    for (int i = 0; i < 3; ++i) {
+      if (c[i] == 0) {
+        em[i * IB_GEN_NCT + t] = 0;
+        continue;
+      }
+      int v[3] = {x, y, z};
+      v[i] -= 1;
+      em[i * IB_GEN_NCT + t] = (unsigned short)(ib_cidx(v[0], v[1], v[2]) | (c[i] << 9));
+    }
   }
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   // range_slot < 0: the redo list (a.redo[0] items at a.redo + 1)
   const bool redo = range_slot < 0;
   const int beg = redo ? 0 : a.ranges[range_slot], end = redo ? a.redo[0] : a.ranges[range_slot + 1];
@@ -241,49 +255,47 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
           if (m == 0 && d.lc == 0 && e >= d.e0) acc[(e - d.e0) * d.nf] += v;
         }
       }
-      // ---- ket VRR: level f stored at ket + koff(f) as [m][fcomp][e]
+      // ---- ket VRR: level f stored at ket + koff(f) as [m][fcomp][e].  One warp per
+      // row (m, fcomp): the f-side indices once per row; its lanes run over e, with
+      // e - 1_i and the exponent of e along i from the table em
       for (int lf = 1; lf <= d.F; ++lf) {
         __syncthreads();
-        const int ncf = ib_ncart(lf), nm = d.F - lf + 1;
-        const long long n = (long long)nm * ncf * d.ncumE;
+        const int ncf = ib_ncart(lf), nm = d.F - lf + 1, E_ = d.ncumE;
         double* dst = ket + ib_koff(d, lf);
-        for (long long idx = tid; idx < n; idx += nt) {
-          const int e = (int)(idx % d.ncumE);
-          const int rest = (int)(idx / d.ncumE);
-          const int fc = rest % ncf, m = rest / ncf;
+        const double* s1 = lf == 1 ? bra : ket + ib_koff(d, lf - 1);
+        const double* s2 = lf <= 2 ? bra : ket + ib_koff(d, lf - 2);  // read only when lf >= 2
+        const int nc1 = ib_ncart(lf - 1), nc2 = ib_ncart(lf - 2);
+        for (int row = warp; row < nm * ncf; row += nwarp) {
+          const int m = row / ncf, fc = row - m * ncf;
           int fx, fy, fz;
           ib_ct_get(ct, ib_ncum(lf - 1) + fc, fx, fy, fz);
           int fv[3] = {fx, fy, fz};
           const int i = fv[0] > 0 ? 0 : (fv[1] > 0 ? 1 : 2);
+          const int nn = fv[i] - 1;  // exponent of f - 1_i along i
           fv[i] -= 1;
           const int f1 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 2);  // in-level index at lf-1
-          // level lf-1 accessor
-          const double* s1 = lf == 1 ? bra : ket + ib_koff(d, lf - 1);
-          const int nc1 = ib_ncart(lf - 1);
-          double v = sh.QC[i] * s1[((size_t)m * nc1 + f1) * d.ncumE + e] +
-                     sh.WQ[i] * s1[((size_t)(m + 1) * nc1 + f1) * d.ncumE + e];
-          if (fv[i] > 0) {
-            const int nn = fv[i];
+          int f2 = 0;
+          if (nn > 0) {
             fv[i] -= 1;
-            const int f2 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 3);
-            fv[i] += 1;
-            const double* s2 = lf == 2 ? bra : ket + ib_koff(d, lf - 2);
-            const int nc2 = ib_ncart(lf - 2);
-            v += nn * sh.o2e *
-                 (s2[((size_t)m * nc2 + f2) * d.ncumE + e] - sh.roe * s2[((size_t)(m + 1) * nc2 + f2) * d.ncumE + e]);
+            f2 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 3);
           }
-          int ex, ey, ez;
-          ib_ct_get(ct, e, ex, ey, ez);
-          int ev[3] = {ex, ey, ez};
-          if (ev[i] > 0) {
-            const int ne_i = ev[i];
-            ev[i] -= 1;
-            const int e1 = ib_cidx(ev[0], ev[1], ev[2]);
-            v += ne_i * sh.o2zpe * s1[((size_t)(m + 1) * nc1 + f1) * d.ncumE + e1];
+          const double qc = sh.QC[i], wq = sh.WQ[i], t2 = nn * sh.o2e, roe = sh.roe, o2zpe = sh.o2zpe;
+          const double* __restrict__ r10 = s1 + ((size_t)m * nc1 + f1) * E_;
+          const double* __restrict__ r11 = s1 + ((size_t)(m + 1) * nc1 + f1) * E_;
+          const double* __restrict__ r20 = s2 + ((size_t)m * nc2 + f2) * E_;
+          const double* __restrict__ r21 = s2 + ((size_t)(m + 1) * nc2 + f2) * E_;
+          double* __restrict__ out = dst + ((size_t)m * ncf + fc) * E_;
+          const unsigned short* emi = em + i * IB_GEN_NCT;
+          const bool to_acc = m == 0 && lf >= d.lc;
+          double* accc = acc + (ib_ncum(lf - 1) + fc - d.f0);  // this f's column of [e0|f0]
+          for (int e = lane; e < E_; e += 32) {
+            double v = qc * r10[e] + wq * r11[e];
+            if (nn > 0) v += t2 * (r20[e] - roe * r21[e]);
+            const unsigned t = emi[e];
+            if (t >> 9) v += (double)(t >> 9) * o2zpe * r11[t & 511];
+            out[e] = v;
+            if (to_acc && e >= d.e0) accc[(size_t)(e - d.e0) * d.nf] += v;
           }
-          dst[((size_t)m * ncf + fc) * d.ncumE + e] = v;
-          if (m == 0 && lf >= d.lc && e >= d.e0)
-            acc[(e - d.e0) * d.nf + (ib_ncum(lf - 1) + fc - d.f0)] += v;
         }
       }
     }

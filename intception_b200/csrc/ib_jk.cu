@@ -52,6 +52,11 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ~1e8 quartet terms, and a plain sum in an order that changes with the
 // quartet list (atomics, a geometry's screening) moves it by ~1e-13
 // relative -- enough to swamp a central difference with h = 1e-4.
+// Block partials of the energy kernel (4 doubles per block), one array per
+// device: calls on one device run in stream order (JKSystem uses one stream).
+#define JK_MAX_PART_BLOCKS 4096
+__device__ double ib_jk_part[4 * JK_MAX_PART_BLOCKS];
+
 struct JkDD {
   double hi, lo;
 };
@@ -65,9 +70,11 @@ __device__ __forceinline__ JkDD jk_dd_add(JkDD a, JkDD b) {
   return r;
 }
 
-// One warp per quartet.  Block k writes its (E_J, E_K) partial sums, each a
-// double-double, to part[4k .. 4k+3]; ib_jk_energy_finish adds the partials in
-// block order into e_out.  The result does not depend on scheduling.
+// One warp per quartet.  Each lane sums its shares in plain double (a few
+// hundred terms, a fixed order), the warp, block and grid sums are
+// double-double: block k writes its (E_J, E_K) partials to part[4k .. 4k+3]
+// and ib_jk_energy_finish adds them in block order into e_out.  The result
+// does not depend on scheduling.
 __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long long* __restrict__ out_off, int nq,
                                     const int* __restrict__ shell_l, const int* __restrict__ fofs,
                                     const double* __restrict__ P, int nbf, const double* __restrict__ blocks,
@@ -75,7 +82,7 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
   __shared__ JkDD red[2][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarp = (gridDim.x * blockDim.x) >> 5;
-  JkDD ej = {0.0, 0.0}, ek = {0.0, 0.0};
+  double sj = 0.0, sk = 0.0;  // this lane's plain sums: a few hundred terms in a fixed order
   for (int q = warp; q < nq; q += nwarp) {
     int s[4], n[4], f[4];
     for (int i = 0; i < 4; ++i) {
@@ -97,11 +104,11 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
       pk += (__ldg(P + (size_t)i * nbf + k) * __ldg(P + (size_t)j * nbf + l) +
              __ldg(P + (size_t)i * nbf + l) * __ldg(P + (size_t)j * nbf + k)) * v;
     }
-    // each lane's share of the quartet term, added compensated to the lane's sums
-    ej = jk_dd_add(ej, 0.5 * deg * pj);
-    ek = jk_dd_add(ek, -0.125 * deg * pk);
+    sj += 0.5 * deg * pj;
+    sk -= 0.125 * deg * pk;
   }
-  // the lanes' double-double sums over the warp, in a fixed shuffle order
+  // the lanes' sums over the warp in double-double, in a fixed shuffle order
+  JkDD ej = {sj, 0.0}, ek = {sk, 0.0};
   for (int o = 16; o > 0; o >>= 1) {
     ej = jk_dd_add(ej, JkDD{__shfl_xor_sync(0xffffffffu, ej.hi, o), __shfl_xor_sync(0xffffffffu, ej.lo, o)});
     ek = jk_dd_add(ek, JkDD{__shfl_xor_sync(0xffffffffu, ek.hi, o), __shfl_xor_sync(0xffffffffu, ek.lo, o)});
@@ -124,15 +131,23 @@ __global__ void ib_jk_energy_kernel(const int* __restrict__ quartets, const long
   }
 }
 
-// One thread: e_out[0..1] += the partials of nb blocks, in block order.
+// One warp: e_out[0..1] += the partials of nb blocks (lane t takes blocks t,
+// t + 32, ..., then the lanes' sums meet in a fixed shuffle order).
 __global__ void ib_jk_energy_finish(const double* __restrict__ part, int nb, double* __restrict__ e_out) {
+  const int lane = threadIdx.x;
   JkDD a = {0.0, 0.0}, b = {0.0, 0.0};
-  for (int k = 0; k < nb; ++k) {
+  for (int k = lane; k < nb; k += 32) {
     a = jk_dd_add(a, JkDD{part[4 * k], part[4 * k + 1]});
     b = jk_dd_add(b, JkDD{part[4 * k + 2], part[4 * k + 3]});
   }
-  e_out[0] += a.hi + a.lo;
-  e_out[1] += b.hi + b.lo;
+  for (int o = 16; o > 0; o >>= 1) {
+    a = jk_dd_add(a, JkDD{__shfl_xor_sync(0xffffffffu, a.hi, o), __shfl_xor_sync(0xffffffffu, a.lo, o)});
+    b = jk_dd_add(b, JkDD{__shfl_xor_sync(0xffffffffu, b.hi, o), __shfl_xor_sync(0xffffffffu, b.lo, o)});
+  }
+  if (lane == 0) {
+    e_out[0] += a.hi + a.lo;
+    e_out[1] += b.hi + b.lo;
+  }
 }
 
 // Gradient contribution of one auxiliary batch: centre `pos` (0..2) of each
@@ -381,15 +396,13 @@ extern "C" int intception_b200_jk_energy(const int* quartets, const long long* o
   const int threads = 256, wpb = threads / 32;
   int blocks_n = (nq + wpb - 1) / wpb;
   if (blocks_n > nsm * 16) blocks_n = nsm * 16;
+  if (blocks_n > JK_MAX_PART_BLOCKS) blocks_n = JK_MAX_PART_BLOCKS;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  double* part = nullptr;  // stream-ordered: freed after the finishing kernel has read it
-  if (cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * 4 * (size_t)blocks_n, s) != cudaSuccess)
-    return IB_ERR_CUDA;
+  double* part = nullptr;  // this device's copy of the file-scope partials array
+  if (cudaGetSymbolAddress(reinterpret_cast<void**>(&part), ib_jk_part) != cudaSuccess) return IB_ERR_CUDA;
   ib_jk_energy_kernel<<<blocks_n, threads, 0, s>>>(quartets, out_off, nq, shell_l, fofs, P, nbf, blocks, part);
-  ib_jk_energy_finish<<<1, 1, 0, s>>>(part, blocks_n, e_out);
-  const cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(part, s);
-  return e == cudaSuccess ? IB_OK : IB_ERR_CUDA;
+  ib_jk_energy_finish<<<1, 32, 0, s>>>(part, blocks_n, e_out);
+  return cudaGetLastError() == cudaSuccess ? IB_OK : IB_ERR_CUDA;
 }
 
 extern "C" int intception_b200_jk_force(const int* quartets, const int* qidx, const long long* aux_off, int naux,
