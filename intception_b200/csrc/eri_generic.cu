@@ -19,9 +19,9 @@
 // pass stores the block and the others add to it.
 //
 // Scratch slice layout (doubles), sizes from ib_generic_dims():
-//   acc  [ne * nf]                 contracted [e0|f0], e in [la,la+lb], f in [lc,lc+ld]
-//   bra  [(L+1) * ncumE]           [e0|00]^(m) over every e <= la+lb
-//   ket  sum_f (F-f+1)*ncart(f)*ncumE   [e0|f0]^(m) for each ket level f >= 1
+//   acc  [nf * ne]                 contracted [e0|f0] stored [f][e], e in [la,la+lb], f in [lc,lc+ld]
+//   bra  [(L+2) * ncumE]           [e0|00]^(m) over every e <= la+lb
+//   ket  3 * klev                  [e0|f0]^(m) of the ket levels f >= 1, level f in slot f mod 3
 //   h0,h1 [hmax] ping-pong buffers for HRR and the spherical transform
 #include "ib_eri_device.cuh"
 #include "ib_generic.cuh"
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
             v += n * sh.o2z * (bra[m * d.ncumE + e2] - sh.roz * bra[(m + 1) * d.ncumE + e2]);
           }
           bra[m * d.ncumE + e] = v;
-          if (m == 0 && d.lc == 0 && e >= d.e0) acc[(e - d.e0) * d.nf] += v;
+          if (m == 0 && d.lc == 0 && e >= d.e0) acc[e - d.e0] += v;  // f = 0 column of [f][e]
         }
       }
       // ---- ket VRR: level f stored at ket + koff(f) as [m][fcomp][e].  One warp per
@@ -287,23 +287,31 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
           double* __restrict__ out = dst + ((size_t)m * ncf + fc) * E_;
           const unsigned short* emi = em + i * IB_GEN_NCT;
           const bool to_acc = m == 0 && lf >= d.lc;
-          double* accc = acc + (ib_ncum(lf - 1) + fc - d.f0);  // this f's column of [e0|f0]
+          double* accc = acc + (size_t)(ib_ncum(lf - 1) + fc - d.f0) * d.ne;  // this f's row of [f][e]
           for (int e = lane; e < E_; e += 32) {
             double v = qc * r10[e] + wq * r11[e];
             if (nn > 0) v += t2 * (r20[e] - roe * r21[e]);
             const unsigned t = emi[e];
             if (t >> 9) v += (double)(t >> 9) * o2zpe * r11[t & 511];
             out[e] = v;
-            if (to_acc && e >= d.e0) accc[(size_t)(e - d.e0) * d.nf] += v;
+            if (to_acc && e >= d.e0) accc[e - d.e0] += v;
           }
         }
       }
     }
     __syncthreads();
     // ---- bra HRR: [e][b][f] layers, (a, b+1i) = (a+1i, b) + AB_i (a, b)
-    double* src = acc;
+    // the contracted table was accumulated as [f][e] (the lanes' e contiguous);
+    // the HRRs read [e][f]: transpose it into h1 (the bra HRR's first layer
+    // writes h0, every later stage alternates)
     double* h0 = w + d.o_h0;
     double* h1 = w + d.o_h1;
+    for (int x = tid; x < d.ne * d.nf; x += nt) {
+      const int e = x / d.nf, f = x - e * d.nf;
+      h1[x] = acc[(size_t)f * d.ne + e];
+    }
+    __syncthreads();
+    double* src = h1;
     for (int j = 1; j <= d.lb; ++j) {
       double* dst = (j & 1) ? h0 : h1;
       const int ne_j = ib_ncum(d.E - j) - d.e0, ne_p = ib_ncum(d.E - j + 1) - d.e0;
