@@ -81,8 +81,8 @@ def parse():
     ap.add_argument('--npairs', type=int, default=4_000_000)
     ap.add_argument('--nq-lattice', type=int, default=2_000_000)
     ap.add_argument('--nq-c5', type=int, default=50_000)
-    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim', 'class',
-                                                     'c5classes'],
+    ap.add_argument('--only', default=None, choices=['fp64', 'fp64_cart', 'screened', 'screened_prim', 'bounds',
+                                                     'class', 'c5classes'],
                     help='profiling: run only this ERI step (W warm-up + K timed) and print its time; fp64_cart '
                          'is the FP64 step with Cartesian output (no spherical transform); class runs one class '
                          '(--cls) alone, FP64 then its FP32 kernel with every quartet in the FP32 tier; c5classes '
@@ -732,17 +732,19 @@ def run_twoidx(args, rank, world, local):
 
 def run_only(args, eng, out):
     """One step kind alone (for profilers): the FP64 step over every quartet,
-    or the screened FP64 step (analytic bounds inside the step)."""
+    the screened FP64 step (analytic bounds inside the step), or the
+    analytic-bound kernel alone (bounds)."""
     import torch
     from intception_b200 import eri
-    screened = args.only in ('screened', 'screened_prim')
+    screened = args.only in ('screened', 'screened_prim', 'bounds')
     bounds = torch.empty(eng.nq, dtype=torch.float64, device='cuda') if screened else None
     eri.set_prim_tol(PRIM_TOL if args.only == 'screened_prim' else 0.0)
 
     def step():
         if screened:
             eng.analytic_bounds(out=bounds)
-        eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW if screened else 0.0)
+        if args.only != 'bounds':  # bounds: the analytic-bound kernel alone
+            eng.compute(out=out, bounds=bounds, skip_below=SKIP_BELOW if screened else 0.0)
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -757,7 +759,8 @@ def run_only(args, eng, out):
     assert eng.device_status() == 0
     print(json.dumps({'only': args.only, 'nq': eng.nq, 'steps': args.steps, 'warmup': args.warmup,
                       'ms_per_step': ev0.elapsed_time(ev1) / args.steps,
-                      'kernels_per_step': eri.EriEngine.last_launch_count() + (1 if screened else 0)}), flush=True)
+                      'kernels_per_step': 1 if args.only == 'bounds' else
+                      eri.EriEngine.last_launch_count() + (1 if screened else 0)}), flush=True)
 
 
 def run_c5_classes(args):

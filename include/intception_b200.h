@@ -245,9 +245,11 @@ int intception_b200_set_prim_tol(double tol);
  * tol, the quartet is recomputed by the generic kernel, which builds every
  * primitive pair on the shell that conditions its HRR.  Default 1e-13
  * (outputs then agree with an exact evaluation to about 1e-13 on such
- * quartets); 0 switches the check off; tol outside [0, 1e-6] returns
- * IB_ERR_ARG.  New: the reference builds the ket by vertical recurrences on
- * both shells and has no such check. */
+ * quartets); 0 switches the check off, and quartets with a pair whose HRR
+ * growth bound is large in the class kernels' shell order then go to the
+ * generic kernel a priori; tol outside [0, 1e-6] returns IB_ERR_ARG.  New:
+ * the reference builds the ket by vertical recurrences on both shells and has
+ * no such check. */
 int intception_b200_set_hrr_tol(double tol);
 
 /* Tuning: register budget of the kernel of canonical class cid for variant v4

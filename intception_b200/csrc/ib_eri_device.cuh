@@ -593,13 +593,27 @@ __device__ __forceinline__ double ib_pair_bound(double K, double zeta, double pa
 // coefficients stay in registers).  Every operand is positive, so the float
 // result is within a few hundred ulp (< 1e-4 relative) of the exact one; the
 // factor 1.001 makes it an upper bound.  The Gaussian factor exp(-x0 x1 R^2 /
-// zeta) stays in FP64 below exp(-80), where float would flush it to zero.
+// zeta): float above exp(-80); down to exp(-708) a float 2^frac scaled by an
+// exact power of two (FP64 range, float accuracy); in the subnormal band FP64
+// exp; zero below exp(-745.2), where FP64 exp is zero too.
 template <int MAXDEG>
 __device__ __forceinline__ double ib_pair_bound_rt(int l0, int l1, bool sph, double cc, double x0, double x1,
                                                    double R) {
   const float z = (float)(x0 + x1), oz = 1.0f / z;
-  const double argd = -x0 * x1 / (x0 + x1) * (R * R);
-  const double e = argd > -80.0 ? (double)__expf((float)argd) : exp(argd);
+  // the Gaussian's argument in float: ~4e-7 relative, so under 3e-4 of the
+  // factor at the exp(-708) end, inside the 1.001 margin with the polynomial's error
+  const float arg = -((float)x0 * (float)x1 * oz) * (float)(R * R);
+  if (arg < -745.2f) return 0.0;  // exp underflows to zero in FP64 there (a NaN goes on)
+  double e;
+  if (arg > -80.0f) {
+    e = (double)__expf(arg);
+  } else if (arg > -708.0f) {
+    // 2^t, t = arg log2(e): float 2^frac times an exact normal power of two (5e-5 relative)
+    const float t = arg * 1.44269504f, n = floorf(t);
+    e = (double)exp2f(t - n) * __longlong_as_double((long long)(1023 + (int)n) << 52);
+  } else {
+    e = exp((double)arg);  // the subnormal band, where a scaled float would round differently
+  }
   const float pa = (float)x1 * oz * (float)R, pb = (float)x0 * oz * (float)R;
   const int deg = l0 + l1;
   float c[MAXDEG + 1];  // MAXDEG >= l0 + l1: the batch's 2 lmax, so the unrolled loops stay short

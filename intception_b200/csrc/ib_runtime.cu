@@ -180,8 +180,8 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
                             const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                             const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz, int nq,
                             int lmax, const double* __restrict__ bounds, double skip_below, double thr, int mixed,
-                            const int* __restrict__ kind, unsigned* __restrict__ keys, int* __restrict__ vals,
-                            int* status) {
+                            const int* __restrict__ kind, int route_rev, unsigned* __restrict__ keys,
+                            int* __restrict__ vals, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], st[4] = {0, 0, 0, 0};
     bool bad = false;
@@ -198,15 +198,18 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int skip = (bounds && bounds[q] < skip_below) ? 1 : 0;
     // a class kernel builds every pair on its higher-l shell; a pair whose
     // horizontal recurrence would lose too many digits that way is built on
-    // the other shell: by the (d f| class kernels for an (f d) pair of an
-    // l <= 3 quartet, else by the generic kernel (ib_reverse_for_classes)
+    // the other shell by the (d f| class kernels for an (f d) pair of an
+    // l <= 3 quartet (ib_reverse_for_classes).  Any other such quartet stays
+    // with its class kernel while the HRR check is on (route_rev 0: the check
+    // hands it to the generic kernel if its estimate is over the tolerance),
+    // else goes to the generic kernel
     const int rv = (!skip && !bad) ? ib_reverse_noinline(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st) : 0;
     const int pb = ib_pair_ext(l[0], l[1]), pk = ib_pair_ext(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
     const int nprim = shell_k[s[0]] * shell_k[s[1]] * shell_k[s[2]] * shell_k[s[3]];
     const int work = min(15, 31 - __clz(max(nprim, 1)));  // floor(log2) of the primitive quartet count
     const int k = kind[cid];
-    const int gen = (!skip && (k == 0 || rv == 2)) ? 1 : 0;
+    const int gen = (!skip && (k == 0 || (rv == 2 && route_rev))) ? 1 : 0;
     const int fp32 = (!gen && !skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
     // primitive quartet counts (powers of two) descending inside a class: the
     // longest quartets start first
@@ -300,46 +303,87 @@ __global__ void ib_zero_screened(const unsigned* __restrict__ keys, int nq, cons
   }
 }
 
-// Analytic screening bound of every quartet: two lanes per quartet (the bra
-// and the ket pair, neighbours in one warp), each summing the Coulomb-norm
-// bound Q of its pair's primitive pairs (ib_pair_bound_rt; the triangle
-// inequality over the contraction), then bounds[q] = Q_ab Q_cd >= |(ab|cd)| of
-// every element (Cauchy-Schwarz in the Coulomb metric).  An l outside [0, 6]
-// gives +inf (never screened; the batch reports it).
+// Analytic screening bound of every quartet: bounds[q] = Q_ab Q_cd >=
+// |(ab|cd)| of every element (Cauchy-Schwarz in the Coulomb metric), Q of a
+// pair the sum of the Coulomb-norm bounds of its primitive pairs
+// (ib_pair_bound_rt; the triangle inequality over the contraction).  An l
+// outside [0, 6] gives +inf (never screened; the batch reports it).
+//
+// One warp takes 16 quartets, 32 pairs (lane 2i the bra of quartet i, lane
+// 2i+1 its ket).  Their primitive pairs (1 to K^2 each) form one list in pair
+// order; the lanes evaluate it strided, 256 entries at a time, into shared
+// memory, and each lane then adds its own pair's entries in order.  Pairs of
+// different lengths no longer hold the warp to the longest one, and each Q is
+// the same ordered sum as a lane looping over its own primitive pairs.
+#define IB_QB_CHUNK 256
 template <int MAXDEG>
-__global__ void ib_quartet_bounds(const int* __restrict__ quartets, int nq, const int* __restrict__ shell_l,
-                                  const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
-                                  const double* __restrict__ shell_xyz, const double* __restrict__ prim_exp,
-                                  const double* __restrict__ prim_coef, int spherical, double* __restrict__ bounds) {
-  const long long nthr = 2LL * ((nq + 15) / 16) * 16;  // whole half-warps: both lanes of a quartet stay together
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t - threadIdx.x % 32 < nthr;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int q = (int)(t >> 1), side = (int)(t & 1);
-    double Q = 0.0;
+__global__ void __launch_bounds__(256) ib_quartet_bounds(const int* __restrict__ quartets, int nq,
+                                  const int* __restrict__ shell_l, const int* __restrict__ shell_k,
+                                  const int* __restrict__ shell_ptr, const double* __restrict__ shell_xyz,
+                                  const double* __restrict__ prim_exp, const double* __restrict__ prim_coef,
+                                  int spherical, double* __restrict__ bounds) {
+  __shared__ double val[8][IB_QB_CHUNK];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* __restrict__ v = val[wib];
+  const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long q0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 16; q0 < nq; q0 += nwarp * 16) {
+    const long long q = q0 + (lane >> 1);
+    const int side = lane & 1;
+    int n = 0, l0 = 0, l1 = 0, k1 = 1, p0 = 0, p1 = 0;
+    double R = 0.0, Q = 0.0;
     if (q < nq) {
       const int s0 = __ldg(quartets + 4 * q + 2 * side), s1 = __ldg(quartets + 4 * q + 2 * side + 1);
-      const int l0 = __ldg(shell_l + s0), l1 = __ldg(shell_l + s1);
+      l0 = __ldg(shell_l + s0);
+      l1 = __ldg(shell_l + s1);
       if (l0 < 0 || l1 < 0 || l0 > IB_LMAX || l1 > IB_LMAX || l0 + l1 > MAXDEG) {  // l above lmax: never screened
         Q = __longlong_as_double(0x7ff0000000000000LL);
       } else {
-        const int k0 = __ldg(shell_k + s0), k1 = __ldg(shell_k + s1);
-        const int p0 = __ldg(shell_ptr + s0), p1 = __ldg(shell_ptr + s1);
+        k1 = __ldg(shell_k + s1);
+        n = __ldg(shell_k + s0) * k1;
+        p0 = __ldg(shell_ptr + s0);
+        p1 = __ldg(shell_ptr + s1);
         double r2 = 0.0;
         for (int d = 0; d < 3; ++d) {
           const double u = __ldg(shell_xyz + 3 * s0 + d) - __ldg(shell_xyz + 3 * s1 + d);
           r2 += u * u;
         }
-        const double R = sqrt(r2);
-        for (int i = 0; i < k0; ++i) {
-          const double x0 = __ldg(prim_exp + p0 + i), c0 = __ldg(prim_coef + p0 + i);
-          for (int j = 0; j < k1; ++j) {
-            const double x1 = __ldg(prim_exp + p1 + j), c1 = __ldg(prim_coef + p1 + j);
-            Q += ib_pair_bound_rt<MAXDEG>(l0, l1, spherical != 0, c0 * c1, x0, x1, R);
-          }
-        }
-        Q *= 1.000001;  // the rounding of the sum
+        R = sqrt(r2);
       }
     }
+    // this pair's first entry in the warp's list, and the list's length
+    int start = n;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, start, o);
+      if (lane >= o) start += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, start, 31);
+    start -= n;
+    for (int c0 = 0; c0 < total; c0 += IB_QB_CHUNK) {
+      for (int t = c0 + lane; t < c0 + IB_QB_CHUNK; t += 32) {
+        // the pair holding entry t: the last lane whose start is <= t (binary search)
+        int j = 0;
+        for (int step = 16; step > 0; step >>= 1) {
+          const int st = __shfl_sync(0xffffffffu, start, j + step);
+          if (st <= t) j += step;
+        }
+        const int sj = __shfl_sync(0xffffffffu, start, j), nj = __shfl_sync(0xffffffffu, n, j);
+        const int k1j = __shfl_sync(0xffffffffu, k1, j), p0j = __shfl_sync(0xffffffffu, p0, j);
+        const int p1j = __shfl_sync(0xffffffffu, p1, j);
+        const int l0j = __shfl_sync(0xffffffffu, l0, j), l1j = __shfl_sync(0xffffffffu, l1, j);
+        const double Rj = __shfl_sync(0xffffffffu, R, j);
+        if (t < total && t - sj < nj) {
+          const int u = t - sj, i0 = u / k1j, i1 = u - i0 * k1j;
+          const double x0 = __ldg(prim_exp + p0j + i0), c0v = __ldg(prim_coef + p0j + i0);
+          const double x1 = __ldg(prim_exp + p1j + i1), c1v = __ldg(prim_coef + p1j + i1);
+          v[t - c0] = ib_pair_bound_rt<MAXDEG>(l0j, l1j, spherical != 0, c0v * c1v, x0, x1, Rj);
+        }
+      }
+      __syncwarp();
+      const int a = max(start, c0), e = min(start + n, c0 + IB_QB_CHUNK);
+      for (int t = a; t < e; ++t) Q += v[t - c0];
+      __syncwarp();
+    }
+    if (n > 0) Q *= 1.000001;  // the rounding of the sum
     const double other = __shfl_xor_sync(0xffffffffu, Q, 1);
     if (q < nq && side == 0) bounds[q] = Q * other * 1.000001;
   }
@@ -738,15 +782,15 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
   for (int h = 0; h < 2; ++h)
     if (rev[h] && !(lperm[2 * h] == 3 && lperm[2 * h + 1] == 2)) to_class = false;
   if (std::max(std::max(lperm[0], lperm[1]), std::max(lperm[2], lperm[3])) > 3) to_class = false;
-  for (int h = 0; h < 2; ++h)
-    if (rev[h]) swp(2 * h, 2 * h + 1);
-  if (to_class) {
-    if (ib_pair_ext(lperm[0], lperm[1]) < ib_pair_ext(lperm[2], lperm[3])) {
-      swp(0, 2);
-      swp(1, 3);
-    }
-  } else if (rev[0] || rev[1]) {
-    route = true;
+  // with the HRR check on, a reversed pair that no (d f| kernel serves stays
+  // with the class kernel in its canonical order (the check redoes it if needed)
+  if (!to_class && (rev[0] || rev[1])) route = !(c->hrr_tol > 0.0);
+  if (to_class || route)
+    for (int h = 0; h < 2; ++h)
+      if (rev[h]) swp(2 * h, 2 * h + 1);
+  if (to_class && ib_pair_ext(lperm[0], lperm[1]) < ib_pair_ext(lperm[2], lperm[3])) {
+    swp(0, 2);
+    swp(1, 3);
   }
   const int pbx = ib_pair_ext(lperm[0], lperm[1]), pkx = ib_pair_ext(lperm[2], lperm[3]);
   const int cidx = to_class ? pbx * (pbx + 1) / 2 + pkx : cid;
@@ -987,7 +1031,8 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   ib_classify<<<grid, 256, 0, s>>>(quartets, basis->shell_l, basis->shell_k, basis->shell_ptr, basis->prim_exp,
                                    basis->shell_xyz, nq, basis->lmax,
                                    use_bounds ? bounds : nullptr, skip_below, fp32_below,
-                                   precision == IB_PREC_MIXED ? 1 : 0, c->kind.as<int>(), c->keys.as<unsigned>(),
+                                   precision == IB_PREC_MIXED ? 1 : 0, c->kind.as<int>(), c->hrr_tol > 0.0 ? 0 : 1,
+                                   c->keys.as<unsigned>(),
                                    c->vals.as<int>(), c->status.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());
@@ -1211,8 +1256,8 @@ int intception_b200_quartet_bounds(const intception_b200_basis* basis, const int
   if (st) return st;
   cudaStream_t s;
   resolve_stream(c, stream, &s);
-  const long long threads = 2LL * ((nq + 15) / 16) * 16;
-  const int grid = (int)std::min<long long>((threads + 255) / 256, (long long)c->nsm * 16);
+  const long long warps = (nq + 15) / 16;  // 16 quartets per warp, 8 warps per block
+  const int grid = (int)std::min<long long>((warps + 7) / 8, (long long)c->nsm * 16);
   if (basis->lmax < 0 || basis->lmax > IB_LMAX) return set_status(IB_ERR_ARG, "quartet_bounds: basis lmax out of range");
 #define IB_QB(D)                                                                                                 \
   ib_quartet_bounds<D><<<grid, 256, 0, s>>>(quartets, nq, basis->shell_l, basis->shell_k, basis->shell_ptr,      \
