@@ -173,13 +173,18 @@ __host__ __device__ inline int ib_pair_ext(int la, int lb) {
 // (f d) pair and all four l <= 3, so the quartet is reordered here for the
 // (d f| class kernels (the pair reversed, then the pair with the larger
 // ib_pair_ext id first); 2: the generic kernel is needed (left unchanged).
+// fd_only (the HRR check is on, and it covers every other pair): only the
+// (f d) pairs of l <= 3 quartets are tested, so the result is 0 or 1.
 __device__ __forceinline__ int ib_reverse_for_classes(const int* __restrict__ shell_k,
                                                       const int* __restrict__ shell_ptr,
                                                       const double* __restrict__ prim_exp,
-                                                      const double* __restrict__ shell_xyz, int* s, int* l, int* st) {
+                                                      const double* __restrict__ shell_xyz, int* s, int* l, int* st,
+                                                      bool fd_only = false) {
+  if (fd_only && max(max(l[0], l[1]), max(l[2], l[3])) > 3) return 0;
   bool rev[2] = {false, false};
   for (int i = 0; i < 4; i += 2) {
     if (!(l[i] > l[i + 1] && l[i + 1] >= 1)) continue;
+    if (fd_only && !(l[i] == 3 && l[i + 1] == 2)) continue;
     double R2 = 0.0;
     for (int d = 0; d < 3; ++d) {
       const double u = shell_xyz[3 * s[i] + d] - shell_xyz[3 * s[i + 1] + d];

@@ -172,8 +172,9 @@ __device__ __forceinline__ void ib_canon(int* s, int* l, int* st) {
 // the occupancy of the whole (gather-latency-bound) kernel.
 __device__ __noinline__ int ib_reverse_noinline(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                                                 const double* __restrict__ prim_exp,
-                                                const double* __restrict__ shell_xyz, int* s, int* l, int* st) {
-  return ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
+                                                const double* __restrict__ shell_xyz, int* s, int* l, int* st,
+                                                bool fd_only) {
+  return ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st, fd_only);
 }
 
 __global__ void ib_classify(const int* __restrict__ quartets, const int* __restrict__ shell_l,
@@ -203,13 +204,14 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     // with its class kernel while the HRR check is on (route_rev 0: the check
     // hands it to the generic kernel if its estimate is over the tolerance),
     // else goes to the generic kernel
-    const int rv = (!skip && !bad) ? ib_reverse_noinline(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st) : 0;
+    const int rv =
+        (!skip && !bad) ? ib_reverse_noinline(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st, !route_rev) : 0;
     const int pb = ib_pair_ext(l[0], l[1]), pk = ib_pair_ext(l[2], l[3]);
     const int cid = pb * (pb + 1) / 2 + pk;
     const int nprim = shell_k[s[0]] * shell_k[s[1]] * shell_k[s[2]] * shell_k[s[3]];
     const int work = min(15, 31 - __clz(max(nprim, 1)));  // floor(log2) of the primitive quartet count
     const int k = kind[cid];
-    const int gen = (!skip && (k == 0 || (rv == 2 && route_rev))) ? 1 : 0;
+    const int gen = (!skip && (k == 0 || rv == 2)) ? 1 : 0;  // rv 2 only when route_rev
     const int fp32 = (!gen && !skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
     // primitive quartet counts (powers of two) descending inside a class: the
     // longest quartets start first
@@ -223,8 +225,8 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
                                const int* __restrict__ quartets, const int* __restrict__ shell_l,
                                const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                                const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz,
-                               const long long* __restrict__ out_off,
-                               int spherical, IbItem* __restrict__ items, int* __restrict__ ranges) {
+                               const long long* __restrict__ out_off, int spherical, int route_rev,
+                               IbItem* __restrict__ items, int* __restrict__ ranges) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
     const int q = order[p];
     int s[4], l[4], n[4];
@@ -239,7 +241,7 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
     const int slot = (int)(key >> 4);  // skip*2048 + generic*1024 + fp32*512 + cid
     // the (d f| classes: the reordering classify chose (the same decision)
     if (((slot >> 10) & 3) == 0 && (slot & 511) >= IB_NPAIR * (IB_NPAIR + 1) / 2)
-      ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
+      ib_reverse_for_classes(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st, !route_rev);
     if (!(slot >> 11)) ib_compact_first(shell_k, shell_ptr, prim_exp, s, l, st);  // evaluated quartets only
     if (((slot >> 10) & 3) == 1) ib_orient_generic(shell_k, shell_ptr, prim_exp, shell_xyz, s, l, st);
     IbItem it;
@@ -1040,7 +1042,8 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
                                           c->vals.as<int>(), c->vals2.as<int>(), nq, 0, kKeyBits, s));
   ib_build_items<<<grid, 256, 0, s>>>(c->keys2.as<unsigned>(), c->vals2.as<int>(), nq, quartets, basis->shell_l,
                                       basis->shell_k, basis->shell_ptr, basis->prim_exp, basis->shell_xyz, out_off,
-                                      spherical ? 1 : 0, c->items.as<IbItem>(), c->ranges.as<int>());
+                                      spherical ? 1 : 0, c->hrr_tol > 0.0 ? 0 : 1, c->items.as<IbItem>(),
+                                      c->ranges.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());
   IbLaunch a = base_launch(c);
