@@ -690,10 +690,7 @@ def run_twoidx(args, rank, world, local):
                 'kernel': 'ib2_%s_kernel' % ('nuclear' if kind == twoidx.NUCLEAR else 'overlap'),
                 'alg_bytes_per_step': nbytes, 'alg_flops_per_step': flops,
                 'fp64_frac': (flops / (ms * 1e-3)) / peak64 if peak64 else None}
-    prof = os.path.join(ROOT, 'profiles', 'traffic_%s.json' % args.workload)
-    if os.path.exists(prof):
-        with open(prof) as fh:
-            roofline['traffic'] = json.load(fh).get('bytes_per_step')
+    roofline['traffic'] = profiled_traffic('traffic_%s.md' % args.workload)
     # e2e: host inputs -> device, the launch, the blocks back to host
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
     h_in = [pin(batch.xa.cpu()), pin(batch.ca.cpu()), pin(batch.la.cpu()), pin(batch.xb.cpu()),
@@ -728,6 +725,18 @@ def run_twoidx(args, rank, world, local):
                 'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': args.steps, 'gpu_launches_per_step': 1, 'clocks': clk.summary()}
         print(json.dumps(line), flush=True)
+
+
+def profiled_traffic(name):
+    """DRAM bytes per step recorded from an ncu capture in profiles/<name>
+    (its line 'bytes per step: N'), or None when there is no such record."""
+    import re
+    path = os.path.join(ROOT, 'profiles', name)
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        m = re.search(r'^bytes per step: ([0-9.eE+]+)', fh.read(), re.M)
+    return float(m.group(1)) if m else None
 
 
 def run_only(args, eng, out):
@@ -958,10 +967,11 @@ def run_eri(args, rank, world, local):
                                'MEASURED_PEAKS.json has no FP64 figure',
                 'kernel': 'whole FP64 step of this rank (per-class kernels run concurrently)',
                 'alg_flops_per_step': flops}
-    prof = os.path.join(ROOT, 'profiles', 'traffic.json')
-    if os.path.exists(prof):
-        with open(prof) as fh:
-            roofline['traffic'] = json.load(fh).get('bytes_per_step')
+    roofline['traffic'] = profiled_traffic('traffic_fp64_l2_sph.md')
+    if roofline['traffic']:
+        roofline['traffic_source'] = ('dram__bytes_read.sum + dram__bytes_write.sum of the FP64 step\'s '
+                                      'kernels, one ncu capture at 2e5 quartets scaled by the quartet count '
+                                      '(profiles/traffic_fp64_l2_sph.md)')
 
     # ---- e2e through the public API with host buffers: every step uploads its
     # inputs from pinned host memory, computes the analytic bounds and the
