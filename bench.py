@@ -409,6 +409,9 @@ def run_c5(args, rank, world, local):
     batch, frac = c5_batch(args.nq_c5)
     eng = eri.EriEngine(batch)
     out = torch.empty(batch.out_size, dtype=torch.float64, device='cuda')
+    if args.only == 'fp64':  # profilers: the FP64 step alone
+        run_only(args, eng, out)
+        return
     bounds = torch.empty(batch.nq, dtype=torch.float64, device='cuda')
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
