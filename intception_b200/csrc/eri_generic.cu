@@ -23,6 +23,8 @@
 //   bra  [(L+2) * ncumE]           [e0|00]^(m) over every e <= la+lb
 //   ket  3 * klev                  [e0|f0]^(m) of the ket levels f >= 1, level f in slot f mod 3
 //   h0,h1 [hmax] ping-pong buffers for HRR and the spherical transform
+#include <cstdlib>
+
 #include "ib_eri_device.cuh"
 #include "ib_generic.cuh"
 
@@ -83,8 +85,9 @@ struct IbGenShared {
 
 }  // namespace
 
-__global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
-                                                               double* __restrict__ scratch, long long slice) {
+template <int MINB>
+__global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
+                                                                     double* __restrict__ scratch, long long slice) {
   __shared__ IbGenShared sh;
   __shared__ unsigned short ct[IB_GEN_NCT];
   // em[i][e]: the index of e - 1_i (low 9 bits) and the exponent of e along i
@@ -404,4 +407,27 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK) ib_eri_generic(const IbLaunch a,
     }  // pass
     __syncthreads();
   }
+}
+
+// Resident blocks per SM the generic kernel is compiled for and launched
+// with: INTCEPTION_B200_GENERIC_BPS = 2 (the default), 3 or 4.  More blocks
+// hide more of the scratch latency but hold fewer registers per thread and
+// more scratch in flight.
+int ib_generic_bps() {
+  static const int v = [] {
+    const char* e = getenv("INTCEPTION_B200_GENERIC_BPS");
+    const int x = e ? atoi(e) : 2;
+    return (x == 3 || x == 4) ? x : 2;
+  }();
+  return v;
+}
+
+cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, int range_slot, int sph, double* scratch,
+                              long long slice) {
+  switch (ib_generic_bps()) {
+    case 3: ib_eri_generic<3><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
+    case 4: ib_eri_generic<4><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
+    default: ib_eri_generic<2><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
+  }
+  return cudaGetLastError();
 }

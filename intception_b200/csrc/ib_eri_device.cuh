@@ -76,6 +76,12 @@ __device__ __forceinline__ void ib_redo_push(const IbLaunch& a, int p) {
   if (!(atomicOr(a.flags + p, 2) & 2)) a.redo[1 + atomicAdd(a.redo, 1)] = p;
 }
 
+// The generic block-per-quartet kernel (eri_generic.cu): blocks per SM it runs
+// with, and its launch (range_slot < 0: the redo list).
+int ib_generic_bps();
+cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, int range_slot, int sph, double* scratch,
+                              long long slice);
+
 // Smallest primitive exponent of shell s.
 __device__ __forceinline__ double ib_min_exp(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                                              const double* __restrict__ prim_exp, int s) {

@@ -26,7 +26,6 @@
 #include "ib_eri_device.cuh"
 #include "ib_generic.cuh"
 
-__global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double* scratch, long long slice);
 void build_sph_host(std::vector<double>& out);
 
 #define IB_NOALLOC_SCRATCH_DOUBLES (size_t(4) << 20)  // 32 MiB
@@ -208,9 +207,8 @@ extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* ba
   a.out = out;
   a.status = d->status;
   a.slice_boost = 1;
-  const long long grid = std::min<long long>({(long long)nq, 2LL * d->nsm, fit});
-  ib_eri_generic<<<(int)grid, IB_GEN_BLOCK, 0, s>>>(a, kNoallocSlot, spherical ? 1 : 0, d->scratch, slice);
-  const cudaError_t e = cudaGetLastError();
+  const long long grid = std::min<long long>({(long long)nq, (long long)ib_generic_bps() * d->nsm, fit});
+  const cudaError_t e = ib_generic_launch((int)grid, s, a, kNoallocSlot, spherical ? 1 : 0, d->scratch, slice);
   if (e != cudaSuccess)
     return ib_runtime_set_status(IB_ERR_CUDA, (std::string("eri_batch_noalloc: ") + cudaGetErrorString(e)).c_str());
   return ib_runtime_set_status(IB_OK, "");

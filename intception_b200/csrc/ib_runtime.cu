@@ -38,7 +38,6 @@ extern const int ib_lmax_emitted;
 extern const int ib_tuned_minb[IB_NCLASS][4];
 extern const int ib_tuned_slice_cap[IB_NCLASS];
 extern const int ib_tuned_fp32[IB_NCLASS];
-__global__ void ib_eri_generic(const IbLaunch a, int range_slot, int sph, double* scratch, long long slice);
 
 namespace {
 
@@ -583,12 +582,12 @@ int class_lmax(int cid) {
 // kernels that fill it).
 cudaError_t redo_launch(Context* c, cudaStream_t s, const IbLaunch& a, bool sph, int lmax) {
   const long long slice = generic_slice(lmax);
-  long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
+  long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
+                                      (long long)(kScratchCap / (slice * sizeof(double))));
   nblk = std::max<long long>(nblk, 1);
   cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
   if (e != cudaSuccess) return e;
-  ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, s>>>(a, -1, sph ? 1 : 0, c->scratch.as<double>(), slice);
-  return cudaGetLastError();
+  return ib_generic_launch((int)nblk, s, a, -1, sph ? 1 : 0, c->scratch.as<double>(), slice);
 }
 
 // Launch the emitted kernels for the given variants and the generic kernel;
@@ -640,11 +639,12 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   // empty range returns at once
   if ((lmax > ib_lmax_emitted || lmax >= 2) && fp64_present) {
     const long long slice = generic_slice(lmax);
-    long long nblk = std::min<long long>(2LL * c->nsm, (long long)(kScratchCap / (slice * sizeof(double))));
+    long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
+                                        (long long)(kScratchCap / (slice * sizeof(double))));
     nblk = std::max<long long>(nblk, 1);
     IB_CUDA(c->scratch.ensure((size_t)nblk * slice * sizeof(double)));
-    ib_eri_generic<<<(int)nblk, IB_GEN_BLOCK, 0, c->side[k % c->nside]>>>(a, kSlotGeneric, sph ? 1 : 0,
-                                                                         c->scratch.as<double>(), slice);
+    IB_CUDA(ib_generic_launch((int)nblk, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0,
+                              c->scratch.as<double>(), slice));
     ++k;
   }
   IB_CUDA(cudaGetLastError());
@@ -856,11 +856,11 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
       IB_CUDA(redo_launch(c, s, a, false, std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l))));
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
-    long long nb = std::min<long long>({(long long)nblk, 2LL * c->nsm,
+    long long nb = std::min<long long>({(long long)nblk, (long long)ib_generic_bps() * c->nsm,
                                         (long long)(kScratchCap / (slice * sizeof(double)))});
     nb = std::max<long long>(nb, 1);
     IB_CUDA(c->scratch.ensure((size_t)nb * slice * sizeof(double)));
-    ib_eri_generic<<<(int)nb, IB_GEN_BLOCK, 0, s>>>(a, kSlotGeneric, 0, c->scratch.as<double>(), slice);
+    IB_CUDA(ib_generic_launch((int)nb, s, a, kSlotGeneric, 0, c->scratch.as<double>(), slice));
   }
   IB_CUDA(cudaGetLastError());
   IbXform x;
