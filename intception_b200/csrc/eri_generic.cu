@@ -291,7 +291,8 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
           const unsigned short* emi = em + i * IB_GEN_NCT;
           const bool to_acc = m == 0 && lf >= d.lc;
           double* accc = acc + (size_t)(ib_ncum(lf - 1) + fc - d.f0) * d.ne;  // this f's row of [f][e]
-          for (int e = lane; e < E_; e += 32) {
+#pragma unroll 4
+          for (int e = lane; e < E_; e += 32) {  // unrolled: the lanes' loads of several e issue together
             double v = qc * r10[e] + wq * r11[e];
             if (nn > 0) v += t2 * (r20[e] - roe * r21[e]);
             const unsigned t = emi[e];

@@ -605,6 +605,24 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
                                                                      zf->out_off, sph ? 1 : 0, a.out);
     ++*nlaunch;
   }
+  // the generic kernel serves the classes without an unrolled kernel and, for
+  // lmax >= 2 with the HRR check off, the quartets classify routes to it (an
+  // empty range returns at once).  From lmax 3 its range is the longest job
+  // of a batch, so it starts first; below, after the class kernels.
+  auto launch_generic = [&]() -> cudaError_t {
+    const long long slice = generic_slice(lmax);
+    long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
+                                        (long long)(kScratchCap / (slice * sizeof(double))));
+    nblk = std::max<long long>(nblk, 1);
+    cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
+    if (e != cudaSuccess) return e;
+    e = ib_generic_launch((int)nblk, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0, c->scratch.as<double>(),
+                          slice);
+    ++k;
+    return e;
+  };
+  const bool generic = (lmax > ib_lmax_emitted || lmax >= 2) && fp64_present;
+  if (generic && lmax >= 3) IB_CUDA(launch_generic());
   for (int prec = 0; prec < 2; ++prec) {
     if ((prec == 0 && !fp64_present) || (prec == 1 && !fp32_present)) continue;
     IbLaunch ap = a;
@@ -634,19 +652,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       }
     }
   }
-  // the generic kernel serves the classes without an unrolled kernel and, for
-  // lmax >= 2, the quartets classify routes to it (ib_orient_generic); an
-  // empty range returns at once
-  if ((lmax > ib_lmax_emitted || lmax >= 2) && fp64_present) {
-    const long long slice = generic_slice(lmax);
-    long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
-                                        (long long)(kScratchCap / (slice * sizeof(double))));
-    nblk = std::max<long long>(nblk, 1);
-    IB_CUDA(c->scratch.ensure((size_t)nblk * slice * sizeof(double)));
-    IB_CUDA(ib_generic_launch((int)nblk, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0,
-                              c->scratch.as<double>(), slice));
-    ++k;
-  }
+  if (generic && lmax < 3) IB_CUDA(launch_generic());
   IB_CUDA(cudaGetLastError());
   for (int i = 0; i < c->nside; ++i) {
     IB_CUDA(cudaEventRecord(c->join[i], c->side[i]));
