@@ -465,6 +465,14 @@ def run_c5(args, rank, world, local):
     msg = timed(graph_step)
     errg = max_over_ranks(float((out - ref).abs().max().item()), world)
     graph.close()
+    # the headline: the fastest path within 1e-10 of exact FP64, then measured again on its own
+    cands = [(ms64, 0.0, 'fp64'), (mss, errs, 'fp64 + screening'), (msm, errm, 'precision tiers')]
+    _, _, path = min([c for c in cands if c[1] <= ERR_BAR] or cands)
+    if path == 'fp64':
+        eri.set_prim_tol(0.0)
+    ms_head = timed({'fp64': lambda: eng.compute(out=out), 'fp64 + screening': lambda: screened_step(eri.PREC_FP64),
+                     'precision tiers': lambda: screened_step(eri.PREC_MIXED)}[path])
+    err_head = max_over_ranks(float((out - ref).abs().max().item()), world)
     eri.set_prim_tol(0.0)
     clk.__exit__(None, None, None)
     # live primitive quartets of the sample (the per-primitive cost against (ff|ff))
@@ -479,13 +487,14 @@ def run_c5(args, rank, world, local):
         nq = batch.nq * world
         print(json.dumps({
             'metric': 'contracted ERI quartets/s on B200, l<=4 K<=8 screened quartets (sample of the 5e7 batch)',
-            'value': nq / (msm * 1e-3), 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': msm, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'f64+f32', 'data': 'synthetic',
+            'value': nq / (ms_head * 1e-3), 'unit': 'quartets/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_head, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64+f32' if path == 'precision tiers' else 'f64', 'data': 'synthetic',
             'config': {'workload': C5_WORKLOAD % batch.nq, 'kept_fraction_of_candidates': frac,
+                       'headline_path': path + ' (the fastest path within 1e-10 of exact FP64, measured again)',
                        'prim_tol': PRIM_TOL, 'fp32_below': FP32_BELOW, 'mixed_tol': MIXED_TOL,
                        'l2': 'outputs %.0f MB per step; no flush' % (batch.out_size * 8 / 1e6)},
-            'max_abs_err_vs_fp64': errm, 'max_abs_err_vs_reference': ref_err,
+            'max_abs_err_vs_fp64': err_head, 'max_abs_err_vs_reference': ref_err,
             'fp64': {'ms_per_step': ms64, 'value': nq / (ms64 * 1e-3), 'note': 'every sampled quartet, FP64',
                      'ns_per_live_primitive_quartet': ms64 * 1e6 / nprim, 'hrr_redo': redo64},
             'fp64_screened': {'ms_per_step': mss, 'value': nq / (mss * 1e-3), 'max_abs_err_vs_fp64': errs,
@@ -494,7 +503,7 @@ def run_c5(args, rank, world, local):
             'cuda_graph': {'ms_per_step': msg, 'max_abs_err_vs_fp64': errg},
             'hrr_tol': HRR_TOL,
             'mixed_over_fp64': mss / msm, 'live_primitive_quartets': nprim,
-            'estimated_5e7_quartets_s': 5e7 / (nq / (msm * 1e-3)),
+            'estimated_5e7_quartets_s': 5e7 / (nq / (ms_head * 1e-3)),
             'cpu_baseline': cpu, 'gpu_launches': launches * args.steps, 'clocks': clk.summary()}), flush=True)
 
 

@@ -48,7 +48,8 @@ constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-
 constexpr int kNRanges = 4 * IB_NCLASS + 4;
 constexpr int kNCounters = 3 * IB_NCLASS;      // quartet counters: FP64 pass, FP32 pass, FP64 recheck pass
 constexpr int kKeyBits = 16;                    // skip(1) generic(1) fp32(1) class(9) work(4): two radix passes
-constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
+constexpr size_t kScratchCap = size_t(4) << 30;
+constexpr int kRedoGroups = 4;  // redo lists of an l >= 3 batch (dispatch)  // bytes of generic-kernel scratch at most
 
 thread_local int tl_status = IB_OK;
 thread_local std::string tl_msg;
@@ -126,7 +127,8 @@ struct Context {
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;    // per sorted item of the last batch: FP32 rejection (bit 0), on the redo list (bit 1)
   int flags_nq = 0;  // its quartet count (flags beyond it are stale)
-  DevBuf redo;     // the last batch's redo list: count, then sorted items
+  DevBuf redo;     // the last batch's redo lists (redo_groups of them, redo_stride ints apart): count, then sorted items
+  int redo_groups = 1, redo_stride = 1;
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
   int kind_h[IB_NCLASS] = {};  // host copy of kind: 2 where the class has FP32 kernels and the FP32 tier uses them
   DevBuf d_stage, d_cart, d_res;
@@ -597,6 +599,17 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   IB_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < c->nside; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
   int k = 0;
+  // redo lists: one per group of side streams when the batch has several
+  // (the class kernels of side stream j fill list j mod G; each group's redo
+  // launch follows its own class kernels and overlaps the others')
+  const bool redo_on = a.redo && a.hrr_tol > 0.0;
+  const int G = redo_on ? std::min(c->redo_groups, c->nside) : 1;
+  // generic-kernel scratch: the range launch's region, then one per grouped redo launch
+  const long long gslice = generic_slice(lmax);
+  const long long gfull = std::max<long long>(
+      1, std::min<long long>((long long)ib_generic_bps() * c->nsm, (long long)(kScratchCap / (gslice * sizeof(double)))));
+  const long long ggroup = gfull;  // each group's redo may take the whole GPU once the others are done
+  if (G > 1) IB_CUDA(c->scratch.ensure((size_t)(gfull + G * ggroup) * gslice * sizeof(double)));
   // screened quartets: zero blocks, concurrent with the class kernels (launched
   // first with 4 blocks per SM: measured no slower than 1 or 2 blocks per SM, or
   // than launching it after the class kernels)
@@ -610,14 +623,10 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   // empty range returns at once).  From lmax 3 its range is the longest job
   // of a batch, so it starts first; below, after the class kernels.
   auto launch_generic = [&]() -> cudaError_t {
-    const long long slice = generic_slice(lmax);
-    long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
-                                        (long long)(kScratchCap / (slice * sizeof(double))));
-    nblk = std::max<long long>(nblk, 1);
-    cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
+    cudaError_t e = c->scratch.ensure((size_t)(gfull + (G > 1 ? G * ggroup : 0)) * gslice * sizeof(double));
     if (e != cudaSuccess) return e;
-    e = ib_generic_launch((int)nblk, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0, c->scratch.as<double>(),
-                          slice);
+    e = ib_generic_launch((int)gfull, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0, c->scratch.as<double>(),
+                          gslice);
     ++k;
     return e;
   };
@@ -635,6 +644,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
       const int vt = variant + 4 * c->minb_idx[cid][variant];
       const int grid = c->nsm * c->occ[cid][vt];
       cudaStream_t ss = c->side[k % c->nside];
+      if (G > 1) ap.redo = a.redo + (size_t)((k % c->nside) % G) * c->redo_stride;
       ap.max_slices = c->slice_cap[cid];
       ap.counter = c->counters.as<int>() + prec * IB_NCLASS + cid;
       c->table[cid].launch(vt, grid, ss, ap);
@@ -654,13 +664,25 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   }
   if (generic && lmax < 3) IB_CUDA(launch_generic());
   IB_CUDA(cudaGetLastError());
+  if (G > 1) {
+    // group g's redo on side stream g, after every class kernel of its streams
+    for (int j = 0; j < c->nside; ++j) IB_CUDA(cudaEventRecord(c->join[j], c->side[j]));
+    for (int g = 0; g < G; ++g) {
+      for (int j = g; j < c->nside; j += G)
+        if (j != g) IB_CUDA(cudaStreamWaitEvent(c->side[g], c->join[j], 0));
+      IbLaunch ag = a;
+      ag.redo = a.redo + (size_t)g * c->redo_stride;
+      IB_CUDA(ib_generic_launch((int)ggroup, c->side[g], ag, -1, sph ? 1 : 0,
+                                c->scratch.as<double>() + (size_t)(gfull + g * ggroup) * gslice, gslice));
+      ++k;
+    }
+  }
   for (int i = 0; i < c->nside; ++i) {
     IB_CUDA(cudaEventRecord(c->join[i], c->side[i]));
     IB_CUDA(cudaStreamWaitEvent(s, c->join[i], 0));
   }
-  // after every class kernel: the quartets they put on the redo list (an
-  // empty list returns at once)
-  if (a.redo && a.hrr_tol > 0.0) {
+  // one redo list: after every class kernel (an empty list returns at once)
+  if (redo_on && G == 1) {
     IB_CUDA(redo_launch(c, s, a, sph, lmax));
     ++k;
   }
@@ -853,6 +875,8 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nblk * sizeof(int), s));
     IB_CUDA(c->redo.ensure((size_t)(nblk + 1) * sizeof(int)));
     IB_CUDA(cudaMemsetAsync(c->redo.p, 0, sizeof(int), s));
+    c->redo_groups = 1;
+    c->redo_stride = nblk + 1;
     c->flags_nq = nblk;
     a.flags = c->flags.as<int>();
     a.redo = c->redo.as<int>();
@@ -1065,8 +1089,12 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   a.prim_tol = screen_prims ? c->prim_tol : 0.0;
   IB_CUDA(c->flags.ensure((size_t)nq * sizeof(int)));
   IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
-  IB_CUDA(c->redo.ensure((size_t)(nq + 1) * sizeof(int)));
-  IB_CUDA(cudaMemsetAsync(c->redo.p, 0, sizeof(int), s));
+  // l >= 3 batches: four redo lists, one per group of side streams (dispatch)
+  c->redo_groups = (basis->lmax >= 3 && c->hrr_tol > 0.0) ? kRedoGroups : 1;
+  c->redo_stride = nq + 1;
+  IB_CUDA(c->redo.ensure((size_t)c->redo_groups * (nq + 1) * sizeof(int)));
+  for (int g = 0; g < c->redo_groups; ++g)
+    IB_CUDA(cudaMemsetAsync(c->redo.as<int>() + (size_t)g * (nq + 1), 0, sizeof(int), s));
   c->flags_nq = nq;
   a.flags = c->flags.as<int>();
   a.redo = c->redo.as<int>();
@@ -1380,9 +1408,13 @@ int intception_b200_last_hrr_redo(void) {
   if (get_context(&c)) return -1;
   if (!c->redo.p) return 0;
   IB_CUDA(cudaDeviceSynchronize());
-  int h = 0;
-  IB_CUDA(cudaMemcpy(&h, c->redo.p, sizeof(int), cudaMemcpyDeviceToHost));
-  return h;
+  int total = 0;
+  for (int g = 0; g < c->redo_groups; ++g) {
+    int h = 0;
+    IB_CUDA(cudaMemcpy(&h, c->redo.as<int>() + (size_t)g * c->redo_stride, sizeof(int), cudaMemcpyDeviceToHost));
+    total += h;
+  }
+  return total;
 }
 
 // Tolerance of the class kernels' HRR rounding-error estimate, in the output's
