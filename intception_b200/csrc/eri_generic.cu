@@ -18,15 +18,32 @@
 // primitive quartet uses, each over those primitive quartets only; the first
 // pass stores the block and the others add to it.
 //
+// One block walks a quartet's primitive quartets one after the other, so a
+// quartet of K = 8 shells alone would outlast a whole batch.  Heavy quartets
+// (IB_GEN_SPLIT_MIN primitive quartets or more) therefore go to a cluster of
+// IB_GEN_SPLIT blocks: block r of the cluster takes primitive quartets r, r +
+// IB_GEN_SPLIT, ... of each pass into its own contracted table; after a
+// cluster barrier the blocks sum the tables in rank order (each a share of the
+// elements) into rank 0's, which then runs the HRRs and stores the block.  The
+// sum order is fixed, so the results do not depend on the timing.  Clusters
+// take heavy quartets from a ticket counter in list order (heaviest first in a
+// range), then every block takes light quartets alone from a second one.
+//
 // Scratch slice layout (doubles), sizes from ib_generic_dims():
 //   acc  [nf * ne]                 contracted [e0|f0] stored [f][e], e in [la,la+lb], f in [lc,lc+ld]
 //   bra  [(L+2) * ncumE]           [e0|00]^(m) over every e <= la+lb
 //   ket  3 * klev                  [e0|f0]^(m) of the ket levels f >= 1, level f in slot f mod 3
 //   h0,h1 [hmax] ping-pong buffers for HRR and the spherical transform
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <atomic>
 #include <cstdlib>
 
 #include "ib_eri_device.cuh"
 #include "ib_generic.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -34,6 +51,8 @@ namespace {
 // (every index the kernel decodes: levels up to 2 IB_LMAX), 5 bits each,
 // filled once per block: the level loops read them instead of decoding.
 #define IB_GEN_NCT 455
+// primitive quartets tested at once (IB_GEN_CHUNK / IB_GEN_BLOCK per thread)
+#define IB_GEN_CHUNK 1024
 static_assert(IB_GEN_NCT == (2 * IB_LMAX + 1) * (2 * IB_LMAX + 2) * (2 * IB_LMAX + 3) / 6, "component table size");
 __device__ __forceinline__ void ib_ct_get(const unsigned short* ct, int cum, int& x, int& y, int& z) {
   const unsigned v = ct[cum];
@@ -81,18 +100,14 @@ struct IbGenShared {
   int use[2];                  // per pair: bit o set when some primitive pair has orientation o
   float R[2];                  // |AB|, |CD| of the item
   long long off;
+  unsigned short live[IB_GEN_CHUNK];  // this rank's live primitive quartets of the chunk (offsets)
+  int wcnt[IB_GEN_BLOCK / 32];        // per warp: live primitive quartets of one round
 };
 
-}  // namespace
-
-template <int MINB>
-__global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLaunch a, int range_slot, int sph,
-                                                                     double* __restrict__ scratch, long long slice) {
-  __shared__ IbGenShared sh;
-  __shared__ unsigned short ct[IB_GEN_NCT];
-  // em[i][e]: the index of e - 1_i (low 9 bits) and the exponent of e along i
-  // (above them; 0: no such component)
-  __shared__ unsigned short em[3 * IB_GEN_NCT];
+// ct[cum]: the Cartesian exponents of every cumulative component index;
+// em[i][e]: the index of e - 1_i (low 9 bits) and the exponent of e along i
+// (above them; 0: no such component).
+__device__ __forceinline__ void ib_gen_tables(unsigned short* ct, unsigned short* em) {
   for (int t = threadIdx.x; t < IB_GEN_NCT; t += blockDim.x) {
     int x, y, z;
     ib_comp_of(t, x, y, z);
@@ -108,15 +123,19 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
       em[i * IB_GEN_NCT + t] = (unsigned short)(ib_cidx(v[0], v[1], v[2]) | (c[i] << 9));
     }
   }
-  __syncthreads();
+}
+
+// One contracted quartet, sorted item p, in the block's scratch slice w.
+// CS > 1: this block is rank crank of the CS blocks of a cluster that evaluate
+// the quartet together (every rank calls this with the same p); wc is rank 0's
+// slice, the ranks' slices follow it slice doubles apart.
+template <int CS>
+__device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, double* __restrict__ w,
+                                            double* __restrict__ wc, long long slice, int crank, IbGenShared& sh,
+                                            const unsigned short* __restrict__ ct,
+                                            const unsigned short* __restrict__ em) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  // range_slot < 0: the redo list (a.redo[0] items at a.redo + 1)
-  const bool redo = range_slot < 0;
-  const int beg = redo ? 0 : a.ranges[range_slot], end = redo ? a.redo[0] : a.ranges[range_slot + 1];
-  double* __restrict__ w = scratch + (size_t)blockIdx.x * (size_t)slice;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int pi = beg + blockIdx.x; pi < end; pi += gridDim.x) {
-    const int p = redo ? a.redo[1 + pi] : pi;
     if (tid == 0) {
       const IbItem it = a.items[p];
       const bool bad = it.st[0] == 0;  // an l out of range: evaluated as (ss|ss), the status already says so
@@ -180,21 +199,51 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
     const double RAB2 = sh.AB[0] * sh.AB[0] + sh.AB[1] * sh.AB[1] + sh.AB[2] * sh.AB[2];
     const double RCD2 = sh.CD[0] * sh.CD[0] + sh.CD[1] * sh.CD[1] + sh.CD[2] * sh.CD[2];
     const int nprim = sh.k[0] * sh.k[1] * sh.k[2] * sh.k[3];
-    for (int pq = 0; pq < nprim; ++pq) {
-      {  // every thread decides alike: skip primitive quartets of other passes and exact zeros
-        int r = pq;
-        const int id = r % sh.k[3]; r /= sh.k[3];
-        const int ic = r % sh.k[2]; r /= sh.k[2];
-        const int ib = r % sh.k[1]; r /= sh.k[1];
-        const int ia = r;
-        const double xa = a.prim_exp[sh.ptr[0] + ia], xb = a.prim_exp[sh.ptr[1] + ib];
-        const double xc = a.prim_exp[sh.ptr[2] + ic], xd = a.prim_exp[sh.ptr[3] + id];
-        // the prefactor's Gaussian exactly as below: zero means the primitive quartet adds exact zeros
-        if (exp(-xa * xb * (1.0 / (xa + xb)) * RAB2 - xc * xd * (1.0 / (xc + xd)) * RCD2) == 0.0) continue;
-        // exponents in the item's order of each pair
-        if (split_b && ib_gen_orient(sh.l0[0], sh.l0[1], ob ? xb : xa, ob ? xa : xb, sh.R[0]) != ob) continue;
-        if (split_k && ib_gen_orient(sh.l0[2], sh.l0[3], ok ? xd : xc, ok ? xc : xd, sh.R[1]) != ok) continue;
+    // The pass's live primitive quartets (not exactly zero, and of this pass's
+    // orientations) are numbered in order; live quartet j belongs to rank
+    // j % CS, so the ranks get equal shares of the work.  A chunk of
+    // IB_GEN_CHUNK is tested in parallel, one quartet per thread and round (a
+    // block prefix of warp ballots numbers them), and this rank's live ones are
+    // listed in order in sh.live.  One block (CS 1) thus adds its live
+    // primitive quartets in ascending order.
+    int base = 0;  // live primitive quartets of the pass before the current round
+    auto ranks_below = [&](int n) { return n > crank ? (n - crank + CS - 1) / CS : 0; };  // this rank's, of the first n
+    for (int c0 = 0; c0 < nprim; c0 += IB_GEN_CHUNK) {
+      const int mine0 = ranks_below(base);
+      for (int k0 = 0; k0 < IB_GEN_CHUNK; k0 += IB_GEN_BLOCK) {
+        const int pq = c0 + k0 + tid;
+        bool live = false;
+        if (pq < nprim) {
+          int r = pq;
+          const int id = r % sh.k[3]; r /= sh.k[3];
+          const int ic = r % sh.k[2]; r /= sh.k[2];
+          const int ib = r % sh.k[1]; r /= sh.k[1];
+          const int ia = r;
+          const double xa = a.prim_exp[sh.ptr[0] + ia], xb = a.prim_exp[sh.ptr[1] + ib];
+          const double xc = a.prim_exp[sh.ptr[2] + ic], xd = a.prim_exp[sh.ptr[3] + id];
+          // the prefactor's Gaussian exactly as below: zero means the primitive quartet adds exact zeros
+          live = exp(-xa * xb * (1.0 / (xa + xb)) * RAB2 - xc * xd * (1.0 / (xc + xd)) * RCD2) != 0.0;
+          // exponents in the item's order of each pair
+          if (live && split_b) live = ib_gen_orient(sh.l0[0], sh.l0[1], ob ? xb : xa, ob ? xa : xb, sh.R[0]) == ob;
+          if (live && split_k) live = ib_gen_orient(sh.l0[2], sh.l0[3], ok ? xd : xc, ok ? xc : xd, sh.R[1]) == ok;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) sh.wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int before = __popc(bal & ((1u << lane) - 1u)), total = 0;
+        for (int w2 = 0; w2 < nwarp; ++w2) {
+          const int cnt = sh.wcnt[w2];
+          before += w2 < warp ? cnt : 0;
+          total += cnt;
+        }
+        const int j = base + before;  // the live ordinal of pq
+        if (live && j % CS == crank) sh.live[(j - crank) / CS - mine0] = (unsigned short)(pq - c0);
+        base += total;
+        __syncthreads();  // sh.wcnt is rewritten by the next round
       }
+      const int nmine = ranks_below(base) - mine0;
+    for (int li = 0; li < nmine; ++li) {
+      const int pq = c0 + sh.live[li];
       __syncthreads();
       if (tid == 0) {
         int r = pq;
@@ -302,8 +351,27 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
           }
         }
       }
-    }
+    }  // this rank's live primitive quartets of the chunk
+    }  // chunk
     __syncthreads();
+    if (CS > 1) {
+      // the ranks' contracted tables are complete: each rank sums its share of
+      // the elements over the ranks, in rank order, into rank 0's table (reads
+      // from L2, __ldcg: a rank's L1 may hold lines another rank has written)
+      __threadfence();
+      cg::this_cluster().sync();
+      const int nacc = d.ne * d.nf, per = (nacc + CS - 1) / CS;
+      const int x1 = min(nacc, (crank + 1) * per);
+      double* __restrict__ acc0 = wc + d.o_acc;
+      for (int x = crank * per + tid; x < x1; x += nt) {
+        double v = __ldcg(acc0 + x);
+        for (int k = 1; k < CS; ++k) v += __ldcg(acc0 + (size_t)k * slice + x);
+        acc0[x] = v;
+      }
+      __threadfence();
+      cg::this_cluster().sync();
+      if (crank != 0) continue;  // rank 0 runs the HRRs and stores the block
+    }
     // ---- bra HRR: [e][b][f] layers, (a, b+1i) = (a+1i, b) + AB_i (a, b)
     // the contracted table was accumulated as [f][e] (the lanes' e contiguous);
     // the HRRs read [e][f]: transpose it into h1 (the bra HRR's first layer
@@ -312,7 +380,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
     double* h1 = w + d.o_h1;
     for (int x = tid; x < d.ne * d.nf; x += nt) {
       const int e = x / d.nf, f = x - e * d.nf;
-      h1[x] = acc[(size_t)f * d.ne + e];
+      h1[x] = CS > 1 ? __ldcg(acc + (size_t)f * d.ne + e) : acc[(size_t)f * d.ne + e];
     }
     __syncthreads();
     double* src = h1;
@@ -407,6 +475,75 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
     __syncthreads();
     }  // pass
     __syncthreads();
+}
+
+}  // namespace
+
+// CS > 1: launched in clusters of CS blocks (ib_generic_launch); the heavy
+// items are shared by a cluster, the light ones taken by single blocks.
+template <int MINB, int CS>
+__global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLaunch a, const IbGenWork wk, int sph,
+                                                                     double* __restrict__ scratch, long long slice) {
+  __shared__ IbGenShared sh;
+  __shared__ unsigned short ct[IB_GEN_NCT];
+  __shared__ unsigned short em[3 * IB_GEN_NCT];
+  __shared__ int ticket;
+  ib_gen_tables(ct, em);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  int crank = 0;
+  if constexpr (CS > 1) crank = (int)cg::this_cluster().block_rank();
+  double* __restrict__ w = scratch + (size_t)blockIdx.x * (size_t)slice;
+  double* __restrict__ wc = w - (size_t)crank * (size_t)slice;  // rank 0's slice (ranks are consecutive blocks)
+  int hb = 0, nh = 0, lb = 0, nl = 0;
+  if (wk.redo) {
+    nh = a.redo[0];
+    nl = a.redo[1];
+  } else {
+    if (wk.heavy_slot >= 0) {
+      hb = a.ranges[wk.heavy_slot];
+      nh = a.ranges[wk.heavy_slot + 1] - hb;
+    }
+    lb = a.ranges[wk.light_slot];
+    nl = a.ranges[wk.light_slot + 1] - lb;
+  }
+  // item t of the heavy list (t < nh), then of the light list
+  auto item = [&](int t) -> int {
+    if (t < nh) return wk.redo ? a.redo[2 + t] : hb + t;
+    t -= nh;
+    return wk.redo ? a.redo[2 + a.redo_cap - 1 - t] : lb + t;
+  };
+  if (!wk.tickets) {  // fixed order, one block per item
+    for (int t = blockIdx.x; t < nh + nl; t += gridDim.x) ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em);
+    return;
+  }
+  if constexpr (CS > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    for (;;) {  // every rank takes the same sequence of items and barriers
+      if (crank == 0 && tid == 0) ticket = atomicAdd(wk.tickets, 1);
+      cl.sync();
+      const int t = *cl.map_shared_rank(&ticket, 0);
+      cl.sync();  // read by every rank before rank 0 takes the next ticket
+      if (t >= nh) break;
+      ib_gen_item<CS>(a, item(t), sph, w, wc, slice, crank, sh, ct, em);
+    }
+  } else {
+    for (;;) {
+      if (tid == 0) ticket = atomicAdd(wk.tickets, 1);
+      __syncthreads();
+      const int t = ticket;
+      __syncthreads();
+      if (t >= nh) break;
+      ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em);
+    }
+  }
+  for (;;) {
+    if (tid == 0) ticket = atomicAdd(wk.tickets + 1, 1);
+    __syncthreads();
+    const int t = ticket;
+    __syncthreads();
+    if (t >= nl) break;
+    ib_gen_item<1>(a, item(nh + t), sph, w, w, slice, 0, sh, ct, em);
   }
 }
 
@@ -423,12 +560,76 @@ int ib_generic_bps() {
   return v;
 }
 
-cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, int range_slot, int sph, double* scratch,
-                              long long slice) {
-  switch (ib_generic_bps()) {
-    case 3: ib_eri_generic<3><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
-    case 4: ib_eri_generic<4><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
-    default: ib_eri_generic<2><<<grid, IB_GEN_BLOCK, 0, s>>>(a, range_slot, sph, scratch, slice); break;
+int ib_generic_split() {
+  static const int v = [] {
+    const char* e = getenv("INTCEPTION_B200_GENERIC_SPLIT");
+    const int x = e ? atoi(e) : 1;
+    return (x == 0 || x == 2) ? x : 1;
+  }();
+  return v;
+}
+
+namespace {
+
+// Clusters of the split kernel resident at once on the current device (cached
+// per device; 0 when the device cannot hold one).
+template <int MINB>
+int split_clusters_resident() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  int v = cache[dev].load();
+  if (v) return v - 1;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = IB_GEN_SPLIT;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(IB_GEN_SPLIT);
+  cfg.blockDim = dim3(IB_GEN_BLOCK);
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, ib_eri_generic<MINB, IB_GEN_SPLIT>, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;  // this launch without clusters; asked again next time
   }
+  cache[dev].store(n + 1);
+  return n;
+}
+
+template <int MINB>
+cudaError_t launch_bps(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph, double* scratch,
+                       long long slice) {
+  if (wk.tickets && wk.split) {
+    const int clusters = std::min(grid / IB_GEN_SPLIT, split_clusters_resident<MINB>());
+    if (clusters > 0) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = IB_GEN_SPLIT;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(clusters * IB_GEN_SPLIT);
+      cfg.blockDim = dim3(IB_GEN_BLOCK);
+      cfg.stream = s;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      return cudaLaunchKernelEx(&cfg, ib_eri_generic<MINB, IB_GEN_SPLIT>, a, wk, sph, scratch, slice);
+    }
+  }
+  ib_eri_generic<MINB, 1><<<grid, IB_GEN_BLOCK, 0, s>>>(a, wk, sph, scratch, slice);
   return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph,
+                              double* scratch, long long slice) {
+  switch (ib_generic_bps()) {
+    case 3: return launch_bps<3>(grid, s, a, wk, sph, scratch, slice);
+    case 4: return launch_bps<4>(grid, s, a, wk, sph, scratch, slice);
+    default: return launch_bps<2>(grid, s, a, wk, sph, scratch, slice);
+  }
 }

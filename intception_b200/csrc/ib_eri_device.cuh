@@ -49,7 +49,10 @@ struct IbLaunch {
   int* status;             // device error word (0 = ok)
   int* flags;              // per sorted item: bit 0 = FP32 result rejected (recompute in FP64),
                            // bit 1 = on the redo list
-  int* redo;               // [0]: count, [1..]: sorted items the generic kernel recomputes (HRR check)
+  int* redo;               // sorted items the generic kernel recomputes (HRR check): [0] heavy count,
+                           // [1] light count, then redo_cap slots, heavy items from the front,
+                           // light ones from the back
+  int redo_cap;            // slots of the redo list (the batch's item count)
   double hrr_tol;          // class kernels: largest accepted HRR rounding-error estimate (0: no check)
   int recheck;             // FP64 kernels: evaluate only items with flag bit 0
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
@@ -71,16 +74,49 @@ struct IbLaunch {
 // with 32 units a quartet that passes a tolerance t is within about 0.7 t.
 #define IB_HRR_ERR_COEF (32.0 * 1.1102230246251565e-16)
 
-// Puts sorted item p on the generic kernel's redo list once (flag bit 1).
+// The generic kernel splits a quartet of at least IB_GEN_SPLIT_MIN primitive
+// quartets ("heavy") over the IB_GEN_SPLIT blocks of a thread-block cluster.
+#ifndef IB_GEN_SPLIT
+#define IB_GEN_SPLIT 8
+#endif
+#define IB_GEN_SPLIT_MIN 128
+
+// Puts sorted item p on the generic kernel's redo list once (flag bit 1):
+// heavy quartets at the front of the list, light ones at the back.
 __device__ __forceinline__ void ib_redo_push(const IbLaunch& a, int p) {
-  if (!(atomicOr(a.flags + p, 2) & 2)) a.redo[1 + atomicAdd(a.redo, 1)] = p;
+  if (atomicOr(a.flags + p, 2) & 2) return;
+  const int* s = a.items[p].s;
+  const int np = a.shell_k[s[0]] * a.shell_k[s[1]] * a.shell_k[s[2]] * a.shell_k[s[3]];
+  if (np >= IB_GEN_SPLIT_MIN)
+    a.redo[2 + atomicAdd(a.redo, 1)] = p;
+  else
+    a.redo[2 + a.redo_cap - 1 - atomicAdd(a.redo + 1, 1)] = p;
 }
 
-// The generic block-per-quartet kernel (eri_generic.cu): blocks per SM it runs
-// with, and its launch (range_slot < 0: the redo list).
+// Items of one generic-kernel launch.  Range form (redo 0): heavy items
+// ranges[heavy_slot] .. ranges[heavy_slot + 1] (heavy_slot < 0: none), light
+// ones ranges[light_slot] .. ranges[light_slot + 1].  List form (redo 1): the
+// launch's redo list (IbLaunch::redo).  tickets: two counters (heavy, light)
+// zeroed before the launch; the blocks take items in list order from them.
+// Null tickets: every item on one block, block b taking items b, b + grid, ...
+// split: with tickets, heavy items go to clusters (0: one block each as well).
+struct IbGenWork {
+  int heavy_slot, light_slot, redo;
+  int* tickets;
+  int split;
+};
+
+// Which generic launches split heavy quartets over clusters:
+// INTCEPTION_B200_GENERIC_SPLIT = 0 none, 1 the redo lists (the default), 2
+// the redo lists and the batch's generic range.
+int ib_generic_split();
+
+// The generic kernel (eri_generic.cu): blocks per SM it runs with, and its
+// launch.  With tickets, heavy items go to clusters of IB_GEN_SPLIT blocks
+// (the grid is rounded down to whole clusters that fit the GPU at once).
 int ib_generic_bps();
-cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, int range_slot, int sph, double* scratch,
-                              long long slice);
+cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph,
+                              double* scratch, long long slice);
 
 // Smallest primitive exponent of shell s.
 __device__ __forceinline__ double ib_min_exp(const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,

@@ -208,7 +208,9 @@ extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* ba
   a.status = d->status;
   a.slice_boost = 1;
   const long long grid = std::min<long long>({(long long)nq, (long long)ib_generic_bps() * d->nsm, fit});
-  const cudaError_t e = ib_generic_launch((int)grid, s, a, kNoallocSlot, spherical ? 1 : 0, d->scratch, slice);
+  // one block per quartet in a fixed order (no tickets: nothing to zero, no cluster)
+  const cudaError_t e =
+      ib_generic_launch((int)grid, s, a, IbGenWork{-1, kNoallocSlot, 0, nullptr}, spherical ? 1 : 0, d->scratch, slice);
   if (e != cudaSuccess)
     return ib_runtime_set_status(IB_ERR_CUDA, (std::string("eri_batch_noalloc: ") + cudaGetErrorString(e)).c_str());
   return ib_runtime_set_status(IB_OK, "");

@@ -43,13 +43,17 @@ namespace {
 
 constexpr int kNSideMax = 64;                   // side streams for concurrent class kernels (upper limit)
 constexpr int kSlotFp32 = 2 * IB_NCLASS;        // ranges offset of the FP32 copies
-constexpr int kSlotGeneric = 4 * IB_NCLASS;     // [begin, end) of the generic (non-emitted) quartets
+constexpr int kSlotGenHeavy = 4 * IB_NCLASS;    // [begin, end) of the generic kernel's heavy quartets
 constexpr int kSlotSkip = 4 * IB_NCLASS + 2;    // [begin, end) of the screened-out quartets
-constexpr int kNRanges = 4 * IB_NCLASS + 4;
+constexpr int kSlotGenLight = 4 * IB_NCLASS + 4;  // [begin, end) of the generic kernel's light quartets
+constexpr int kNRanges = 4 * IB_NCLASS + 6;
 constexpr int kNCounters = 3 * IB_NCLASS;      // quartet counters: FP64 pass, FP32 pass, FP64 recheck pass
-constexpr int kKeyBits = 16;                    // skip(1) generic(1) fp32(1) class(9) work(4): two radix passes
-constexpr size_t kScratchCap = size_t(4) << 30;
-constexpr int kRedoGroups = 4;  // redo lists of an l >= 3 batch (dispatch)  // bytes of generic-kernel scratch at most
+// sort key: skip(1) generic(1) fp32(1) class(9) work(4), two radix passes; a
+// generic quartet's class and work bits hold light(1) and its cost code (8)
+constexpr int kKeyBits = 16;
+constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
+constexpr int kRedoGroups = 4;  // redo lists of an l >= 3 batch (dispatch)
+constexpr int kTickets = 2 * (1 + kRedoGroups);  // generic-kernel ticket pairs: the range launch, each redo list
 
 thread_local int tl_status = IB_OK;
 thread_local std::string tl_msg;
@@ -127,8 +131,9 @@ struct Context {
   DevBuf sw_quartets, sw_sizes, sw_off, sw_tmp, sw_blocks;  // Schwarz-bound work buffers
   DevBuf flags;    // per sorted item of the last batch: FP32 rejection (bit 0), on the redo list (bit 1)
   int flags_nq = 0;  // its quartet count (flags beyond it are stale)
-  DevBuf redo;     // the last batch's redo lists (redo_groups of them, redo_stride ints apart): count, then sorted items
-  int redo_groups = 1, redo_stride = 1;
+  DevBuf redo;     // the last batch's redo lists (redo_groups of them, redo_stride ints apart; IbLaunch::redo)
+  int redo_groups = 1, redo_stride = 2;
+  DevBuf tickets;  // kTickets ints: the generic kernel's ticket pairs (zeroed by every dispatch)
   DevBuf kind;                                              // per class: 0 generic, 1 FP64, 2 FP64+FP32
   int kind_h[IB_NCLASS] = {};  // host copy of kind: 2 where the class has FP32 kernels and the FP32 tier uses them
   DevBuf d_stage, d_cart, d_res;
@@ -215,9 +220,19 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
     const int gen = (!skip && (k == 0 || rv == 2)) ? 1 : 0;  // rv 2 only when route_rev
     const int fp32 = (!gen && !skip && mixed && k == 2 && bounds[q] < thr) ? 1 : 0;
     // primitive quartet counts (powers of two) descending inside a class: the
-    // longest quartets start first
-    keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | (unsigned(cid) << 4) |
-              unsigned(15 - work);
+    // longest quartets start first.  The generic kernel's quartets: heavy ones
+    // (split over a cluster) first, then light ones, each by a cost estimate
+    // descending (primitive quartets x (contracted [e0|f0] elements + 64), in
+    // quarter powers of two), whatever their class
+    unsigned low = (unsigned(cid) << 4) | unsigned(15 - work);
+    if (gen) {
+      const long long ne = ib_ncum(l[0] + l[1]) - ib_ncum(l[0] - 1), nf = ib_ncum(l[2] + l[3]) - ib_ncum(l[2] - 1);
+      const unsigned long long cost = (unsigned long long)max(nprim, 1) * (unsigned long long)(ne * nf + 64);
+      const int e2 = 63 - __clzll((long long)cost);  // >= 6
+      const int qc = min(255, 4 * e2 + (int)((cost >> (e2 - 2)) & 3));
+      low = (unsigned(nprim < IB_GEN_SPLIT_MIN) << 12) | (unsigned(255 - qc) << 4);
+    }
+    keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | low;
     vals[q] = q;
   }
 }
@@ -259,9 +274,12 @@ __global__ void ib_build_items(const unsigned* __restrict__ keys, const int* __r
       if (next < 0) ranges[kSlotSkip + 1] = p + 1;
       continue;
     }
-    if ((slot >> 10) & 1) {  // no unrolled kernel: one contiguous range for the generic kernel
-      if (prev < 0 || !((prev >> 10) & 1)) ranges[kSlotGeneric] = p;
-      if (next < 0 || ((next >> 10) & 3) != 1) ranges[kSlotGeneric + 1] = p + 1;
+    if ((slot >> 10) & 1) {  // the generic kernel's quartets: a heavy range, then a light one
+      // 0: not the generic kernel's, 1: heavy, 2: light
+      auto state = [](int sl) { return (sl < 0 || (sl >> 10) != 1) ? 0 : 1 + ((sl >> 8) & 1); };
+      const int st_p = state(slot), rs = st_p == 1 ? kSlotGenHeavy : kSlotGenLight;
+      if (state(prev) != st_p) ranges[rs] = p;
+      if (state(next) != st_p) ranges[rs + 1] = p + 1;
       continue;
     }
     const int cid = slot & 511, fp32 = (slot >> 9) & 1;
@@ -581,21 +599,26 @@ int class_lmax(int cid) {
 }
 
 // The generic kernel over the redo list of a (on stream s, after the class
-// kernels that fill it).
-cudaError_t redo_launch(Context* c, cudaStream_t s, const IbLaunch& a, bool sph, int lmax) {
+// kernels that fill it); tickets: a zeroed pair (null: fixed order, no cluster).
+cudaError_t redo_launch(Context* c, cudaStream_t s, const IbLaunch& a, bool sph, int lmax, int* tickets) {
   const long long slice = generic_slice(lmax);
   long long nblk = std::min<long long>((long long)ib_generic_bps() * c->nsm,
                                       (long long)(kScratchCap / (slice * sizeof(double))));
   nblk = std::max<long long>(nblk, 1);
   cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
   if (e != cudaSuccess) return e;
-  return ib_generic_launch((int)nblk, s, a, -1, sph ? 1 : 0, c->scratch.as<double>(), slice);
+  const IbGenWork wk{-1, 0, 1, tickets, ib_generic_split() >= 1};
+  return ib_generic_launch((int)nblk, s, a, wk, sph ? 1 : 0, c->scratch.as<double>(), slice);
 }
 
 // Launch the emitted kernels for the given variants and the generic kernel;
 // items/ranges already on the device.  Returns the number of kernels launched.
 int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, bool fp32_present, bool sph,
              int lmax, int* nlaunch, const ZeroFill* zf = nullptr) {
+  // the generic kernel's tickets: pair 0 for its range launch, pair 1 + g for redo list g
+  IB_CUDA(c->tickets.ensure(kTickets * sizeof(int)));
+  IB_CUDA(cudaMemsetAsync(c->tickets.p, 0, kTickets * sizeof(int), s));
+  int* const tk = c->tickets.as<int>();
   IB_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < c->nside; ++i) IB_CUDA(cudaStreamWaitEvent(c->side[i], c->fork, 0));
   int k = 0;
@@ -625,8 +648,11 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   auto launch_generic = [&]() -> cudaError_t {
     cudaError_t e = c->scratch.ensure((size_t)(gfull + (G > 1 ? G * ggroup : 0)) * gslice * sizeof(double));
     if (e != cudaSuccess) return e;
-    e = ib_generic_launch((int)gfull, c->side[k % c->nside], a, kSlotGeneric, sph ? 1 : 0, c->scratch.as<double>(),
-                          gslice);
+    // a batch's generic range is long enough to keep every block busy: its
+    // heavy quartets stay on single blocks unless INTCEPTION_B200_GENERIC_SPLIT=2
+    e = ib_generic_launch((int)gfull, c->side[k % c->nside], a,
+                          IbGenWork{kSlotGenHeavy, kSlotGenLight, 0, tk, ib_generic_split() >= 2},
+                          sph ? 1 : 0, c->scratch.as<double>(), gslice);
     ++k;
     return e;
   };
@@ -672,7 +698,8 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
         if (j != g) IB_CUDA(cudaStreamWaitEvent(c->side[g], c->join[j], 0));
       IbLaunch ag = a;
       ag.redo = a.redo + (size_t)g * c->redo_stride;
-      IB_CUDA(ib_generic_launch((int)ggroup, c->side[g], ag, -1, sph ? 1 : 0,
+      const IbGenWork wk{-1, 0, 1, tk + 2 * (1 + g), ib_generic_split() >= 1};
+      IB_CUDA(ib_generic_launch((int)ggroup, c->side[g], ag, wk, sph ? 1 : 0,
                                 c->scratch.as<double>() + (size_t)(gfull + g * ggroup) * gslice, gslice));
       ++k;
     }
@@ -683,7 +710,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   }
   // one redo list: after every class kernel (an empty list returns at once)
   if (redo_on && G == 1) {
-    IB_CUDA(redo_launch(c, s, a, sph, lmax));
+    IB_CUDA(redo_launch(c, s, a, sph, lmax, tk + 2));
     ++k;
   }
   *nlaunch += k;
@@ -844,8 +871,8 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     hrg[2 * cidx] = 0;
     hrg[2 * cidx + 1] = nblk;
   } else {
-    hrg[kSlotGeneric] = 0;
-    hrg[kSlotGeneric + 1] = nblk;
+    hrg[kSlotGenLight] = 0;  // one block per item (no cluster split in the drop-in)
+    hrg[kSlotGenLight + 1] = nblk;
   }
   for (int i = 0; i < 4; ++i)
     if (sph) std::memcpy(h + o_T[i], sh[i].T, tsize[i] * sizeof(double));
@@ -873,24 +900,27 @@ int dropin(DropShell* sh, bool sph, double* output_array) {
     IB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
     IB_CUDA(c->flags.ensure((size_t)nblk * sizeof(int)));
     IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nblk * sizeof(int), s));
-    IB_CUDA(c->redo.ensure((size_t)(nblk + 1) * sizeof(int)));
-    IB_CUDA(cudaMemsetAsync(c->redo.p, 0, sizeof(int), s));
+    IB_CUDA(c->redo.ensure((size_t)(nblk + 2) * sizeof(int)));
+    IB_CUDA(cudaMemsetAsync(c->redo.p, 0, 2 * sizeof(int), s));
     c->redo_groups = 1;
-    c->redo_stride = nblk + 1;
+    c->redo_stride = nblk + 2;
     c->flags_nq = nblk;
     a.flags = c->flags.as<int>();
     a.redo = c->redo.as<int>();
+    a.redo_cap = nblk;
     a.hrr_tol = c->hrr_tol;
     c->table[cidx].launch(vt, grid, s, a);
     if (a.hrr_tol > 0.0)
-      IB_CUDA(redo_launch(c, s, a, false, std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l))));
+      IB_CUDA(redo_launch(c, s, a, false, std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)),
+                          nullptr));
   } else {
     const long long slice = generic_slice(std::max(std::max(sh[0].l, sh[1].l), std::max(sh[2].l, sh[3].l)));
     long long nb = std::min<long long>({(long long)nblk, (long long)ib_generic_bps() * c->nsm,
                                         (long long)(kScratchCap / (slice * sizeof(double)))});
     nb = std::max<long long>(nb, 1);
     IB_CUDA(c->scratch.ensure((size_t)nb * slice * sizeof(double)));
-    IB_CUDA(ib_generic_launch((int)nb, s, a, kSlotGeneric, 0, c->scratch.as<double>(), slice));
+    IB_CUDA(ib_generic_launch((int)nb, s, a, IbGenWork{-1, kSlotGenLight, 0, nullptr}, 0, c->scratch.as<double>(),
+                              slice));
   }
   IB_CUDA(cudaGetLastError());
   IbXform x;
@@ -1091,13 +1121,14 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
   IB_CUDA(cudaMemsetAsync(c->flags.p, 0, (size_t)nq * sizeof(int), s));
   // l >= 3 batches: four redo lists, one per group of side streams (dispatch)
   c->redo_groups = (basis->lmax >= 3 && c->hrr_tol > 0.0) ? kRedoGroups : 1;
-  c->redo_stride = nq + 1;
-  IB_CUDA(c->redo.ensure((size_t)c->redo_groups * (nq + 1) * sizeof(int)));
+  c->redo_stride = nq + 2;
+  IB_CUDA(c->redo.ensure((size_t)c->redo_groups * (nq + 2) * sizeof(int)));
   for (int g = 0; g < c->redo_groups; ++g)
-    IB_CUDA(cudaMemsetAsync(c->redo.as<int>() + (size_t)g * (nq + 1), 0, sizeof(int), s));
+    IB_CUDA(cudaMemsetAsync(c->redo.as<int>() + (size_t)g * (nq + 2), 0, 2 * sizeof(int), s));
   c->flags_nq = nq;
   a.flags = c->flags.as<int>();
   a.redo = c->redo.as<int>();
+  a.redo_cap = nq;
   a.hrr_tol = c->hrr_tol;
   if (precision == IB_PREC_MIXED) a.mixed_tol = mixed_tol;
   const ZeroFill zf = {c->keys.as<unsigned>(), nq, quartets, basis->shell_l, out_off};
@@ -1410,9 +1441,9 @@ int intception_b200_last_hrr_redo(void) {
   IB_CUDA(cudaDeviceSynchronize());
   int total = 0;
   for (int g = 0; g < c->redo_groups; ++g) {
-    int h = 0;
-    IB_CUDA(cudaMemcpy(&h, c->redo.as<int>() + (size_t)g * c->redo_stride, sizeof(int), cudaMemcpyDeviceToHost));
-    total += h;
+    int h[2] = {0, 0};  // heavy and light counts
+    IB_CUDA(cudaMemcpy(h, c->redo.as<int>() + (size_t)g * c->redo_stride, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    total += h[0] + h[1];
   }
   return total;
 }

@@ -315,6 +315,23 @@ def _quad_one(args):
     return loader.oracle_batch_quad(b.subset(np.array([q])), T)
 
 
+def generic_split():
+    """generic_split_sph.npz: l 3..4 quartets (exponents log-uniform in
+    [0.1, 1e3], centres in a 3-bohr cube), 16 with K = 4 on every shell (256
+    primitive quartets each: the generic kernel splits those of its classes
+    over a cluster) and 16 with K drawn from 1, 2, 4 (light and heavy mixed).
+    out holds exact values (the C restatement in binary128); the restatement
+    in double is off by up to 7.5e-12 on them (on one (fg|gf) quartet)."""
+    T = basis.sph_matrices(6)
+    heavy = basis.independent_quartet_batch(11, 16, [3, 4], [4], 0.1, 1.0e3, 3.0, True)
+    mixed_k = basis.independent_quartet_batch(11, 16, [3, 4], [1, 2, 4], 0.1, 1.0e3, 3.0, True)
+    mb = compact_batch([(heavy, q) for q in range(heavy.nq)] + [(mixed_k, q) for q in range(mixed_k.nq)])
+    from multiprocessing import Pool
+    with Pool(os.cpu_count() or 1) as p:
+        parts = p.map(_quad_one, [(mb, q, T) for q in range(mb.nq)], chunksize=1)
+    save_batch('generic_split_sph', mb, T, np.concatenate(parts))
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['twoidx']:
         twoidx()
@@ -322,8 +339,11 @@ if __name__ == '__main__':
         c1()
     elif sys.argv[1:] == ['mixed']:
         mixed()
+    elif sys.argv[1:] == ['generic_split']:
+        generic_split()
     else:
         main()
         twoidx()
         c1()
         mixed()
+        generic_split()

@@ -130,3 +130,17 @@ def test_mixed_contraction_fixture_exact_values():
     # the reference's double recurrences (bra HRR in the caller's shell order)
     # miss the exact values by more than the parity bar on some of these quartets
     assert np.abs(ref - exact).max() > tolerance(exact)
+
+
+def test_generic_split_fixture_exact_values():
+    """The generic-split fixture's exact values re-evaluated (its two cheapest
+    quartets), and the double restatement against them: close, but off by
+    more than the parity bar on its heavy quartets."""
+    b, T, exact = load_batch('generic_split_sph')
+    sizes = basis.block_sizes(b.shell_l, b.quartets, True)
+    cost = [int(np.prod(b.shell_k[s])) for s in b.quartets]
+    for q in np.argsort(cost, kind='stable')[:2]:
+        out = loader.oracle_batch_quad(b.subset(np.array([q])), T)
+        assert np.array_equal(out, exact[b.out_off[q]:b.out_off[q] + sizes[q]])
+    err = np.abs(loader.oracle_batch(b, T) - exact).max()
+    assert tolerance(exact) < err < 1e-10
