@@ -21,13 +21,14 @@
 // One block walks a quartet's primitive quartets one after the other, so a
 // quartet of K = 8 shells alone would outlast a whole batch.  Heavy quartets
 // (IB_GEN_SPLIT_MIN primitive quartets or more) therefore go to a cluster of
-// IB_GEN_SPLIT blocks: block r of the cluster takes primitive quartets r, r +
-// IB_GEN_SPLIT, ... of each pass into its own contracted table; after a
-// cluster barrier the blocks sum the tables in rank order (each a share of the
-// elements) into rank 0's, which then runs the HRRs and stores the block.  The
-// sum order is fixed, so the results do not depend on the timing.  Clusters
-// take heavy quartets from a ticket counter in list order (heaviest first in a
-// range), then every block takes light quartets alone from a second one.
+// CS blocks (2 or 4, chosen per launch): each pass numbers its live primitive
+// quartets in order and block r of the cluster adds those numbered r, r + CS,
+// ... into its own contracted table; after a cluster barrier the blocks sum the tables
+// in rank order (each a share of the elements) into rank 0's, which then runs
+// the HRRs and stores the block.  The sum order is fixed, so the results do
+// not depend on the timing.  Clusters take heavy quartets from a ticket
+// counter in list order (heaviest first in a range), then every block takes
+// light quartets alone from a second one.
 //
 // Scratch slice layout (doubles), sizes from ib_generic_dims():
 //   acc  [nf * ne]                 contracted [e0|f0] stored [f][e], e in [la,la+lb], f in [lc,lc+ld]
@@ -563,17 +564,17 @@ int ib_generic_bps() {
 int ib_generic_split() {
   static const int v = [] {
     const char* e = getenv("INTCEPTION_B200_GENERIC_SPLIT");
-    const int x = e ? atoi(e) : 1;
-    return (x == 0 || x == 2) ? x : 1;
+    const int x = e ? atoi(e) : 2;
+    return (x == 0 || x == 1) ? x : 2;
   }();
   return v;
 }
 
 namespace {
 
-// Clusters of the split kernel resident at once on the current device (cached
-// per device; 0 when the device cannot hold one).
-template <int MINB>
+// Clusters of CS blocks of the split kernel resident at once on the current
+// device (cached per device; 0 when the device cannot hold one).
+template <int MINB, int CS>
 int split_clusters_resident() {
   static std::atomic<int> cache[64];
   int dev = 0;
@@ -583,15 +584,15 @@ int split_clusters_resident() {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = IB_GEN_SPLIT;
+  at[0].val.clusterDim.x = CS;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
-  cfg.gridDim = dim3(IB_GEN_SPLIT);
+  cfg.gridDim = dim3(CS);
   cfg.blockDim = dim3(IB_GEN_BLOCK);
   cfg.attrs = at;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, ib_eri_generic<MINB, IB_GEN_SPLIT>, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, ib_eri_generic<MINB, CS>, &cfg) != cudaSuccess) {
     (void)cudaGetLastError();
     return 0;  // this launch without clusters; asked again next time
   }
@@ -599,26 +600,35 @@ int split_clusters_resident() {
   return n;
 }
 
+// The launch with clusters of CS blocks (as many as fit the grid and the GPU
+// at once); without clusters when none fits.
+template <int MINB, int CS>
+cudaError_t launch_split(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph,
+                         double* scratch, long long slice) {
+  const int clusters = std::min(grid / CS, split_clusters_resident<MINB, CS>());
+  if (clusters > 0) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CS;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(clusters * CS);
+    cfg.blockDim = dim3(IB_GEN_BLOCK);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, ib_eri_generic<MINB, CS>, a, wk, sph, scratch, slice);
+  }
+  ib_eri_generic<MINB, 1><<<grid, IB_GEN_BLOCK, 0, s>>>(a, wk, sph, scratch, slice);
+  return cudaGetLastError();
+}
+
 template <int MINB>
 cudaError_t launch_bps(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph, double* scratch,
                        long long slice) {
-  if (wk.tickets && wk.split) {
-    const int clusters = std::min(grid / IB_GEN_SPLIT, split_clusters_resident<MINB>());
-    if (clusters > 0) {
-      cudaLaunchConfig_t cfg = {};
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = IB_GEN_SPLIT;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      cfg.gridDim = dim3(clusters * IB_GEN_SPLIT);
-      cfg.blockDim = dim3(IB_GEN_BLOCK);
-      cfg.stream = s;
-      cfg.attrs = at;
-      cfg.numAttrs = 1;
-      return cudaLaunchKernelEx(&cfg, ib_eri_generic<MINB, IB_GEN_SPLIT>, a, wk, sph, scratch, slice);
-    }
-  }
+  if (wk.tickets && wk.split >= 4) return launch_split<MINB, 4>(grid, s, a, wk, sph, scratch, slice);
+  if (wk.tickets && wk.split >= 2) return launch_split<MINB, 2>(grid, s, a, wk, sph, scratch, slice);
   ib_eri_generic<MINB, 1><<<grid, IB_GEN_BLOCK, 0, s>>>(a, wk, sph, scratch, slice);
   return cudaGetLastError();
 }

@@ -75,10 +75,8 @@ struct IbLaunch {
 #define IB_HRR_ERR_COEF (32.0 * 1.1102230246251565e-16)
 
 // The generic kernel splits a quartet of at least IB_GEN_SPLIT_MIN primitive
-// quartets ("heavy") over the IB_GEN_SPLIT blocks of a thread-block cluster.
-#ifndef IB_GEN_SPLIT
-#define IB_GEN_SPLIT 8
-#endif
+// quartets ("heavy") over the blocks of a thread-block cluster (2 or 4, the
+// launch's IbGenWork::split).
 #define IB_GEN_SPLIT_MIN 128
 
 // Puts sorted item p on the generic kernel's redo list once (flag bit 1):
@@ -99,7 +97,8 @@ __device__ __forceinline__ void ib_redo_push(const IbLaunch& a, int p) {
 // launch's redo list (IbLaunch::redo).  tickets: two counters (heavy, light)
 // zeroed before the launch; the blocks take items in list order from them.
 // Null tickets: every item on one block, block b taking items b, b + grid, ...
-// split: with tickets, heavy items go to clusters (0: one block each as well).
+// split: with tickets, heavy items go to clusters of this many blocks (2 or 4;
+// 0: one block each as well).
 struct IbGenWork {
   int heavy_slot, light_slot, redo;
   int* tickets;
@@ -107,13 +106,13 @@ struct IbGenWork {
 };
 
 // Which generic launches split heavy quartets over clusters:
-// INTCEPTION_B200_GENERIC_SPLIT = 0 none, 1 the redo lists (the default), 2
-// the redo lists and the batch's generic range.
+// INTCEPTION_B200_GENERIC_SPLIT = 0 none, 1 the redo lists, 2 the redo lists
+// and the batch's generic range (the default).
 int ib_generic_split();
 
 // The generic kernel (eri_generic.cu): blocks per SM it runs with, and its
-// launch.  With tickets, heavy items go to clusters of IB_GEN_SPLIT blocks
-// (the grid is rounded down to whole clusters that fit the GPU at once).
+// launch.  With tickets and wk.split, heavy items go to clusters of wk.split
+// blocks (the grid is rounded down to whole clusters that fit the GPU at once).
 int ib_generic_bps();
 cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, const IbGenWork& wk, int sph,
                               double* scratch, long long slice);

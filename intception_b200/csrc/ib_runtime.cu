@@ -54,6 +54,12 @@ constexpr int kKeyBits = 16;
 constexpr size_t kScratchCap = size_t(4) << 30;  // bytes of generic-kernel scratch at most
 constexpr int kRedoGroups = 4;  // redo lists of an l >= 3 batch (dispatch)
 constexpr int kTickets = 2 * (1 + kRedoGroups);  // generic-kernel ticket pairs: the range launch, each redo list
+// blocks per cluster sharing a heavy generic quartet: a redo list is short and
+// its end waits for its heaviest quartets, so 4; a batch's generic range keeps
+// every block busy, and rank 0's HRRs idle fewer ranks with 2 (l <= 4 sample,
+// 2 000 quartets of one class: (gg|gg) 878 against 1 038 ns per live primitive
+// quartet with 2 and 4, the redo-heavy (gg|ff) 387 against 325)
+constexpr int kSplitRedo = 4, kSplitRange = 2;
 
 thread_local int tl_status = IB_OK;
 thread_local std::string tl_msg;
@@ -607,7 +613,7 @@ cudaError_t redo_launch(Context* c, cudaStream_t s, const IbLaunch& a, bool sph,
   nblk = std::max<long long>(nblk, 1);
   cudaError_t e = c->scratch.ensure((size_t)nblk * slice * sizeof(double));
   if (e != cudaSuccess) return e;
-  const IbGenWork wk{-1, 0, 1, tickets, ib_generic_split() >= 1};
+  const IbGenWork wk{-1, 0, 1, tickets, ib_generic_split() >= 1 ? kSplitRedo : 0};
   return ib_generic_launch((int)nblk, s, a, wk, sph ? 1 : 0, c->scratch.as<double>(), slice);
 }
 
@@ -648,10 +654,9 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
   auto launch_generic = [&]() -> cudaError_t {
     cudaError_t e = c->scratch.ensure((size_t)(gfull + (G > 1 ? G * ggroup : 0)) * gslice * sizeof(double));
     if (e != cudaSuccess) return e;
-    // a batch's generic range is long enough to keep every block busy: its
-    // heavy quartets stay on single blocks unless INTCEPTION_B200_GENERIC_SPLIT=2
+    // heavy quartets of the range over clusters too (INTCEPTION_B200_GENERIC_SPLIT 2)
     e = ib_generic_launch((int)gfull, c->side[k % c->nside], a,
-                          IbGenWork{kSlotGenHeavy, kSlotGenLight, 0, tk, ib_generic_split() >= 2},
+                          IbGenWork{kSlotGenHeavy, kSlotGenLight, 0, tk, ib_generic_split() >= 2 ? kSplitRange : 0},
                           sph ? 1 : 0, c->scratch.as<double>(), gslice);
     ++k;
     return e;
@@ -698,7 +703,7 @@ int dispatch(Context* c, cudaStream_t s, const IbLaunch& a, bool fp64_present, b
         if (j != g) IB_CUDA(cudaStreamWaitEvent(c->side[g], c->join[j], 0));
       IbLaunch ag = a;
       ag.redo = a.redo + (size_t)g * c->redo_stride;
-      const IbGenWork wk{-1, 0, 1, tk + 2 * (1 + g), ib_generic_split() >= 1};
+      const IbGenWork wk{-1, 0, 1, tk + 2 * (1 + g), ib_generic_split() >= 1 ? kSplitRedo : 0};
       IB_CUDA(ib_generic_launch((int)ggroup, c->side[g], ag, wk, sph ? 1 : 0,
                                 c->scratch.as<double>() + (size_t)(gfull + g * ggroup) * gslice, gslice));
       ++k;

@@ -35,10 +35,17 @@ def test_heavy_generic_quartets_match_exact_values():
 
 
 def test_heavy_generic_quartets_are_reproducible():
-    # wide exponents: some quartets of unrolled classes also go to the redo list
+    # the generic range: (gg|gg) quartets of K 6..8, split over 2-block clusters
     b = basis.independent_quartet_batch(12, 64, [4], [6, 7, 8], 0.05, 1.0e4, 5.0, True)
+    assert np.array_equal(_run(b), _run(b))
+
+
+def test_split_redo_lists_are_reproducible():
+    # the redo lists (4-block clusters): quartets of unrolled classes the HRR check hands over
+    b, _, _ = load_batch('mixed_contraction_sph')
     first = _run(b)
     redo = eri.last_hrr_redo()
+    assert redo > 0
     second = _run(b)
     assert eri.last_hrr_redo() == redo
     assert np.array_equal(first, second)
