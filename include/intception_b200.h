@@ -217,6 +217,14 @@ int intception_b200_last_fp32_rejections(void);
  * (intception_b200_set_hrr_tol).  New: the reference has no counterpart. */
 int intception_b200_last_hrr_redo(void);
 
+/* Blocks of the generic kernel's launch on the current device when heavy
+ * quartets are split over thread-block clusters of cluster_size blocks (2 or
+ * 4): whole clusters that fit the GPU at once, at most the launch's grid of
+ * resident blocks per SM x SMs; cluster_size 1 gives that grid (no clusters).
+ * Any other size, or no CUDA device, returns -1.  New: the reference has no
+ * counterpart. */
+int intception_b200_generic_grid(int cluster_size);
+
 /* Tuning: at most cap lane groups (a power of two; 0 = no cap) share one
  * contracted quartet in the kernel of canonical class cid (cid < 0: every
  * class).  The kernels spread a quartet's primitive quartets over more groups

@@ -107,24 +107,28 @@ struct IbGenShared {
 
 // ct[cum]: the Cartesian exponents of every cumulative component index;
 // em[i][e]: the index of e - 1_i (low 9 bits) and the exponent of e along i
-// (above them; 0: no such component).
-__device__ __forceinline__ void ib_gen_tables(unsigned short* ct, unsigned short* em) {
+// (above them; 0: no such component); eu[i][e]: the index of e + 1_i (0 for
+// the top level, whose e + 1_i no recurrence reads).  The recurrences look
+// their neighbours up here: decoding them into small arrays indexed by i put
+// those arrays in local memory, written and read for every element.
+__device__ __forceinline__ void ib_gen_tables(unsigned short* ct, unsigned short* em, unsigned short* eu) {
   for (int t = threadIdx.x; t < IB_GEN_NCT; t += blockDim.x) {
     int x, y, z;
     ib_comp_of(t, x, y, z);
     ct[t] = (unsigned short)(x | (y << 5) | (z << 10));
-    const int c[3] = {x, y, z};
-    for (int i = 0; i < 3; ++i) {
-      if (c[i] == 0) {
-        em[i * IB_GEN_NCT + t] = 0;
-        continue;
-      }
-      int v[3] = {x, y, z};
-      v[i] -= 1;
-      em[i * IB_GEN_NCT + t] = (unsigned short)(ib_cidx(v[0], v[1], v[2]) | (c[i] << 9));
-    }
+    const bool top = x + y + z == 2 * IB_LMAX;
+    em[t] = x ? (unsigned short)(ib_cidx(x - 1, y, z) | (x << 9)) : 0;
+    em[IB_GEN_NCT + t] = y ? (unsigned short)(ib_cidx(x, y - 1, z) | (y << 9)) : 0;
+    em[2 * IB_GEN_NCT + t] = z ? (unsigned short)(ib_cidx(x, y, z - 1) | (z << 9)) : 0;
+    eu[t] = top ? 0 : (unsigned short)ib_cidx(x + 1, y, z);
+    eu[IB_GEN_NCT + t] = top ? 0 : (unsigned short)ib_cidx(x, y + 1, z);
+    eu[2 * IB_GEN_NCT + t] = top ? 0 : (unsigned short)ib_cidx(x, y, z + 1);
   }
 }
+
+// Direction of the recurrence that builds component (x, y, z): the first
+// nonzero exponent.
+__device__ __forceinline__ int ib_gen_dir(int x, int y) { return x > 0 ? 0 : (y > 0 ? 1 : 2); }
 
 // One contracted quartet, sorted item p, in the block's scratch slice w.
 // CS > 1: this block is rank crank of the CS blocks of a cluster that evaluate
@@ -134,7 +138,8 @@ template <int CS>
 __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, double* __restrict__ w,
                                             double* __restrict__ wc, long long slice, int crank, IbGenShared& sh,
                                             const unsigned short* __restrict__ ct,
-                                            const unsigned short* __restrict__ em) {
+                                            const unsigned short* __restrict__ em,
+                                            const unsigned short* __restrict__ eu) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) {
@@ -293,15 +298,12 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
           const int m = idx / nce, e = ib_ncum(le - 1) + idx % nce;
           int ex, ey, ez;
           ib_ct_get(ct, e, ex, ey, ez);
-          int ev[3] = {ex, ey, ez};
-          const int i = ev[0] > 0 ? 0 : (ev[1] > 0 ? 1 : 2);
-          ev[i] -= 1;
-          const int e1 = ib_cidx(ev[0], ev[1], ev[2]);
+          const int i = ib_gen_dir(ex, ey);
+          const unsigned t1 = em[i * IB_GEN_NCT + e];
+          const int e1 = t1 & 511, n = (int)(t1 >> 9) - 1;  // e - 1_i, its exponent along i
           double v = sh.PA[i] * bra[m * d.ncumE + e1] + sh.WP[i] * bra[(m + 1) * d.ncumE + e1];
-          if (ev[i] > 0) {
-            const int n = ev[i];
-            ev[i] -= 1;
-            const int e2 = ib_cidx(ev[0], ev[1], ev[2]);
+          if (n > 0) {
+            const int e2 = em[i * IB_GEN_NCT + e1] & 511;  // e - 2_i
             v += n * sh.o2z * (bra[m * d.ncumE + e2] - sh.roz * bra[(m + 1) * d.ncumE + e2]);
           }
           bra[m * d.ncumE + e] = v;
@@ -322,16 +324,12 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
           const int m = row / ncf, fc = row - m * ncf;
           int fx, fy, fz;
           ib_ct_get(ct, ib_ncum(lf - 1) + fc, fx, fy, fz);
-          int fv[3] = {fx, fy, fz};
-          const int i = fv[0] > 0 ? 0 : (fv[1] > 0 ? 1 : 2);
-          const int nn = fv[i] - 1;  // exponent of f - 1_i along i
-          fv[i] -= 1;
-          const int f1 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 2);  // in-level index at lf-1
+          const int i = ib_gen_dir(fx, fy);
+          const unsigned tf = em[i * IB_GEN_NCT + ib_ncum(lf - 1) + fc];
+          const int nn = (int)(tf >> 9) - 1;              // exponent of f - 1_i along i
+          const int f1 = (int)(tf & 511) - ib_ncum(lf - 2);  // in-level index of f - 1_i at lf-1
           int f2 = 0;
-          if (nn > 0) {
-            fv[i] -= 1;
-            f2 = ib_cidx(fv[0], fv[1], fv[2]) - ib_ncum(lf - 3);
-          }
+          if (nn > 0) f2 = (int)(em[i * IB_GEN_NCT + (tf & 511)] & 511) - ib_ncum(lf - 3);  // f - 2_i
           const double qc = sh.QC[i], wq = sh.WQ[i], t2 = nn * sh.o2e, roe = sh.roe, o2zpe = sh.o2zpe;
           const double* __restrict__ r10 = s1 + ((size_t)m * nc1 + f1) * E_;
           const double* __restrict__ r11 = s1 + ((size_t)(m + 1) * nc1 + f1) * E_;
@@ -396,15 +394,9 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
         const int b = rest % ncb, e = rest / ncb;
         int bx, by, bz;
         ib_ct_get(ct, ib_ncum(j - 1) + b, bx, by, bz);
-        int bv[3] = {bx, by, bz};
-        const int i = bv[0] > 0 ? 0 : (bv[1] > 0 ? 1 : 2);
-        bv[i] -= 1;
-        const int bm = ib_cidx(bv[0], bv[1], bv[2]) - ib_ncum(j - 2);
-        int ex, ey, ez;
-        ib_ct_get(ct, d.e0 + e, ex, ey, ez);
-        int ev[3] = {ex, ey, ez};
-        ev[i] += 1;
-        const int ep = ib_cidx(ev[0], ev[1], ev[2]) - d.e0;
+        const int i = ib_gen_dir(bx, by);
+        const int bm = (int)(em[i * IB_GEN_NCT + ib_ncum(j - 1) + b] & 511) - ib_ncum(j - 2);  // b - 1_i
+        const int ep = (int)eu[i * IB_GEN_NCT + d.e0 + e] - d.e0;                             // e + 1_i
         dst[idx] = src[((size_t)ep * ncp + bm) * d.nf + f] + sh.AB[i] * src[((size_t)e * ncp + bm) * d.nf + f];
       }
       __syncthreads();
@@ -422,15 +414,9 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
         const int c = rest % nc_j, ab = rest / nc_j;
         int dx, dy, dz;
         ib_ct_get(ct, ib_ncum(j - 1) + dd, dx, dy, dz);
-        int dv[3] = {dx, dy, dz};
-        const int i = dv[0] > 0 ? 0 : (dv[1] > 0 ? 1 : 2);
-        dv[i] -= 1;
-        const int dm = ib_cidx(dv[0], dv[1], dv[2]) - ib_ncum(j - 2);
-        int cx, cy, cz;
-        ib_ct_get(ct, d.f0 + c, cx, cy, cz);
-        int cv[3] = {cx, cy, cz};
-        cv[i] += 1;
-        const int cp = ib_cidx(cv[0], cv[1], cv[2]) - d.f0;
+        const int i = ib_gen_dir(dx, dy);
+        const int dm = (int)(em[i * IB_GEN_NCT + ib_ncum(j - 1) + dd] & 511) - ib_ncum(j - 2);  // d - 1_i
+        const int cp = (int)eu[i * IB_GEN_NCT + d.f0 + c] - d.f0;                              // c + 1_i
         dst[idx] = src[((size_t)ab * nc_p + cp) * ndp + dm] + sh.CD[i] * src[((size_t)ab * nc_p + c) * ndp + dm];
       }
       __syncthreads();
@@ -440,6 +426,7 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
     int dims[4] = {ib_ncart(d.la), ib_ncart(d.lb), ib_ncart(d.lc), ib_ncart(d.ld)};
     const int ls[4] = {d.la, d.lb, d.lc, d.ld};
     if (sph) {
+#pragma unroll  // constant axis: dims, nd and ls stay in registers
       for (int axis = 3; axis >= 0; --axis) {
         double* dst = (src == h0) ? h1 : h0;
         const int l = ls[axis], ncs = ib_ncart(l), ns = 2 * l + 1;
@@ -462,13 +449,14 @@ __device__ __forceinline__ void ib_gen_item(const IbLaunch& a, int p, int sph, d
       }
     }
     double* o = a.out + sh.off;
-    const int n = dims[0] * dims[1] * dims[2] * dims[3];
+    // the block's extents and strides in registers (dims is indexed by axis above)
+    const int n1 = dims[1], n2 = dims[2], n3 = dims[3], n = dims[0] * n1 * n2 * n3;
+    const long long st0 = sh.st[0], st1 = sh.st[1], st2 = sh.st[2], st3 = sh.st[3];
     for (int idx = tid; idx < n; idx += nt) {
-      const int i3 = idx % dims[3], r3 = idx / dims[3];
-      const int i2 = r3 % dims[2], r2 = r3 / dims[2];
-      const int i1 = r2 % dims[1], i0 = r2 / dims[1];
-      double* dst = o + (long long)i0 * sh.st[0] + (long long)i1 * sh.st[1] + (long long)i2 * sh.st[2] +
-                    (long long)i3 * sh.st[3];
+      const int i3 = idx % n3, r3 = idx / n3;
+      const int i2 = r3 % n2, r2 = r3 / n2;
+      const int i1 = r2 % n1, i0 = r2 / n1;
+      double* dst = o + i0 * st0 + i1 * st1 + i2 * st2 + i3 * st3;
       // each element once per pass; an earlier pass's stores are visible after its closing barrier
       *dst = first ? src[idx] : *dst + src[idx];
     }
@@ -488,8 +476,9 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
   __shared__ IbGenShared sh;
   __shared__ unsigned short ct[IB_GEN_NCT];
   __shared__ unsigned short em[3 * IB_GEN_NCT];
+  __shared__ unsigned short eu[3 * IB_GEN_NCT];
   __shared__ int ticket;
-  ib_gen_tables(ct, em);
+  ib_gen_tables(ct, em, eu);
   __syncthreads();
   const int tid = threadIdx.x;
   int crank = 0;
@@ -515,7 +504,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
     return wk.redo ? a.redo[2 + a.redo_cap - 1 - t] : lb + t;
   };
   if (!wk.tickets) {  // fixed order, one block per item
-    for (int t = blockIdx.x; t < nh + nl; t += gridDim.x) ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em);
+    for (int t = blockIdx.x; t < nh + nl; t += gridDim.x) ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em, eu);
     return;
   }
   if constexpr (CS > 1) {
@@ -526,7 +515,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
       const int t = *cl.map_shared_rank(&ticket, 0);
       cl.sync();  // read by every rank before rank 0 takes the next ticket
       if (t >= nh) break;
-      ib_gen_item<CS>(a, item(t), sph, w, wc, slice, crank, sh, ct, em);
+      ib_gen_item<CS>(a, item(t), sph, w, wc, slice, crank, sh, ct, em, eu);
     }
   } else {
     for (;;) {
@@ -535,7 +524,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
       const int t = ticket;
       __syncthreads();
       if (t >= nh) break;
-      ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em);
+      ib_gen_item<1>(a, item(t), sph, w, w, slice, 0, sh, ct, em, eu);
     }
   }
   for (;;) {
@@ -544,7 +533,7 @@ __global__ void __launch_bounds__(IB_GEN_BLOCK, MINB) ib_eri_generic(const IbLau
     const int t = ticket;
     __syncthreads();
     if (t >= nl) break;
-    ib_gen_item<1>(a, item(nh + t), sph, w, w, slice, 0, sh, ct, em);
+    ib_gen_item<1>(a, item(nh + t), sph, w, w, slice, 0, sh, ct, em, eu);
   }
 }
 
@@ -641,5 +630,29 @@ cudaError_t ib_generic_launch(int grid, cudaStream_t s, const IbLaunch& a, const
     case 3: return launch_bps<3>(grid, s, a, wk, sph, scratch, slice);
     case 4: return launch_bps<4>(grid, s, a, wk, sph, scratch, slice);
     default: return launch_bps<2>(grid, s, a, wk, sph, scratch, slice);
+  }
+}
+
+namespace {
+template <int MINB>
+int grid_of(int cs, int grid) {
+  if (cs == 2) return 2 * std::min(grid / 2, split_clusters_resident<MINB, 2>());
+  if (cs == 4) return 4 * std::min(grid / 4, split_clusters_resident<MINB, 4>());
+  return grid;
+}
+}  // namespace
+
+extern "C" int intception_b200_generic_grid(int cluster_size) {
+  if (cluster_size != 1 && cluster_size != 2 && cluster_size != 4) return -1;
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return -1;
+  }
+  const int grid = ib_generic_bps() * nsm;
+  switch (ib_generic_bps()) {
+    case 3: return grid_of<3>(cluster_size, grid);
+    case 4: return grid_of<4>(cluster_size, grid);
+    default: return grid_of<2>(cluster_size, grid);
   }
 }

@@ -118,6 +118,8 @@ def load():
     lib.intception_b200_set_hrr_tol.restype = C.c_int
     lib.intception_b200_last_hrr_redo.argtypes = []
     lib.intception_b200_last_hrr_redo.restype = C.c_int
+    lib.intception_b200_generic_grid.argtypes = [C.c_int]
+    lib.intception_b200_generic_grid.restype = C.c_int
     lib.intception_b200_set_class_minb.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.intception_b200_set_class_minb.restype = C.c_int
     lib.intception_b200_set_class_fp32.argtypes = [C.c_int, C.c_int]
@@ -184,6 +186,12 @@ def last_hrr_redo():
     """Quartets of the last batch the generic kernel recomputed for the HRR
     check (waits for the device)."""
     return load().intception_b200_last_hrr_redo()
+
+
+def generic_grid(cluster_size):
+    """Blocks of the generic kernel's launch with heavy quartets split over
+    clusters of cluster_size blocks (1: no clusters) on the current device."""
+    return load().intception_b200_generic_grid(int(cluster_size))
 
 
 def set_class_minb(cls, variant, minb):

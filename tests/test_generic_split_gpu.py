@@ -40,6 +40,17 @@ def test_heavy_generic_quartets_are_reproducible():
     assert np.array_equal(_run(b), _run(b))
 
 
+def test_cluster_grids():
+    import torch
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    full = eri.generic_grid(1)
+    assert full >= nsm
+    for cs in (2, 4):
+        g = eri.generic_grid(cs)
+        assert 0 < g <= full and g % cs == 0
+    assert eri.generic_grid(3) == -1
+
+
 def test_split_redo_lists_are_reproducible():
     # the redo lists (4-block clusters): quartets of unrolled classes the HRR check hands over
     b, _, _ = load_batch('mixed_contraction_sph')
