@@ -559,6 +559,15 @@ int ib_generic_split() {
   return v;
 }
 
+int ib_generic_split_min() {
+  static const int v = [] {
+    const char* e = getenv("INTCEPTION_B200_GENERIC_SPLIT_MIN");
+    const int x = e ? atoi(e) : IB_GEN_SPLIT_MIN;
+    return x >= 1 ? x : IB_GEN_SPLIT_MIN;
+  }();
+  return v;
+}
+
 namespace {
 
 // Clusters of CS blocks of the split kernel resident at once on the current

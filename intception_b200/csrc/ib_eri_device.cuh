@@ -53,6 +53,7 @@ struct IbLaunch {
                            // [1] light count, then redo_cap slots, heavy items from the front,
                            // light ones from the back
   int redo_cap;            // slots of the redo list (the batch's item count)
+  int split_min;           // primitive quartets from which a generic quartet is heavy (ib_generic_split_min)
   double hrr_tol;          // class kernels: largest accepted HRR rounding-error estimate (0: no check)
   int recheck;             // FP64 kernels: evaluate only items with flag bit 0
   double mixed_tol;        // FP32 kernels: largest accepted error bound per quartet
@@ -74,10 +75,12 @@ struct IbLaunch {
 // with 32 units a quartet that passes a tolerance t is within about 0.7 t.
 #define IB_HRR_ERR_COEF (32.0 * 1.1102230246251565e-16)
 
-// The generic kernel splits a quartet of at least IB_GEN_SPLIT_MIN primitive
-// quartets ("heavy") over the blocks of a thread-block cluster (2 or 4, the
-// launch's IbGenWork::split).
+// The generic kernel splits a quartet of at least split_min primitive quartets
+// ("heavy") over the blocks of a thread-block cluster (2 or 4, the launch's
+// IbGenWork::split); split_min is IB_GEN_SPLIT_MIN unless
+// INTCEPTION_B200_GENERIC_SPLIT_MIN sets another (ib_generic_split_min).
 #define IB_GEN_SPLIT_MIN 128
+int ib_generic_split_min();
 
 // Puts sorted item p on the generic kernel's redo list once (flag bit 1):
 // heavy quartets at the front of the list, light ones at the back.
@@ -85,7 +88,7 @@ __device__ __forceinline__ void ib_redo_push(const IbLaunch& a, int p) {
   if (atomicOr(a.flags + p, 2) & 2) return;
   const int* s = a.items[p].s;
   const int np = a.shell_k[s[0]] * a.shell_k[s[1]] * a.shell_k[s[2]] * a.shell_k[s[3]];
-  if (np >= IB_GEN_SPLIT_MIN)
+  if (np >= a.split_min)
     a.redo[2 + atomicAdd(a.redo, 1)] = p;
   else
     a.redo[2 + a.redo_cap - 1 - atomicAdd(a.redo + 1, 1)] = p;

@@ -207,6 +207,7 @@ extern "C" int intception_b200_eri_batch_noalloc(const intception_b200_basis* ba
   a.out = out;
   a.status = d->status;
   a.slice_boost = 1;
+  a.split_min = IB_GEN_SPLIT_MIN;  // unused here: one block per quartet, no redo list
   const long long grid = std::min<long long>({(long long)nq, (long long)ib_generic_bps() * d->nsm, fit});
   // one block per quartet in a fixed order (no tickets: nothing to zero, no cluster)
   const cudaError_t e =

@@ -193,8 +193,8 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
                             const int* __restrict__ shell_k, const int* __restrict__ shell_ptr,
                             const double* __restrict__ prim_exp, const double* __restrict__ shell_xyz, int nq,
                             int lmax, const double* __restrict__ bounds, double skip_below, double thr, int mixed,
-                            const int* __restrict__ kind, int route_rev, unsigned* __restrict__ keys,
-                            int* __restrict__ vals, int* status) {
+                            const int* __restrict__ kind, int route_rev, int split_min,
+                            unsigned* __restrict__ keys, int* __restrict__ vals, int* status) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     int s[4], l[4], st[4] = {0, 0, 0, 0};
     bool bad = false;
@@ -236,7 +236,7 @@ __global__ void ib_classify(const int* __restrict__ quartets, const int* __restr
       const unsigned long long cost = (unsigned long long)max(nprim, 1) * (unsigned long long)(ne * nf + 64);
       const int e2 = 63 - __clzll((long long)cost);  // >= 6
       const int qc = min(255, 4 * e2 + (int)((cost >> (e2 - 2)) & 3));
-      low = (unsigned(nprim < IB_GEN_SPLIT_MIN) << 12) | (unsigned(255 - qc) << 4);
+      low = (unsigned(nprim < split_min) << 12) | (unsigned(255 - qc) << 4);
     }
     keys[q] = (unsigned(skip) << 15) | (unsigned(gen) << 14) | (unsigned(fp32) << 13) | low;
     vals[q] = q;
@@ -574,6 +574,7 @@ IbLaunch base_launch(Context* c) {
   a.sph = c->sph.as<double>();
   a.status = c->status.as<int>();
   a.slice_boost = c->slice_boost;
+  a.split_min = ib_generic_split_min();
   return a;
 }
 
@@ -1099,7 +1100,7 @@ int batch_impl(Context* c, const intception_b200_basis* basis, const int* quarte
                                    basis->shell_xyz, nq, basis->lmax,
                                    use_bounds ? bounds : nullptr, skip_below, fp32_below,
                                    precision == IB_PREC_MIXED ? 1 : 0, c->kind.as<int>(), c->hrr_tol > 0.0 ? 0 : 1,
-                                   c->keys.as<unsigned>(),
+                                   ib_generic_split_min(), c->keys.as<unsigned>(),
                                    c->vals.as<int>(), c->status.as<int>());
   ++*nl;
   IB_CUDA(cudaGetLastError());
