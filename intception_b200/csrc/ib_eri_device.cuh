@@ -79,7 +79,10 @@ struct IbLaunch {
 // ("heavy") over the blocks of a thread-block cluster (2 or 4, the launch's
 // IbGenWork::split); split_min is IB_GEN_SPLIT_MIN unless
 // INTCEPTION_B200_GENERIC_SPLIT_MIN sets another (ib_generic_split_min).
-#define IB_GEN_SPLIT_MIN 128
+// 512: on the l <= 4 workload's classes, 2 000 quartets each, 3-10 % faster
+// than 128 per live primitive quartet ((gg|ff) with the HRR check 291 against
+// 323 ns), 1 024 no better
+#define IB_GEN_SPLIT_MIN 512
 int ib_generic_split_min();
 
 // Puts sorted item p on the generic kernel's redo list once (flag bit 1):

@@ -317,14 +317,13 @@ def _quad_one(args):
 
 def generic_split():
     """generic_split_sph.npz: l 3..4 quartets (exponents log-uniform in
-    [0.1, 1e3], centres in a 3-bohr cube), 16 with K = 4 on every shell (256
+    [0.1, 1e3], centres in a 3-bohr cube), 16 with K = 5 on every shell (625
     primitive quartets each: the generic kernel splits those of its classes
-    over a cluster) and 16 with K drawn from 1, 2, 4 (light and heavy mixed).
-    out holds exact values (the C restatement in binary128); the restatement
-    in double is off by up to 7.5e-12 on them (on one (fg|gf) quartet)."""
+    over a cluster) and 16 with K drawn from 1, 2, 5 (light and heavy mixed).
+    out holds exact values (the C restatement in binary128)."""
     T = basis.sph_matrices(6)
-    heavy = basis.independent_quartet_batch(11, 16, [3, 4], [4], 0.1, 1.0e3, 3.0, True)
-    mixed_k = basis.independent_quartet_batch(11, 16, [3, 4], [1, 2, 4], 0.1, 1.0e3, 3.0, True)
+    heavy = basis.independent_quartet_batch(11, 16, [3, 4], [5], 0.1, 1.0e3, 3.0, True)
+    mixed_k = basis.independent_quartet_batch(11, 16, [3, 4], [1, 2, 5], 0.1, 1.0e3, 3.0, True)
     mb = compact_batch([(heavy, q) for q in range(heavy.nq)] + [(mixed_k, q) for q in range(mixed_k.nq)])
     from multiprocessing import Pool
     with Pool(os.cpu_count() or 1) as p:

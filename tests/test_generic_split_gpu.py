@@ -1,6 +1,6 @@
 """Heavy quartets of the generic kernel: one quartet shared by a cluster.
 
-A quartet of 128 or more primitive quartets that the generic kernel evaluates
+A quartet of 512 or more primitive quartets that the generic kernel evaluates
 (its class has no unrolled kernel, or the HRR check put it on the redo list)
 is split over the 8 blocks of a thread-block cluster, each taking every 8th
 primitive quartet; the partial contracted tables are summed in rank order.
@@ -25,10 +25,10 @@ def _run(b):
 
 def test_heavy_generic_quartets_match_exact_values():
     # l 3..4: (gf|gf), (gg|gf), (gg|gg) run on the generic kernel, the other
-    # classes on their unrolled kernels beside it; K = 4 on every shell of the
-    # first 16 quartets (256 primitive quartets each), K in 1, 2, 4 on the rest.
-    # The exact values are binary128 evaluations of the C restatement (its
-    # double evaluation is off by up to 7.5e-12 here)
+    # classes on their unrolled kernels beside it; K = 5 on every shell of the
+    # first 16 quartets (625 primitive quartets each, above the split
+    # threshold of 512), K in 1, 2, 5 on the rest.  The exact values are
+    # binary128 evaluations of the C restatement
     b, _, exact = load_batch('generic_split_sph')
     out = _run(b)
     assert np.abs(out - exact).max() <= tolerance(exact)
